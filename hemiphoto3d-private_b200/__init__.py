@@ -1,0 +1,415 @@
+"""B200 PatchMatch multi-view stereo: Python binding of the C ABI in include/hpmvs.h.
+
+The engine is the CUDA library ``lib/libhpmvs.so`` built in-tree for sm_100a.
+This module only binds it (ctypes) and mirrors the reference's stage call
+``runPatchMatchMVS(images, cameras, sfm, config)``
+(src/dense_recon/patchmatch_mvs.h:39-44) as :func:`run_patchmatch_mvs`, with the
+SfM-derived inputs (source views, depth range) passed explicitly.  There is no
+CPU fallback: importing without the built library raises ``ImportError``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libhpmvs.so")
+
+MAX_SOURCES = 8
+MAX_RADIUS = 7
+
+OK = 0
+STATUS_NAMES = {
+    0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of device memory", 4: "not found",
+    5: "timed out", 6: "unsupported", 7: "I/O error", 8: "busy", 9: "cancelled",
+}
+DTYPE_U8, DTYPE_F16, DTYPE_F32 = 0, 1, 2
+PRECISION_F32, PRECISION_F16ACC = 0, 1
+MEMORY_HOST, MEMORY_DEVICE = 0, 1
+
+
+class HpError(RuntimeError):
+    """A non-OK hp_status; ``status`` holds the code."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class Camera(C.Structure):
+    _fields_ = [("K", C.c_double * 9), ("R", C.c_double * 9), ("t", C.c_double * 3)]
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("radius", C.c_int), ("stride", C.c_int), ("top_k", C.c_int), ("precision", C.c_int),
+        ("refine_steps", C.c_int), ("iter_decay", C.c_float), ("step_decay", C.c_float),
+        ("tile_w", C.c_int), ("tile_h", C.c_int),
+    ]
+
+
+class Job(C.Structure):
+    _fields_ = [
+        ("ref_image", C.c_int), ("num_sources", C.c_int), ("src_images", C.c_int * MAX_SOURCES),
+        ("ref_cam", Camera), ("src_cams", Camera * MAX_SOURCES),
+        ("depth_min", C.c_float), ("depth_max", C.c_float),
+        ("seed", C.c_uint64), ("view_id", C.c_uint32), ("iterations", C.c_int),
+        ("use_coeffs", C.c_int), ("kinv", C.c_float * 9), ("ab", (C.c_float * 12) * MAX_SOURCES),
+    ]
+
+
+class Maps(C.Structure):
+    _fields_ = [("memory", C.c_int), ("depth", C.c_void_p), ("normal", C.c_void_p), ("cost", C.c_void_p)]
+
+
+def _load() -> C.CDLL:
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is not built; run `make -C {_HERE}` (or __graft_entry__.build()) first")
+    lib = C.CDLL(LIB_PATH)
+    P = C.POINTER
+    sigs = {
+        "hp_status_string": (C.c_char_p, [C.c_int]),
+        "hp_params_default": (None, [P(Params)]),
+        "hp_version": (C.c_char_p, []),
+        "hp_ctx_create": (C.c_int, [C.c_int, P(C.c_void_p)]),
+        "hp_ctx_destroy": (C.c_int, [C.c_void_p]),
+        "hp_ctx_last_error": (C.c_char_p, [C.c_void_p]),
+        "hp_ctx_synchronize": (C.c_int, [C.c_void_p]),
+        "hp_ctx_mem_info": (C.c_int, [C.c_void_p, P(C.c_size_t), P(C.c_size_t)]),
+        "hp_image_upload": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, P(C.c_int)]),
+        "hp_image_release": (C.c_int, [C.c_void_p, C.c_int]),
+        "hp_image_size": (C.c_int, [C.c_void_p, C.c_int, P(C.c_int), P(C.c_int)]),
+        "hp_setup_homographies": (C.c_int, [P(Camera), P(Camera), C.c_int, P(C.c_double), P(C.c_double)]),
+        "hp_solve": (C.c_int, [C.c_void_p, P(Job), C.c_int, P(Params), P(Maps)]),
+        "hp_init_hypotheses": (C.c_int, [C.c_void_p, P(Job), P(Params), P(Maps)]),
+        "hp_ncc_cost": (C.c_int, [C.c_void_p, P(Job), P(Params), P(Maps)]),
+        "hp_propagate_pass": (C.c_int, [C.c_void_p, P(Job), P(Params), P(Maps), C.c_int, C.c_int]),
+        "hp_geometric_filter": (C.c_int, [C.c_void_p, P(Camera), C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                          C.c_void_p, C.c_int, P(Camera), P(C.c_void_p), P(C.c_void_p),
+                                          C.c_int, C.c_float, C.c_float, C.c_int]),
+        "hp_pfm_write": (C.c_int, [C.c_char_p, C.c_void_p, C.c_int, C.c_int, C.c_int]),
+        "hp_pfm_read": (C.c_int, [C.c_char_p, C.c_void_p, C.c_size_t, P(C.c_int), P(C.c_int), P(C.c_int)]),
+    }
+    for name, (res, args) in sigs.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+#: Every exported entry point of include/hpmvs.h (checked against the .so by the tests).
+EXPORTS = (
+    "hp_status_string", "hp_params_default", "hp_version", "hp_ctx_create", "hp_ctx_destroy",
+    "hp_ctx_last_error", "hp_ctx_synchronize", "hp_ctx_mem_info", "hp_image_upload", "hp_image_release",
+    "hp_image_size", "hp_setup_homographies", "hp_solve", "hp_init_hypotheses", "hp_ncc_cost",
+    "hp_propagate_pass", "hp_geometric_filter", "hp_pfm_write", "hp_pfm_read",
+)
+
+
+def default_params(**kw) -> Params:
+    """hp_params_default() with keyword overrides (radius, stride, precision, ...)."""
+    p = Params()
+    lib.hp_params_default(C.byref(p))
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise TypeError(f"unknown parameter {k}")
+        setattr(p, k, v)
+    return p
+
+
+def make_camera(K, R, t) -> Camera:
+    c = Camera()
+    c.K[:] = [float(v) for v in np.asarray(K, np.float64).ravel()]
+    c.R[:] = [float(v) for v in np.asarray(R, np.float64).ravel()]
+    c.t[:] = [float(v) for v in np.asarray(t, np.float64).ravel()]
+    return c
+
+
+def setup_homographies(ref: Camera, srcs: Sequence[Camera]):
+    """FP64 (K_ref^-1, [A|b] per source) as the engine computes them."""
+    n = len(srcs)
+    kinv = (C.c_double * 9)()
+    ab = (C.c_double * (12 * max(n, 1)))()
+    arr = (Camera * max(n, 1))(*srcs)
+    st = lib.hp_setup_homographies(C.byref(ref), arr, n, kinv, ab)
+    if st != OK:
+        raise HpError(st, "hp_setup_homographies")
+    return np.array(kinv[:], np.float64).reshape(3, 3), np.array(ab[: 12 * n], np.float64).reshape(n, 12)
+
+
+def _ptr(a) -> int:
+    """Address of a numpy array (host) or a torch tensor (device)."""
+    if isinstance(a, np.ndarray):
+        if not a.flags["C_CONTIGUOUS"]:
+            raise ValueError("arrays must be C-contiguous")
+        return a.ctypes.data
+    return int(a.data_ptr())
+
+
+def _mem(a) -> int:
+    return MEMORY_HOST if isinstance(a, np.ndarray) else MEMORY_DEVICE
+
+
+class Context:
+    """An engine context (hp_ctx): one device, one stream, resident images."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        st = lib.hp_ctx_create(device, C.byref(h))
+        if st != OK:
+            raise HpError(st, f"hp_ctx_create(device={device})")
+        self._h = h
+        self.device = device
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.hp_ctx_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st: int, what: str):
+        if st != OK:
+            raise HpError(st, f"{what}: {lib.hp_ctx_last_error(self._h).decode()}")
+
+    @property
+    def handle(self):
+        return self._h
+
+    def synchronize(self):
+        self._check(lib.hp_ctx_synchronize(self._h), "hp_ctx_synchronize")
+
+    def mem_info(self):
+        f, t = C.c_size_t(), C.c_size_t()
+        self._check(lib.hp_ctx_mem_info(self._h, C.byref(f), C.byref(t)), "hp_ctx_mem_info")
+        return f.value, t.value
+
+    def upload(self, img) -> int:
+        """Upload a grayscale image (numpy u8/f16/f32 on host, or a contiguous torch CUDA tensor)."""
+        dt = {np.dtype(np.uint8): DTYPE_U8, np.dtype(np.float16): DTYPE_F16, np.dtype(np.float32): DTYPE_F32}
+        if isinstance(img, np.ndarray):
+            img = np.ascontiguousarray(img)
+            code = dt.get(img.dtype)
+        else:
+            import torch
+            code = {torch.uint8: DTYPE_U8, torch.float16: DTYPE_F16, torch.float32: DTYPE_F32}.get(img.dtype)
+            if not img.is_contiguous():
+                raise ValueError("device image must be contiguous")
+        if code is None:
+            raise TypeError(f"unsupported image dtype {img.dtype}")
+        h, w = img.shape
+        iid = C.c_int()
+        self._check(lib.hp_image_upload(self._h, _ptr(img), _mem(img), w, h, code, C.byref(iid)), "hp_image_upload")
+        return iid.value
+
+    def release(self, image_id: int):
+        self._check(lib.hp_image_release(self._h, image_id), "hp_image_release")
+
+    def solve(self, jobs: Sequence[Job], params: Params, outs: Sequence[Maps]):
+        jarr = (Job * len(jobs))(*jobs)
+        marr = (Maps * len(outs))(*outs)
+        self._check(lib.hp_solve(self._h, jarr, len(jobs), C.byref(params), marr), "hp_solve")
+
+    def init_hypotheses(self, job: Job, params: Params, maps: Maps):
+        self._check(lib.hp_init_hypotheses(self._h, C.byref(job), C.byref(params), C.byref(maps)),
+                    "hp_init_hypotheses")
+
+    def ncc_cost(self, job: Job, params: Params, maps: Maps):
+        self._check(lib.hp_ncc_cost(self._h, C.byref(job), C.byref(params), C.byref(maps)), "hp_ncc_cost")
+
+    def propagate_pass(self, job: Job, params: Params, maps: Maps, iteration: int, color: int):
+        self._check(lib.hp_propagate_pass(self._h, C.byref(job), C.byref(params), C.byref(maps), iteration, color),
+                    "hp_propagate_pass")
+
+    def geometric_filter(self, ref_cam: Camera, depth, normal, confidence, src_cams: Sequence[Camera],
+                         src_depths, src_normals, depth_tol=0.12, normal_tol_cos=-1.0, min_consistent=2):
+        """In-place filter (depth and confidence); arrays all host numpy or all device tensors."""
+        h, w = depth.shape[:2]
+        n = len(src_cams)
+        cams = (Camera * max(n, 1))(*src_cams)
+        dps = (C.c_void_p * max(n, 1))(*[_ptr(a) for a in src_depths])
+        nps = (C.c_void_p * max(n, 1))(*[_ptr(a) for a in src_normals])
+        self._check(lib.hp_geometric_filter(self._h, C.byref(ref_cam), w, h, _ptr(depth), _ptr(normal),
+                                            _ptr(confidence), n, cams, dps, nps, _mem(depth), depth_tol,
+                                            normal_tol_cos, min_consistent), "hp_geometric_filter")
+
+
+def make_job(ref_image: int, src_images: Sequence[int], ref_cam: Camera, src_cams: Sequence[Camera],
+             depth_min: float, depth_max: float, seed: int = 42, view_id: int = 0, iterations: int = 12,
+             coeffs=None) -> Job:
+    """Build an hp_job.  ``coeffs`` = (kinv[9], ab[S,12]) float32 replaces the FP64 setup."""
+    if not 1 <= len(src_images) <= MAX_SOURCES or len(src_images) != len(src_cams):
+        raise ValueError("need 1..8 sources with one camera each")
+    j = Job()
+    j.ref_image = ref_image
+    j.num_sources = len(src_images)
+    for i, s in enumerate(src_images):
+        j.src_images[i] = s
+        j.src_cams[i] = src_cams[i]
+    j.ref_cam = ref_cam
+    j.depth_min, j.depth_max = float(depth_min), float(depth_max)
+    j.seed, j.view_id, j.iterations = int(seed), int(view_id), int(iterations)
+    if coeffs is not None:
+        kinv, ab = coeffs
+        j.use_coeffs = 1
+        j.kinv[:] = [float(v) for v in np.asarray(kinv, np.float32).ravel()]
+        ab = np.asarray(ab, np.float32).reshape(-1, 12)
+        for s in range(ab.shape[0]):
+            j.ab[s][:] = [float(v) for v in ab[s]]
+    return j
+
+
+def host_maps(h: int, w: int):
+    """(Maps, depth, normal, cost) with fresh host arrays."""
+    depth = np.zeros((h, w), np.float32)
+    normal = np.zeros((h, w, 3), np.float32)
+    cost = np.zeros((h, w), np.float32)
+    return maps_of(depth, normal, cost), depth, normal, cost
+
+
+def maps_of(depth, normal, cost) -> Maps:
+    """Maps over existing arrays (host numpy or device tensors, not mixed).
+
+    The returned struct keeps the arrays alive (``.arrays``): the engine writes
+    through its raw pointers, so the arrays must outlive every call using it.
+    """
+    m = Maps(_mem(depth), _ptr(depth), _ptr(normal), _ptr(cost))
+    m.arrays = (depth, normal, cost)
+    return m
+
+
+def pfm_write(path: str, data: np.ndarray):
+    data = np.ascontiguousarray(data, np.float32)
+    ch = 1 if data.ndim == 2 else data.shape[2]
+    st = lib.hp_pfm_write(path.encode(), data.ctypes.data, data.shape[1], data.shape[0], ch)
+    if st != OK:
+        raise HpError(st, f"hp_pfm_write({path})")
+
+
+def pfm_read(path: str) -> np.ndarray:
+    w, h, ch = C.c_int(), C.c_int(), C.c_int()
+    st = lib.hp_pfm_read(path.encode(), None, 0, C.byref(w), C.byref(h), C.byref(ch))
+    if st != OK:
+        raise HpError(st, f"hp_pfm_read({path})")
+    out = np.empty((h.value, w.value, ch.value) if ch.value == 3 else (h.value, w.value), np.float32)
+    st = lib.hp_pfm_read(path.encode(), out.ctypes.data, out.size, C.byref(w), C.byref(h), C.byref(ch))
+    if st != OK:
+        raise HpError(st, f"hp_pfm_read({path})")
+    return out
+
+
+# --------------------------------------------------------------------------------------------
+# Mirror of the reference's stage API (types.h DepthMap / PipelineConfig, patchmatch_mvs.h).
+# --------------------------------------------------------------------------------------------
+
+@dataclass
+class ViewParams:
+    """MVSViewParams (src/dense_recon/patchmatch_mvs.h:22-28): a reference image, its sources, depth range."""
+    ref_image_id: int
+    source_ids: List[int]
+    depth_min: float
+    depth_max: float
+
+
+@dataclass
+class DepthMap:
+    """DepthMap (include/types.h:85-91): depth (0 = invalid), camera-frame normal, confidence = 1 - cost/2."""
+    image_id: int
+    depth: np.ndarray
+    normal: np.ndarray
+    confidence: np.ndarray
+    cost: np.ndarray = field(repr=False, default=None)
+
+    @property
+    def width(self):
+        return self.depth.shape[1]
+
+    @property
+    def height(self):
+        return self.depth.shape[0]
+
+
+@dataclass
+class MVSConfig:
+    """The PipelineConfig fields the stage reads (include/types.h:120-169, patchmatch_mvs.cu:1065-1070)."""
+    mvs_iterations: int = 12
+    mvs_patch_size: int = 11
+    window_stride: int = 1
+    precision: int = PRECISION_F32
+    geometric_filter: bool = True
+    save_intermediate: bool = False
+    output_dir: Optional[str] = None
+    device: int = 0
+
+
+def run_patchmatch_mvs(images: Sequence[np.ndarray], cameras: Sequence[Camera], views: Sequence[ViewParams],
+                       config: MVSConfig = MVSConfig(), ctx: Optional[Context] = None) -> List[DepthMap]:
+    """runPatchMatchMVS (patchmatch_mvs.cu:1028-1388) with explicit view parameters.
+
+    Views without sources are skipped (:1089-1092); the per-view seed is
+    42 + 1e6 * ref_id (:1106); radius = (patch_size - 1) / 2 clamped to 1..7;
+    confidence = 1 - cost / 2 (:1246-1252); with iterations > 0 and >= 2 maps the
+    geometric filter runs with tolerance 0.12, normal check off, 2 agreeing
+    sources (:1267-1384); PFM depth is written per view when save_intermediate.
+    """
+    own = ctx is None
+    ctx = ctx or Context(config.device)
+    try:
+        radius = min(MAX_RADIUS, max(1, (config.mvs_patch_size - 1) // 2))
+        params = default_params(radius=radius, stride=config.window_stride, precision=config.precision)
+        ids = {}
+        views = [v for v in views if v.source_ids]
+        for v in views:
+            for i in [v.ref_image_id, *v.source_ids]:
+                if i not in ids:
+                    ids[i] = ctx.upload(images[i])
+        jobs, outs, maps = [], [], []
+        for v in views:
+            h, w = images[v.ref_image_id].shape[:2]
+            m, d, n, c = host_maps(h, w)
+            jobs.append(make_job(ids[v.ref_image_id], [ids[s] for s in v.source_ids], cameras[v.ref_image_id],
+                                 [cameras[s] for s in v.source_ids], v.depth_min, v.depth_max,
+                                 seed=42 + 1_000_000 * v.ref_image_id, view_id=v.ref_image_id,
+                                 iterations=config.mvs_iterations))
+            outs.append(m)
+            maps.append((d, n, c))
+        if jobs:
+            ctx.solve(jobs, params, outs)
+        result = [DepthMap(v.ref_image_id, d, n, (1.0 - c * 0.5).astype(np.float32), c)
+                  for v, (d, n, c) in zip(views, maps)]
+        if config.geometric_filter and config.mvs_iterations > 0 and len(result) >= 2:
+            # In place and in view order, as the reference does: a later view
+            # checks against sources already filtered earlier in the loop.
+            by_id = {dm.image_id: dm for dm in result}
+            for v, dm in zip(views, result):
+                srcs = [s for s in v.source_ids if s in by_id and by_id[s].depth.shape == dm.depth.shape]
+                if len(srcs) >= 2:
+                    ctx.geometric_filter(cameras[v.ref_image_id], dm.depth, dm.normal, dm.confidence,
+                                         [cameras[s] for s in srcs], [by_id[s].depth for s in srcs],
+                                         [by_id[s].normal for s in srcs])
+        if config.save_intermediate and config.output_dir:
+            for dm in result:
+                pfm_write(os.path.join(config.output_dir, f"depth_{dm.image_id}.pfm"), dm.depth)
+        for i in ids.values():
+            ctx.release(i)
+        return result
+    finally:
+        if own:
+            ctx.close()

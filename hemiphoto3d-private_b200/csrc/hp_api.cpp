@@ -1,0 +1,696 @@
+// Host side of the C ABI declared in include/hpmvs.h.
+//
+// A context owns one CUDA stream on one device, the uploaded images (FP32 and
+// FP16 pitched planes plus linear-filter texture objects over block-linear
+// arrays), and grow-only scratch for hypotheses.  A solve builds one ViewDesc
+// per job, uploads them once, and issues every red-black half-pass as a single
+// launch over the tiles of all jobs still iterating, with no host
+// synchronisation between launches (the reference synchronises after each,
+// src/utils/cuda_utils.cuh:18-22).
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "hp_internal.h"
+
+
+namespace {
+
+struct Image {
+    int W = 0, H = 0;
+    float* f32 = nullptr;
+    size_t pitch32 = 0;  // bytes
+    __half* f16 = nullptr;
+    size_t pitch16 = 0;  // bytes
+    cudaArray_t arr32 = nullptr, arr16 = nullptr;
+    cudaTextureObject_t tex32 = 0, tex16 = 0;
+};
+
+// Grow-only device buffer.
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t bytes) {
+        if (bytes <= cap) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        cudaError_t e = cudaMalloc(&p, bytes);
+        if (e == cudaSuccess) cap = bytes;
+        return e;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+}  // namespace
+
+struct hp_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    std::map<int, Image> images;
+    int next_id = 1;
+    DevBuf state;   // hypotheses + costs of all jobs of a solve
+    DevBuf descs;   // ViewDesc array
+    DevBuf lists;   // active-view lists and tile prefixes
+    DevBuf staging; // host-memory results pass through here
+};
+
+namespace {
+
+hp_status fail(hp_ctx* c, hp_status s, const char* fmt, ...) {
+    if (c) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof buf, fmt, ap);
+        va_end(ap);
+        c->err = buf;
+    }
+    return s;
+}
+
+#define HP_CUDA(call)                                                                              \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            return fail(ctx, e_ == cudaErrorMemoryAllocation ? HP_ERR_OUT_OF_MEMORY : HP_ERR_CUDA, \
+                        "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__);       \
+    } while (0)
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+void mat3_mul(const double* a, const double* b, double* c) {
+    for (int r = 0; r < 3; ++r)
+        for (int k = 0; k < 3; ++k)
+            c[3 * r + k] = a[3 * r] * b[k] + a[3 * r + 1] * b[3 + k] + a[3 * r + 2] * b[6 + k];
+}
+
+bool mat3_inv(const double* m, double* inv) {
+    double det = m[0] * (m[4] * m[8] - m[5] * m[7]) - m[1] * (m[3] * m[8] - m[5] * m[6]) +
+                 m[2] * (m[3] * m[7] - m[4] * m[6]);
+    if (!(std::fabs(det) > 1e-300)) return false;
+    double id = 1.0 / det;
+    inv[0] = (m[4] * m[8] - m[5] * m[7]) * id;
+    inv[1] = (m[2] * m[7] - m[1] * m[8]) * id;
+    inv[2] = (m[1] * m[5] - m[2] * m[4]) * id;
+    inv[3] = (m[5] * m[6] - m[3] * m[8]) * id;
+    inv[4] = (m[0] * m[8] - m[2] * m[6]) * id;
+    inv[5] = (m[2] * m[3] - m[0] * m[5]) * id;
+    inv[6] = (m[3] * m[7] - m[4] * m[6]) * id;
+    inv[7] = (m[1] * m[6] - m[0] * m[7]) * id;
+    inv[8] = (m[0] * m[4] - m[1] * m[3]) * id;
+    return true;
+}
+
+hp_status check_params(hp_ctx* ctx, const hp_params* p) {
+    if (!p) return fail(ctx, HP_ERR_INVALID_ARG, "params is null");
+    if (p->radius < 1 || p->radius > HP_MAX_RADIUS)
+        return fail(ctx, HP_ERR_INVALID_ARG, "radius %d outside 1..%d", p->radius, HP_MAX_RADIUS);
+    if (p->stride < 1 || p->stride > 2) return fail(ctx, HP_ERR_INVALID_ARG, "stride %d not 1 or 2", p->stride);
+    if (p->top_k < 1 || p->top_k > HP_MAX_TOP_K)
+        return fail(ctx, HP_ERR_INVALID_ARG, "top_k %d outside 1..%d", p->top_k, HP_MAX_TOP_K);
+    if (p->precision != HP_PRECISION_F32 && p->precision != HP_PRECISION_F16ACC)
+        return fail(ctx, HP_ERR_INVALID_ARG, "unknown precision %d", p->precision);
+    if (p->refine_steps < 0 || p->refine_steps > 4)
+        return fail(ctx, HP_ERR_INVALID_ARG, "refine_steps %d outside 0..4", p->refine_steps);
+    if (!(p->iter_decay > 0.f && p->iter_decay <= 1.f) || !(p->step_decay > 0.f && p->step_decay <= 1.f))
+        return fail(ctx, HP_ERR_INVALID_ARG, "decay factors must lie in (0, 1]");
+    return HP_OK;
+}
+
+hp::SolveConsts consts_of(const hp_params* p) {
+    hp::SolveConsts sc;
+    sc.radius = p->radius;
+    sc.stride = p->stride;
+    sc.top_k = p->top_k;
+    sc.refine_steps = p->refine_steps;
+    sc.iter_decay = p->iter_decay;
+    sc.step_decay = p->step_decay;
+    return sc;
+}
+
+// Validate a job and fill the image/camera part of its descriptor.
+hp_status fill_desc(hp_ctx* ctx, const hp_job* j, int jobno, hp::ViewDesc* d) {
+    std::memset(d, 0, sizeof *d);
+    auto it = ctx->images.find(j->ref_image);
+    if (it == ctx->images.end()) return fail(ctx, HP_ERR_NOT_FOUND, "job %d: unknown ref image %d", jobno, j->ref_image);
+    const Image& ref = it->second;
+    if (j->num_sources < 1 || j->num_sources > HP_MAX_SOURCES)
+        return fail(ctx, HP_ERR_INVALID_ARG, "job %d: num_sources %d outside 1..%d", jobno, j->num_sources,
+                    HP_MAX_SOURCES);
+    if (!(j->depth_min > 0.f) || !(j->depth_max > j->depth_min) || !std::isfinite(j->depth_max))
+        return fail(ctx, HP_ERR_INVALID_ARG, "job %d: depth range [%g, %g] invalid", jobno, j->depth_min,
+                    j->depth_max);
+    if (j->iterations < 0 || j->iterations > 1000)
+        return fail(ctx, HP_ERR_INVALID_ARG, "job %d: iterations %d outside 0..1000", jobno, j->iterations);
+    d->ref = ref.f32;
+    d->ref16 = ref.f16;
+    d->ref_pitch = static_cast<int>(ref.pitch32 / sizeof(float));
+    d->ref16_pitch = static_cast<int>(ref.pitch16 / sizeof(__half));
+    d->W = ref.W;
+    d->H = ref.H;
+    d->S = j->num_sources;
+    for (int s = 0; s < j->num_sources; ++s) {
+        auto si = ctx->images.find(j->src_images[s]);
+        if (si == ctx->images.end())
+            return fail(ctx, HP_ERR_NOT_FOUND, "job %d: unknown source image %d", jobno, j->src_images[s]);
+        if (si->second.W != ref.W || si->second.H != ref.H)
+            return fail(ctx, HP_ERR_INVALID_ARG, "job %d: source %d is %dx%d, reference is %dx%d", jobno, s,
+                        si->second.W, si->second.H, ref.W, ref.H);
+        d->src_tex[s] = si->second.tex32;
+        d->src_tex16[s] = si->second.tex16;
+    }
+    if (j->use_coeffs) {
+        std::memcpy(d->kinv, j->kinv, sizeof d->kinv);
+        for (int s = 0; s < j->num_sources; ++s) std::memcpy(d->ab[s], j->ab[s], sizeof d->ab[s]);
+    } else {
+        double kinv[9], ab[HP_MAX_SOURCES * 12];
+        hp_status st = hp_setup_homographies(&j->ref_cam, j->src_cams, j->num_sources, kinv, ab);
+        if (st != HP_OK) return fail(ctx, st, "job %d: singular reference intrinsics", jobno);
+        for (int i = 0; i < 9; ++i) d->kinv[i] = static_cast<float>(kinv[i]);
+        for (int s = 0; s < j->num_sources; ++s)
+            for (int i = 0; i < 12; ++i) d->ab[s][i] = static_cast<float>(ab[12 * s + i]);
+    }
+    d->tiles_x = (ref.W + hp::TILE_W - 1) / hp::TILE_W;
+    d->tiles_y = (ref.H + hp::TILE_H - 1) / hp::TILE_H;
+    d->dmin = j->depth_min;
+    d->dmax = j->depth_max;
+    d->seed_lo = static_cast<uint32_t>(j->seed);
+    d->seed_hi = static_cast<uint32_t>(j->seed >> 32);
+    d->view_id = j->view_id;
+    d->iterations = j->iterations;
+    return HP_OK;
+}
+
+// Everything one solve needs on the device: descriptors, state, launch lists.
+struct Prepared {
+    std::vector<hp::ViewDesc> host;   // host copies (with device pointers)
+    hp::ViewDesc* dev = nullptr;
+    std::vector<int> list_offsets;    // per iteration: offset into lists buffer
+    std::vector<int> list_counts;     // per iteration: number of active views
+    std::vector<int> list_tiles;      // per iteration: total tiles
+    int* lists = nullptr;
+    int max_iter = 0;
+};
+
+hp_status prepare(hp_ctx* ctx, const hp_job* jobs, int n, Prepared* P) {
+    P->host.resize(n);
+    size_t state_bytes = 0;
+    std::vector<size_t> offs(n);
+    for (int k = 0; k < n; ++k) {
+        hp_status st = fill_desc(ctx, &jobs[k], k, &P->host[k]);
+        if (st != HP_OK) return st;
+        offs[k] = state_bytes;
+        size_t px = static_cast<size_t>(P->host[k].W) * P->host[k].H;
+        state_bytes += ((px * sizeof(float4) + px * sizeof(float)) + 255) & ~size_t(255);
+        P->max_iter = std::max(P->max_iter, jobs[k].iterations);
+    }
+    HP_CUDA(ctx->state.ensure(state_bytes));
+    for (int k = 0; k < n; ++k) {
+        char* base = static_cast<char*>(ctx->state.p) + offs[k];
+        size_t px = static_cast<size_t>(P->host[k].W) * P->host[k].H;
+        P->host[k].hyp = reinterpret_cast<float4*>(base);
+        P->host[k].cost = reinterpret_cast<float*>(base + px * sizeof(float4));
+    }
+    HP_CUDA(ctx->descs.ensure(n * sizeof(hp::ViewDesc)));
+    P->dev = static_cast<hp::ViewDesc*>(ctx->descs.p);
+    HP_CUDA(cudaMemcpyAsync(P->dev, P->host.data(), n * sizeof(hp::ViewDesc), cudaMemcpyHostToDevice,
+                            ctx->stream));
+    // Launch lists: entry 0 covers all views (init, initial cost); entry 1+it
+    // the views still iterating at iteration it.
+    std::vector<int> ints;
+    const int n_lists = 1 + P->max_iter;
+    for (int l = 0; l < n_lists; ++l) {
+        std::vector<int> act;
+        for (int k = 0; k < n; ++k)
+            if (l == 0 || jobs[k].iterations > l - 1) act.push_back(k);
+        P->list_offsets.push_back(static_cast<int>(ints.size()));
+        P->list_counts.push_back(static_cast<int>(act.size()));
+        for (int k : act) ints.push_back(k);
+        int acc = 0;
+        for (int k : act) {
+            ints.push_back(acc);
+            acc += P->host[k].tiles_x * P->host[k].tiles_y;
+        }
+        ints.push_back(acc);
+        P->list_tiles.push_back(acc);
+    }
+    HP_CUDA(ctx->lists.ensure(ints.size() * sizeof(int)));
+    P->lists = static_cast<int*>(ctx->lists.p);
+    HP_CUDA(cudaMemcpyAsync(P->lists, ints.data(), ints.size() * sizeof(int), cudaMemcpyHostToDevice,
+                            ctx->stream));
+    // The staging vectors above are pageable: the copies complete before return.
+    HP_CUDA(cudaStreamSynchronize(ctx->stream));
+    return HP_OK;
+}
+
+hp::BatchList batch_of(const Prepared& P, int list) {
+    hp::BatchList bl;
+    bl.views = P.dev;
+    bl.n_active = P.list_counts[list];
+    bl.active = P.lists + P.list_offsets[list];
+    bl.tile_prefix = bl.active + bl.n_active;
+    bl.total_tiles = P.list_tiles[list];
+    return bl;
+}
+
+// Copy a job's packed state out to the caller's maps.
+hp_status export_maps(hp_ctx* ctx, const Prepared& P, int k, hp_maps* m, bool want_depth_normal, bool want_cost) {
+    const hp::ViewDesc& v = P.host[k];
+    const size_t px = static_cast<size_t>(v.W) * v.H;
+    float* d = want_depth_normal ? m->depth : nullptr;
+    float* nrm = want_depth_normal ? m->normal : nullptr;
+    float* c = want_cost ? m->cost : nullptr;
+    if (m->memory == HP_MEMORY_DEVICE) {
+        HP_CUDA(hp::launch_unpack(P.host.data(), k, d, nrm, c, ctx->stream));
+        return HP_OK;
+    }
+    HP_CUDA(ctx->staging.ensure(px * 5 * sizeof(float)));
+    float* sd = static_cast<float*>(ctx->staging.p);
+    float* sn = sd + px;
+    float* sc = sn + 3 * px;
+    HP_CUDA(hp::launch_unpack(P.host.data(), k, d ? sd : nullptr, nrm ? sn : nullptr, c ? sc : nullptr,
+                              ctx->stream));
+    if (d) HP_CUDA(cudaMemcpyAsync(d, sd, px * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    if (nrm) HP_CUDA(cudaMemcpyAsync(nrm, sn, 3 * px * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    if (c) HP_CUDA(cudaMemcpyAsync(c, sc, px * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    HP_CUDA(cudaStreamSynchronize(ctx->stream));
+    return HP_OK;
+}
+
+// Load caller maps into a job's packed state.
+hp_status import_maps(hp_ctx* ctx, const Prepared& P, int k, const hp_maps* m, bool with_cost) {
+    const hp::ViewDesc& v = P.host[k];
+    const size_t px = static_cast<size_t>(v.W) * v.H;
+    if (!m->depth || !m->normal || (with_cost && !m->cost))
+        return fail(ctx, HP_ERR_INVALID_ARG, "maps: depth/normal%s pointer is null", with_cost ? "/cost" : "");
+    if (m->memory == HP_MEMORY_DEVICE) {
+        HP_CUDA(hp::launch_pack(P.host.data(), k, m->depth, m->normal, with_cost ? m->cost : nullptr, ctx->stream));
+        return HP_OK;
+    }
+    HP_CUDA(ctx->staging.ensure(px * 5 * sizeof(float)));
+    float* sd = static_cast<float*>(ctx->staging.p);
+    float* sn = sd + px;
+    float* sc = sn + 3 * px;
+    HP_CUDA(cudaMemcpyAsync(sd, m->depth, px * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    HP_CUDA(cudaMemcpyAsync(sn, m->normal, 3 * px * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    if (with_cost) HP_CUDA(cudaMemcpyAsync(sc, m->cost, px * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    HP_CUDA(hp::launch_pack(P.host.data(), k, sd, sn, with_cost ? sc : nullptr, ctx->stream));
+    HP_CUDA(cudaStreamSynchronize(ctx->stream));
+    return HP_OK;
+}
+
+hp_status launch_cost(hp_ctx* ctx, const hp::BatchList& bl, const hp_params* p) {
+    hp::SolveConsts sc = consts_of(p);
+    cudaError_t e = p->precision == HP_PRECISION_F16ACC ? hp::launch_cost_f16(bl, sc, ctx->stream)
+                                                        : hp::launch_cost_f32(bl, sc, ctx->stream);
+    HP_CUDA(e);
+    return HP_OK;
+}
+
+hp_status launch_pass(hp_ctx* ctx, const hp::BatchList& bl, const hp_params* p, int it, int color) {
+    hp::SolveConsts sc = consts_of(p);
+    cudaError_t e = p->precision == HP_PRECISION_F16ACC ? hp::launch_propagate_f16(bl, sc, it, color, ctx->stream)
+                                                        : hp::launch_propagate_f32(bl, sc, it, color, ctx->stream);
+    HP_CUDA(e);
+    return HP_OK;
+}
+
+void free_image(Image& im) {
+    if (im.tex32) cudaDestroyTextureObject(im.tex32);
+    if (im.tex16) cudaDestroyTextureObject(im.tex16);
+    if (im.arr32) cudaFreeArray(im.arr32);
+    if (im.arr16) cudaFreeArray(im.arr16);
+    if (im.f32) cudaFree(im.f32);
+    if (im.f16) cudaFree(im.f16);
+    im = Image();
+}
+
+cudaError_t make_linear_texture(cudaArray_t arr, cudaTextureObject_t* tex) {
+    cudaResourceDesc rd;
+    std::memset(&rd, 0, sizeof rd);
+    rd.resType = cudaResourceTypeArray;
+    rd.res.array.array = arr;
+    cudaTextureDesc td;
+    std::memset(&td, 0, sizeof td);
+    td.addressMode[0] = cudaAddressModeClamp;
+    td.addressMode[1] = cudaAddressModeClamp;
+    td.filterMode = cudaFilterModeLinear;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 0;
+    return cudaCreateTextureObject(tex, &rd, &td, nullptr);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* hp_status_string(hp_status s) {
+    switch (s) {
+        case HP_OK: return "ok";
+        case HP_ERR_INVALID_ARG: return "invalid argument";
+        case HP_ERR_CUDA: return "CUDA error";
+        case HP_ERR_OUT_OF_MEMORY: return "out of device memory";
+        case HP_ERR_NOT_FOUND: return "not found";
+        case HP_ERR_TIMEOUT: return "timed out";
+        case HP_ERR_UNSUPPORTED: return "unsupported";
+        case HP_ERR_IO: return "I/O error";
+        case HP_ERR_BUSY: return "busy";
+        case HP_ERR_CANCELLED: return "cancelled";
+    }
+    return "unknown status";
+}
+
+const char* hp_version(void) { return "0.1.0"; }
+
+void hp_params_default(hp_params* p) {
+    if (!p) return;
+    p->radius = 5;
+    p->stride = 1;
+    p->top_k = 3;
+    p->precision = HP_PRECISION_F32;
+    p->refine_steps = 2;
+    p->iter_decay = 0.6f;
+    p->step_decay = 0.5f;
+    p->tile_w = 0;
+    p->tile_h = 0;
+}
+
+hp_status hp_ctx_create(int device, hp_ctx** out) {
+    if (!out) return HP_ERR_INVALID_ARG;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return HP_ERR_CUDA;
+    }
+    if (device < 0 || device >= n) return HP_ERR_INVALID_ARG;
+    std::unique_ptr<hp_ctx> c(new hp_ctx);
+    c->device = device;
+    DeviceGuard g(device);
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return HP_ERR_CUDA;
+    *out = c.release();
+    return HP_OK;
+}
+
+hp_status hp_ctx_destroy(hp_ctx* ctx) {
+    if (!ctx) return HP_ERR_INVALID_ARG;
+    {
+        DeviceGuard g(ctx->device);
+        cudaStreamSynchronize(ctx->stream);
+        for (auto& kv : ctx->images) free_image(kv.second);
+        ctx->state.release();
+        ctx->descs.release();
+        ctx->lists.release();
+        ctx->staging.release();
+        cudaStreamDestroy(ctx->stream);
+    }
+    delete ctx;
+    return HP_OK;
+}
+
+const char* hp_ctx_last_error(const hp_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+hp_status hp_ctx_synchronize(hp_ctx* ctx) {
+    if (!ctx) return HP_ERR_INVALID_ARG;
+    DeviceGuard g(ctx->device);
+    HP_CUDA(cudaStreamSynchronize(ctx->stream));
+    return HP_OK;
+}
+
+hp_status hp_ctx_mem_info(hp_ctx* ctx, size_t* free_bytes, size_t* total_bytes) {
+    if (!ctx || !free_bytes || !total_bytes) return HP_ERR_INVALID_ARG;
+    DeviceGuard g(ctx->device);
+    HP_CUDA(cudaMemGetInfo(free_bytes, total_bytes));
+    return HP_OK;
+}
+
+hp_status hp_image_upload(hp_ctx* ctx, const void* data, int memory, int width, int height, int dtype,
+                          int* image_id) {
+    if (!ctx) return HP_ERR_INVALID_ARG;
+    if (!data || !image_id) return fail(ctx, HP_ERR_INVALID_ARG, "image_upload: null pointer");
+    if (width < 2 || height < 2 || width > 32768 || height > 32768)
+        return fail(ctx, HP_ERR_INVALID_ARG, "image_upload: size %dx%d outside 2..32768", width, height);
+    if (dtype != HP_DTYPE_U8 && dtype != HP_DTYPE_F16 && dtype != HP_DTYPE_F32)
+        return fail(ctx, HP_ERR_INVALID_ARG, "image_upload: unknown dtype %d", dtype);
+    if (memory != HP_MEMORY_HOST && memory != HP_MEMORY_DEVICE)
+        return fail(ctx, HP_ERR_INVALID_ARG, "image_upload: unknown memory kind %d", memory);
+    DeviceGuard g(ctx->device);
+    const size_t esz = dtype == HP_DTYPE_U8 ? 1 : (dtype == HP_DTYPE_F16 ? 2 : 4);
+    const size_t bytes = static_cast<size_t>(width) * height * esz;
+    Image im;
+    im.W = width;
+    im.H = height;
+    void* raw = nullptr;
+    auto cleanup = [&]() {
+        if (raw && memory == HP_MEMORY_HOST) cudaFree(raw);
+        free_image(im);
+    };
+    cudaError_t e;
+#define HP_UP(call)                                                                                   \
+    do {                                                                                              \
+        e = (call);                                                                                   \
+        if (e != cudaSuccess) {                                                                       \
+            cleanup();                                                                                \
+            return fail(ctx, e == cudaErrorMemoryAllocation ? HP_ERR_OUT_OF_MEMORY : HP_ERR_CUDA,      \
+                        "image_upload: %s: %s", #call, cudaGetErrorString(e));                        \
+        }                                                                                             \
+    } while (0)
+    const void* src = data;
+    if (memory == HP_MEMORY_HOST) {
+        HP_UP(cudaMalloc(&raw, bytes));
+        HP_UP(cudaMemcpyAsync(raw, data, bytes, cudaMemcpyHostToDevice, ctx->stream));
+        src = raw;
+    }
+    HP_UP(cudaMallocPitch(reinterpret_cast<void**>(&im.f32), &im.pitch32, width * sizeof(float), height));
+    HP_UP(cudaMallocPitch(reinterpret_cast<void**>(&im.f16), &im.pitch16, width * sizeof(__half), height));
+    HP_UP(hp::launch_to_f32(src, dtype, width, height, im.f32, static_cast<int>(im.pitch32 / sizeof(float)), im.f16,
+                            static_cast<int>(im.pitch16 / sizeof(__half)), ctx->stream));
+    cudaChannelFormatDesc d32 = cudaCreateChannelDesc<float>();
+    cudaChannelFormatDesc d16 = cudaCreateChannelDescHalf();
+    HP_UP(cudaMallocArray(&im.arr32, &d32, width, height));
+    HP_UP(cudaMallocArray(&im.arr16, &d16, width, height));
+    HP_UP(cudaMemcpy2DToArrayAsync(im.arr32, 0, 0, im.f32, im.pitch32, width * sizeof(float), height,
+                                   cudaMemcpyDeviceToDevice, ctx->stream));
+    HP_UP(cudaMemcpy2DToArrayAsync(im.arr16, 0, 0, im.f16, im.pitch16, width * sizeof(__half), height,
+                                   cudaMemcpyDeviceToDevice, ctx->stream));
+    HP_UP(make_linear_texture(im.arr32, &im.tex32));
+    HP_UP(make_linear_texture(im.arr16, &im.tex16));
+    HP_UP(cudaStreamSynchronize(ctx->stream));
+#undef HP_UP
+    if (raw && memory == HP_MEMORY_HOST) cudaFree(raw);
+    int id = ctx->next_id++;
+    ctx->images[id] = im;
+    *image_id = id;
+    return HP_OK;
+}
+
+hp_status hp_image_release(hp_ctx* ctx, int image_id) {
+    if (!ctx) return HP_ERR_INVALID_ARG;
+    auto it = ctx->images.find(image_id);
+    if (it == ctx->images.end()) return fail(ctx, HP_ERR_NOT_FOUND, "image_release: unknown image %d", image_id);
+    DeviceGuard g(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    free_image(it->second);
+    ctx->images.erase(it);
+    return HP_OK;
+}
+
+hp_status hp_image_size(hp_ctx* ctx, int image_id, int* width, int* height) {
+    if (!ctx || !width || !height) return HP_ERR_INVALID_ARG;
+    auto it = ctx->images.find(image_id);
+    if (it == ctx->images.end()) return fail(ctx, HP_ERR_NOT_FOUND, "image_size: unknown image %d", image_id);
+    *width = it->second.W;
+    *height = it->second.H;
+    return HP_OK;
+}
+
+hp_status hp_setup_homographies(const hp_camera* ref, const hp_camera* srcs, int num_sources, double* kinv9,
+                                double* ab) {
+    if (!ref || !kinv9 || num_sources < 0 || num_sources > HP_MAX_SOURCES || (num_sources > 0 && (!srcs || !ab)))
+        return HP_ERR_INVALID_ARG;
+    if (!mat3_inv(ref->K, kinv9)) return HP_ERR_INVALID_ARG;
+    double RrT[9];
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) RrT[3 * r + c] = ref->R[3 * c + r];
+    for (int s = 0; s < num_sources; ++s) {
+        const hp_camera& cs = srcs[s];
+        double Rrel[9], tmp[9], A[9], trel[3];
+        mat3_mul(cs.R, RrT, Rrel);  // R_rel = R_s R_ref^T
+        for (int r = 0; r < 3; ++r)
+            trel[r] = cs.t[r] - (Rrel[3 * r] * ref->t[0] + Rrel[3 * r + 1] * ref->t[1] + Rrel[3 * r + 2] * ref->t[2]);
+        mat3_mul(Rrel, kinv9, tmp);
+        mat3_mul(cs.K, tmp, A);  // A = K_s R_rel K_ref^-1
+        double* o = ab + 12 * s;
+        std::memcpy(o, A, sizeof A);
+        for (int r = 0; r < 3; ++r) o[9 + r] = cs.K[3 * r] * trel[0] + cs.K[3 * r + 1] * trel[1] + cs.K[3 * r + 2] * trel[2];
+    }
+    return HP_OK;
+}
+
+hp_status hp_solve(hp_ctx* ctx, const hp_job* jobs, int num_jobs, const hp_params* params, hp_maps* out) {
+    if (!ctx) return HP_ERR_INVALID_ARG;
+    if (!jobs || !out || num_jobs < 1) return fail(ctx, HP_ERR_INVALID_ARG, "solve: no jobs or outputs");
+    hp_status st = check_params(ctx, params);
+    if (st != HP_OK) return st;
+    for (int k = 0; k < num_jobs; ++k)
+        if (!out[k].depth || !out[k].normal || !out[k].cost)
+            return fail(ctx, HP_ERR_INVALID_ARG, "solve: output maps of job %d incomplete", k);
+    DeviceGuard g(ctx->device);
+    Prepared P;
+    if ((st = prepare(ctx, jobs, num_jobs, &P)) != HP_OK) return st;
+    hp::BatchList all = batch_of(P, 0);
+    HP_CUDA(hp::launch_init(all, ctx->stream));
+    if ((st = launch_cost(ctx, all, params)) != HP_OK) return st;
+    for (int it = 0; it < P.max_iter; ++it) {
+        hp::BatchList bl = batch_of(P, 1 + it);
+        if ((st = launch_pass(ctx, bl, params, it, 0)) != HP_OK) return st;
+        if ((st = launch_pass(ctx, bl, params, it, 1)) != HP_OK) return st;
+    }
+    for (int k = 0; k < num_jobs; ++k)
+        if ((st = export_maps(ctx, P, k, &out[k], true, true)) != HP_OK) return st;
+    HP_CUDA(cudaStreamSynchronize(ctx->stream));
+    return HP_OK;
+}
+
+hp_status hp_init_hypotheses(hp_ctx* ctx, const hp_job* job, const hp_params* params, hp_maps* out) {
+    if (!ctx) return HP_ERR_INVALID_ARG;
+    if (!job || !out || !out->depth || !out->normal) return fail(ctx, HP_ERR_INVALID_ARG, "init: null argument");
+    hp_status st = check_params(ctx, params);
+    if (st != HP_OK) return st;
+    DeviceGuard g(ctx->device);
+    Prepared P;
+    if ((st = prepare(ctx, job, 1, &P)) != HP_OK) return st;
+    HP_CUDA(hp::launch_init(batch_of(P, 0), ctx->stream));
+    if ((st = export_maps(ctx, P, 0, out, true, false)) != HP_OK) return st;
+    HP_CUDA(cudaStreamSynchronize(ctx->stream));
+    return HP_OK;
+}
+
+hp_status hp_ncc_cost(hp_ctx* ctx, const hp_job* job, const hp_params* params, hp_maps* maps) {
+    if (!ctx) return HP_ERR_INVALID_ARG;
+    if (!job || !maps || !maps->cost) return fail(ctx, HP_ERR_INVALID_ARG, "ncc_cost: null argument");
+    hp_status st = check_params(ctx, params);
+    if (st != HP_OK) return st;
+    DeviceGuard g(ctx->device);
+    Prepared P;
+    if ((st = prepare(ctx, job, 1, &P)) != HP_OK) return st;
+    if ((st = import_maps(ctx, P, 0, maps, false)) != HP_OK) return st;
+    if ((st = launch_cost(ctx, batch_of(P, 0), params)) != HP_OK) return st;
+    if ((st = export_maps(ctx, P, 0, maps, false, true)) != HP_OK) return st;
+    HP_CUDA(cudaStreamSynchronize(ctx->stream));
+    return HP_OK;
+}
+
+hp_status hp_propagate_pass(hp_ctx* ctx, const hp_job* job, const hp_params* params, hp_maps* maps, int iteration,
+                            int color) {
+    if (!ctx) return HP_ERR_INVALID_ARG;
+    if (!job || !maps) return fail(ctx, HP_ERR_INVALID_ARG, "propagate_pass: null argument");
+    if (color != 0 && color != 1) return fail(ctx, HP_ERR_INVALID_ARG, "propagate_pass: color %d not 0/1", color);
+    if (iteration < 0) return fail(ctx, HP_ERR_INVALID_ARG, "propagate_pass: negative iteration");
+    hp_status st = check_params(ctx, params);
+    if (st != HP_OK) return st;
+    DeviceGuard g(ctx->device);
+    Prepared P;
+    if ((st = prepare(ctx, job, 1, &P)) != HP_OK) return st;
+    if ((st = import_maps(ctx, P, 0, maps, true)) != HP_OK) return st;
+    if ((st = launch_pass(ctx, batch_of(P, 0), params, iteration, color)) != HP_OK) return st;
+    if ((st = export_maps(ctx, P, 0, maps, true, true)) != HP_OK) return st;
+    HP_CUDA(cudaStreamSynchronize(ctx->stream));
+    return HP_OK;
+}
+
+hp_status hp_geometric_filter(hp_ctx* ctx, const hp_camera* ref_cam, int width, int height, float* depth,
+                              const float* normal, float* confidence, int num_sources, const hp_camera* src_cams,
+                              const float* const* src_depths, const float* const* src_normals, int memory,
+                              float depth_tol, float normal_tol_cos, int min_consistent) {
+    if (!ctx) return HP_ERR_INVALID_ARG;
+    if (!ref_cam || !depth || !normal || !confidence || (num_sources > 0 && (!src_cams || !src_depths || !src_normals)))
+        return fail(ctx, HP_ERR_INVALID_ARG, "geometric_filter: null argument");
+    if (num_sources < 0 || num_sources > HP_MAX_SOURCES)
+        return fail(ctx, HP_ERR_INVALID_ARG, "geometric_filter: num_sources %d outside 0..%d", num_sources,
+                    HP_MAX_SOURCES);
+    if (width < 1 || height < 1) return fail(ctx, HP_ERR_INVALID_ARG, "geometric_filter: empty map");
+    DeviceGuard g(ctx->device);
+    hp::FilterArgs a;
+    std::memset(&a, 0, sizeof a);
+    double kinv[9];
+    if (!mat3_inv(ref_cam->K, kinv)) return fail(ctx, HP_ERR_INVALID_ARG, "geometric_filter: singular K");
+    for (int i = 0; i < 9; ++i) {
+        a.ref_kinv[i] = static_cast<float>(kinv[i]);
+        a.ref_R[i] = static_cast<float>(ref_cam->R[i]);
+    }
+    for (int i = 0; i < 3; ++i) a.ref_t[i] = static_cast<float>(ref_cam->t[i]);
+    for (int s = 0; s < num_sources; ++s) {
+        for (int i = 0; i < 9; ++i) {
+            a.src[s].K[i] = static_cast<float>(src_cams[s].K[i]);
+            a.src[s].R[i] = static_cast<float>(src_cams[s].R[i]);
+        }
+        for (int i = 0; i < 3; ++i) a.src[s].t[i] = static_cast<float>(src_cams[s].t[i]);
+    }
+    a.S = num_sources;
+    a.W = width;
+    a.H = height;
+    a.depth_tol = depth_tol;
+    a.normal_tol_cos = normal_tol_cos;
+    a.min_consistent = min_consistent;
+    const size_t px = static_cast<size_t>(width) * height;
+    if (memory == HP_MEMORY_DEVICE) {
+        for (int s = 0; s < num_sources; ++s) {
+            a.src_depth[s] = src_depths[s];
+            a.src_normal[s] = src_normals[s];
+        }
+        HP_CUDA(hp::launch_geometric_filter(a, depth, normal, confidence, ctx->stream));
+        HP_CUDA(cudaStreamSynchronize(ctx->stream));
+        return HP_OK;
+    }
+    // Host maps: stage ref (depth, normal, conf) and every source map once.
+    const size_t need = px * (5 + 4 * static_cast<size_t>(num_sources)) * sizeof(float);
+    HP_CUDA(ctx->staging.ensure(need));
+    float* sd = static_cast<float*>(ctx->staging.p);
+    float* sn = sd + px;
+    float* sc = sn + 3 * px;
+    float* srcbase = sc + px;
+    HP_CUDA(cudaMemcpyAsync(sd, depth, px * 4, cudaMemcpyHostToDevice, ctx->stream));
+    HP_CUDA(cudaMemcpyAsync(sn, normal, 3 * px * 4, cudaMemcpyHostToDevice, ctx->stream));
+    HP_CUDA(cudaMemcpyAsync(sc, confidence, px * 4, cudaMemcpyHostToDevice, ctx->stream));
+    for (int s = 0; s < num_sources; ++s) {
+        float* dd = srcbase + static_cast<size_t>(s) * 4 * px;
+        HP_CUDA(cudaMemcpyAsync(dd, src_depths[s], px * 4, cudaMemcpyHostToDevice, ctx->stream));
+        HP_CUDA(cudaMemcpyAsync(dd + px, src_normals[s], 3 * px * 4, cudaMemcpyHostToDevice, ctx->stream));
+        a.src_depth[s] = dd;
+        a.src_normal[s] = dd + px;
+    }
+    HP_CUDA(hp::launch_geometric_filter(a, sd, sn, sc, ctx->stream));
+    HP_CUDA(cudaMemcpyAsync(depth, sd, px * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    HP_CUDA(cudaMemcpyAsync(confidence, sc, px * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    HP_CUDA(cudaStreamSynchronize(ctx->stream));
+    return HP_OK;
+}
+
+}  // extern "C"

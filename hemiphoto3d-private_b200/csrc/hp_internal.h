@@ -1,0 +1,90 @@
+// Internal types shared by the engine's host code and kernels.
+#pragma once
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/hpmvs.h"
+
+namespace hp {
+
+// Pixel tile one CTA covers: TILE_W x TILE_H pixels, 256 threads.  In a
+// red-black half-pass each thread owns one pixel of the active color (a warp
+// covers one 64-pixel row segment); the full-map kernels give each thread the
+// two horizontally adjacent pixels of its pair.
+constexpr int TILE_W = 64;
+constexpr int TILE_H = 8;
+constexpr int CTA_THREADS = 256;
+
+// Per-view descriptor, resident in device memory for the duration of a solve.
+// Hypotheses are packed (depth, nx, ny, nz) so one 16-byte load fetches a
+// pixel's plane; cost is a separate float plane.
+struct ViewDesc {
+    const float* ref;                 // FP32 reference image, row pitch ref_pitch floats
+    const __half* ref16;              // FP16 reference image, row pitch ref16_pitch halves
+    cudaTextureObject_t src_tex[HP_MAX_SOURCES];    // FP32 sources, linear filter
+    cudaTextureObject_t src_tex16[HP_MAX_SOURCES];  // FP16 sources, linear filter
+    float kinv[9];
+    float ab[HP_MAX_SOURCES][12];     // A (9), b (3) per source
+    float4* hyp;                      // H*W
+    float* cost;                      // H*W
+    int ref_pitch, ref16_pitch;
+    int W, H, S;
+    int tiles_x, tiles_y;
+    float dmin, dmax;
+    uint32_t seed_lo, seed_hi, view_id;
+    int iterations;
+};
+
+// Solver constants for one launch.
+struct SolveConsts {
+    int radius, stride, top_k, refine_steps;
+    float iter_decay, step_decay;
+};
+
+// A batch launch covers the tiles of several views: view k owns flattened
+// tile indices [tile_prefix[k], tile_prefix[k+1]).
+struct BatchList {
+    const ViewDesc* views;      // all views of the solve
+    const int* active;          // indices of the views in this launch
+    const int* tile_prefix;     // n_active + 1 entries
+    int n_active;
+    int total_tiles;
+};
+
+// Geometric-filter launch arguments: FP32 cameras (cast from FP64 like the
+// reference's eigenToGPUCamera) and one depth / AoS-normal pointer per source.
+struct FilterCam {
+    float K[9], R[9], t[3];
+};
+struct FilterArgs {
+    float ref_kinv[9], ref_R[9], ref_t[3];
+    FilterCam src[HP_MAX_SOURCES];
+    const float* src_depth[HP_MAX_SOURCES];
+    const float* src_normal[HP_MAX_SOURCES];
+    int S, W, H;
+    float depth_tol, normal_tol_cos;
+    int min_consistent;
+};
+
+}  // namespace hp
+
+// Kernel launchers (defined in the .cu files), all on the given stream.
+namespace hp {
+cudaError_t launch_init(const BatchList& bl, cudaStream_t st);
+cudaError_t launch_cost_f32(const BatchList& bl, const SolveConsts& sc, cudaStream_t st);
+cudaError_t launch_propagate_f32(const BatchList& bl, const SolveConsts& sc, int iteration, int color,
+                                 cudaStream_t st);
+cudaError_t launch_cost_f16(const BatchList& bl, const SolveConsts& sc, cudaStream_t st);
+cudaError_t launch_propagate_f16(const BatchList& bl, const SolveConsts& sc, int iteration, int color,
+                                 cudaStream_t st);
+cudaError_t launch_unpack(const ViewDesc* views_host_copy, int view, float* depth, float* normal, float* cost,
+                          cudaStream_t st);
+cudaError_t launch_pack(const ViewDesc* views_host_copy, int view, const float* depth, const float* normal,
+                        const float* cost, cudaStream_t st);
+cudaError_t launch_geometric_filter(const FilterArgs& a, float* depth, const float* normal, float* conf,
+                                    cudaStream_t st);
+cudaError_t launch_to_f32(const void* src, int dtype, int W, int H, float* dst, int dst_pitch, __half* dst16,
+                          int dst16_pitch, cudaStream_t st);
+}  // namespace hp

@@ -1,0 +1,415 @@
+// FP16-storage / FP32-accumulate PatchMatch kernels for sm_100a.
+//
+// Same algorithm as the FP32 path (init is shared; cost, propagation and
+// refinement follow src/dense_recon/patchmatch_mvs.cu:222-343 and :519-655),
+// re-derived for throughput:
+//  - Sources are FP16 textures (half the texel bytes of FP32); the hardware
+//    linear filter returns FP32.
+//  - Per (candidate, source) the plane-induced homography is folded into one
+//    3x3 H = A + b (K^-T n)^T / (n.P), with the +0.5 texel-centre offset folded
+//    into its first two rows; taps then step w += s*H[:,0] along a row: three
+//    adds, one reciprocal and two multiplies per tap instead of ~25 operations.
+//  - If the warped window's four corners lie inside the valid source region
+//    (the warp of a rectangle with one-signed depth is the convex quad of its
+//    corners) every tap is valid and the per-tap bounds tests are skipped.
+//  - The reference window is mean-subtracted per pixel once per visit and,
+//    for windows of up to 64 taps, held in registers as half2 pairs.  Window
+//    sums use mean-shifted values (compensated variance): FP16 products and
+//    per-row FP16 partial sums, flushed into FP32 accumulators every row.
+//  - Windows touching the source border take a checked FP32 path with the
+//    reference's validity rules (|w_z| >= 1e-8, u in [0, W-1), v in [0, H-1),
+//    count >= taps/2) on mean-shifted sums.
+#include <cuda_fp16.h>
+
+#include "hp_internal.h"
+#include "hp_rng.cuh"
+
+namespace hp {
+
+namespace {
+
+constexpr int MAX_TW = TILE_W + 2 * HP_MAX_RADIUS;
+constexpr int MAX_TH = TILE_H + 2 * HP_MAX_RADIUS;
+
+__device__ __forceinline__ const ViewDesc* locate_tile16(const BatchList& bl, int t, int* tx, int* ty) {
+    int lo = 0, hi = bl.n_active - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (bl.tile_prefix[mid] <= t) lo = mid; else hi = mid - 1;
+    }
+    const ViewDesc* v = &bl.views[bl.active[lo]];
+    int local = t - bl.tile_prefix[lo];
+    *tx = local % v->tiles_x;
+    *ty = local / v->tiles_x;
+    return v;
+}
+
+__device__ __forceinline__ void load_ref_tile16(float* s_ref, int tw, int th, const ViewDesc* v, int x0, int y0,
+                                                int r) {
+    const int W = v->W, H = v->H;
+    for (int i = threadIdx.x; i < tw * th; i += CTA_THREADS) {
+        int ty = i / tw, tx = i - ty * tw;
+        int gx = min(max(x0 - r + tx, 0), W - 1);
+        int gy = min(max(y0 - r + ty, 0), H - 1);
+        s_ref[i] = __half2float(v->ref16[static_cast<size_t>(gy) * v->ref16_pitch + gx]);
+    }
+}
+
+// Per-pixel reference window, mean-subtracted.
+template <int R, int ST>
+struct RefWindow {
+    static constexpr int SIDE = (2 * R) / ST + 1;
+    static constexpr int N = SIDE * SIDE;
+    static constexpr int PAIRS = (SIDE + 1) / 2;          // half2 per row (last may be half-empty)
+    static constexpr bool IN_REGS = SIDE * PAIRS <= 32;
+    __half2 q[IN_REGS ? SIDE * PAIRS : 1];
+    float mean;     // window mean
+    float ssd;      // sum (r - mean)^2
+};
+
+template <int R, int ST>
+__device__ __forceinline__ void load_window(RefWindow<R, ST>& w, const float* s_ref, int tw, int lx, int ly) {
+    constexpr int SIDE = RefWindow<R, ST>::SIDE;
+    float sum = 0.f;
+#pragma unroll
+    for (int i = 0; i < SIDE; ++i)
+#pragma unroll
+        for (int j = 0; j < SIDE; ++j) sum += s_ref[(ly + i * ST) * tw + lx + j * ST];
+    const float mean = sum * (1.0f / RefWindow<R, ST>::N);
+    float ssd = 0.f;
+#pragma unroll
+    for (int i = 0; i < SIDE; ++i)
+#pragma unroll
+        for (int j = 0; j < SIDE; ++j) {
+            const float d = s_ref[(ly + i * ST) * tw + lx + j * ST] - mean;
+            ssd = fmaf(d, d, ssd);
+        }
+    w.mean = mean;
+    w.ssd = ssd;
+    if constexpr (RefWindow<R, ST>::IN_REGS) {
+        constexpr int PAIRS = RefWindow<R, ST>::PAIRS;
+#pragma unroll
+        for (int i = 0; i < SIDE; ++i)
+#pragma unroll
+            for (int p = 0; p < PAIRS; ++p) {
+                const float a = s_ref[(ly + i * ST) * tw + lx + (2 * p) * ST] - mean;
+                const float b = (2 * p + 1 < SIDE) ? s_ref[(ly + i * ST) * tw + lx + (2 * p + 1) * ST] - mean : 0.f;
+                w.q[i * PAIRS + p] = __floats2half2_rn(a, b);
+            }
+    }
+}
+
+// Approximate reciprocal (PTX rcp.approx.ftz.f32, ~1 ulp): the warped-coordinate
+// divide of the fast path.
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+struct Plane {
+    float h[9];  // homography with the +0.5 texel offset folded into rows 0, 1
+};
+
+// Checked FP32 evaluation of one source (border windows): reference validity
+// rules, mean-shifted sums.  Returns the source cost (1 - NCC or 2).
+template <int R, int ST>
+__device__ float source_cost_checked(const Plane& P, cudaTextureObject_t tex, const RefWindow<R, ST>& w,
+                                     const float* s_ref, int tw, int lx, int ly, int x, int y, float fW, float fH) {
+    constexpr int SIDE = RefWindow<R, ST>::SIDE;
+    float sr = 0.f, ss = 0.f, srr = 0.f, sss = 0.f, srs = 0.f;
+    int count = 0;
+    const float c0 = w.mean;
+    for (int i = 0; i < SIDE; ++i) {
+        const float py = static_cast<float>(y - R + i * ST);
+        for (int j = 0; j < SIDE; ++j) {
+            const float px = static_cast<float>(x - R + j * ST);
+            const float wz = fmaf(P.h[6], px, fmaf(P.h[7], py, P.h[8]));
+            if (fabsf(wz) < 1e-8f) continue;
+            const float iz = __frcp_rn(wz);
+            const float u = fmaf(P.h[0], px, fmaf(P.h[1], py, P.h[2])) * iz;  // = u_ref + 0.5
+            const float v = fmaf(P.h[3], px, fmaf(P.h[4], py, P.h[5])) * iz;
+            if (u < 0.5f || u >= fW - 0.5f || v < 0.5f || v >= fH - 0.5f) continue;
+            const float sv = tex2D<float>(tex, u, v) - c0;
+            const float rv = s_ref[(ly + i * ST) * tw + lx + j * ST] - c0;
+            sr += rv;
+            ss += sv;
+            srr = fmaf(rv, rv, srr);
+            sss = fmaf(sv, sv, sss);
+            srs = fmaf(rv, sv, srs);
+            ++count;
+        }
+    }
+    if (count < RefWindow<R, ST>::N / 2) return 2.0f;
+    const float n = static_cast<float>(count);
+    const float num = fmaf(n, srs, -sr * ss);
+    const float dr = fmaf(n, srr, -sr * sr);
+    const float ds = fmaf(n, sss, -ss * ss);
+    if (dr < 1e-6f || ds < 1e-6f) return 2.0f;
+    const float ncc = fmaxf(-1.0f, fminf(1.0f, num * rsqrtf(dr) * rsqrtf(ds)));
+    return 1.0f - ncc;
+}
+
+// Fast path: all taps valid.  Sums of e = s - mean and products (r - mean) e
+// in FP16 per row, flushed to FP32.
+template <int R, int ST>
+__device__ __forceinline__ float source_cost_fast(const Plane& P, cudaTextureObject_t tex, const RefWindow<R, ST>& w,
+                                                  const float* s_ref, int tw, int lx, int ly, int x, int y) {
+    constexpr int SIDE = RefWindow<R, ST>::SIDE;
+    constexpr int PAIRS = RefWindow<R, ST>::PAIRS;
+    const float c0 = w.mean;
+    const __half2 c0h = __float2half2_rn(c0);
+    float s1 = 0.f, s2 = 0.f, s3 = 0.f;
+    const float sx0 = static_cast<float>(x - R), sy0 = static_cast<float>(y - R);
+    const float hx0 = P.h[0] * ST, hx1 = P.h[3] * ST, hx2 = P.h[6] * ST;
+#pragma unroll
+    for (int i = 0; i < SIDE; ++i) {
+        const float py = sy0 + static_cast<float>(i * ST);
+        float wx = fmaf(P.h[0], sx0, fmaf(P.h[1], py, P.h[2]));
+        float wy = fmaf(P.h[3], sx0, fmaf(P.h[4], py, P.h[5]));
+        float wz = fmaf(P.h[6], sx0, fmaf(P.h[7], py, P.h[8]));
+        __half2 a1 = __float2half2_rn(0.f), a2 = a1, a3 = a1;
+#pragma unroll
+        for (int p = 0; p < PAIRS; ++p) {
+            float iz = rcp_approx(wz);
+            const float sa = tex2D<float>(tex, wx * iz, wy * iz);
+            wx += hx0; wy += hx1; wz += hx2;
+            float sb = 0.f;
+            if (2 * p + 1 < SIDE) {
+                iz = rcp_approx(wz);
+                sb = tex2D<float>(tex, wx * iz, wy * iz);
+                wx += hx0; wy += hx1; wz += hx2;
+            }
+            __half2 e = __hsub2(__floats2half2_rn(sa, sb), c0h);
+            if (2 * p + 1 >= SIDE) e = __halves2half2(__low2half(e), __float2half_rn(0.f));
+            __half2 rq;
+            if constexpr (RefWindow<R, ST>::IN_REGS) {
+                rq = w.q[i * PAIRS + p];
+            } else {
+                const float ra = s_ref[(ly + i * ST) * tw + lx + (2 * p) * ST] - c0;
+                const float rb = (2 * p + 1 < SIDE) ? s_ref[(ly + i * ST) * tw + lx + (2 * p + 1) * ST] - c0 : 0.f;
+                rq = __floats2half2_rn(ra, rb);
+            }
+            a1 = __hadd2(a1, e);
+            a2 = __hfma2(e, e, a2);
+            a3 = __hfma2(rq, e, a3);
+        }
+        const float2 f1 = __half22float2(a1), f2 = __half22float2(a2), f3 = __half22float2(a3);
+        s1 += f1.x + f1.y;
+        s2 += f2.x + f2.y;
+        s3 += f3.x + f3.y;
+    }
+    constexpr float n = static_cast<float>(RefWindow<R, ST>::N);
+    // n*sum(r^2)-sum(r)^2 = n*ssd, n*sum(s^2)-sum(s)^2 = n*s2 - s1^2, cov numerator n*s3 (sum(r - mean) = 0).
+    const float dr = n * w.ssd;
+    const float ds = fmaf(n, s2, -s1 * s1);
+    if (dr < 1e-6f || ds < 1e-6f) return 2.0f;
+    const float ncc = fmaxf(-1.0f, fminf(1.0f, n * s3 * rsqrtf(dr) * rsqrtf(ds)));
+    return 1.0f - ncc;
+}
+
+template <int R, int ST>
+__device__ __forceinline__ float cost_f16(const RefWindow<R, ST>& w, const float* s_ref, int tw, int lx, int ly,
+                                          int x, int y, float d, float cnx, float cny, float cnz,
+                                          const ViewDesc* __restrict__ v, int topk) {
+    const float* k = v->kinv;
+    const float fx = static_cast<float>(x), fy = static_cast<float>(y);
+    const float Px = d * fmaf(k[0], fx, fmaf(k[1], fy, k[2]));
+    const float Py = d * fmaf(k[3], fx, fmaf(k[4], fy, k[5]));
+    const float Pz = d * fmaf(k[6], fx, fmaf(k[7], fy, k[8]));
+    const float ndp = fmaf(cnx, Px, fmaf(cny, Py, cnz * Pz));
+    if (fabsf(ndp) < 1e-8f) return 2.0f;
+    const float ind = __frcp_rn(ndp);
+    const float m0 = fmaf(k[0], cnx, fmaf(k[3], cny, k[6] * cnz)) * ind;
+    const float m1 = fmaf(k[1], cnx, fmaf(k[4], cny, k[7] * cnz)) * ind;
+    const float m2 = fmaf(k[2], cnx, fmaf(k[5], cny, k[8] * cnz)) * ind;
+    const float fW = static_cast<float>(v->W), fH = static_cast<float>(v->H);
+    const float xa = static_cast<float>(x - R), xb = static_cast<float>(x - R + (RefWindow<R, ST>::SIDE - 1) * ST);
+    const float ya = static_cast<float>(y - R), yb = static_cast<float>(y - R + (RefWindow<R, ST>::SIDE - 1) * ST);
+    float top0 = 2.0f, top1 = 2.0f, top2 = 2.0f;
+    const int S = v->S;
+    for (int s = 0; s < S; ++s) {
+        const float* A = v->ab[s];
+        Plane P;
+        P.h[6] = fmaf(A[11], m0, A[6]);
+        P.h[7] = fmaf(A[11], m1, A[7]);
+        P.h[8] = fmaf(A[11], m2, A[8]);
+        P.h[0] = fmaf(0.5f, P.h[6], fmaf(A[9], m0, A[0]));
+        P.h[1] = fmaf(0.5f, P.h[7], fmaf(A[9], m1, A[1]));
+        P.h[2] = fmaf(0.5f, P.h[8], fmaf(A[9], m2, A[2]));
+        P.h[3] = fmaf(0.5f, P.h[6], fmaf(A[10], m0, A[3]));
+        P.h[4] = fmaf(0.5f, P.h[7], fmaf(A[10], m1, A[4]));
+        P.h[5] = fmaf(0.5f, P.h[8], fmaf(A[10], m2, A[5]));
+        // Corner test (margin 1e-3 px): one-signed depth and all four corners inside.
+        bool inside = true;
+        float zsign = 0.f;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const float px = (c & 1) ? xb : xa, py = (c & 2) ? yb : ya;
+            const float wz = fmaf(P.h[6], px, fmaf(P.h[7], py, P.h[8]));
+            const float u = fmaf(P.h[0], px, fmaf(P.h[1], py, P.h[2])) / wz;
+            const float vv = fmaf(P.h[3], px, fmaf(P.h[4], py, P.h[5])) / wz;
+            if (c == 0) zsign = wz;
+            inside = inside && (fabsf(wz) > 1e-6f) && (wz * zsign > 0.f) && u >= 0.501f && u < fW - 0.501f &&
+                     vv >= 0.501f && vv < fH - 0.501f;
+        }
+        const cudaTextureObject_t tex = v->src_tex16[s];
+        const float c = inside ? source_cost_fast<R, ST>(P, tex, w, s_ref, tw, lx, ly, x, y)
+                               : source_cost_checked<R, ST>(P, tex, w, s_ref, tw, lx, ly, x, y, fW, fH);
+        if (c < top2) {
+            top2 = c;
+            if (top2 < top1) {
+                float t = top1; top1 = top2; top2 = t;
+                if (top1 < top0) { t = top0; top0 = top1; top1 = t; }
+            }
+        }
+    }
+    const int kk = min(topk, S);
+    float sum = top0;
+    if (kk > 1) sum += top1;
+    if (kk > 2) sum += top2;
+    return sum / static_cast<float>(kk);
+}
+
+__device__ __forceinline__ bool same_plane16(float4 a, float4 b) {
+    return __float_as_uint(a.x) == __float_as_uint(b.x) && __float_as_uint(a.y) == __float_as_uint(b.y) &&
+           __float_as_uint(a.z) == __float_as_uint(b.z) && __float_as_uint(a.w) == __float_as_uint(b.w);
+}
+
+template <int R, int ST>
+__global__ void __launch_bounds__(CTA_THREADS) cost16_kernel(BatchList bl, SolveConsts sc) {
+    __shared__ float s_ref[MAX_TW * MAX_TH];
+    int tile_x, tile_y;
+    const ViewDesc* v = locate_tile16(bl, blockIdx.x, &tile_x, &tile_y);
+    const int tw = TILE_W + 2 * R, th = TILE_H + 2 * R;
+    const int x0 = tile_x * TILE_W, y0 = tile_y * TILE_H;
+    load_ref_tile16(s_ref, tw, th, v, x0, y0, R);
+    __syncthreads();
+    const int ly = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int y = y0 + ly;
+    if (y >= v->H) return;
+    for (int j = 0; j < 2; ++j) {
+        const int lx = 2 * lane + j, x = x0 + lx;
+        if (x >= v->W) continue;
+        RefWindow<R, ST> w;
+        load_window<R, ST>(w, s_ref, tw, lx, ly);
+        const size_t idx = static_cast<size_t>(y) * v->W + x;
+        const float4 h = v->hyp[idx];
+        v->cost[idx] = cost_f16<R, ST>(w, s_ref, tw, lx, ly, x, y, h.x, h.y, h.z, h.w, v, sc.top_k);
+    }
+}
+
+template <int R, int ST>
+__global__ void __launch_bounds__(CTA_THREADS) propagate16_kernel(BatchList bl, SolveConsts sc, int iteration,
+                                                                  int color) {
+    __shared__ float s_ref[MAX_TW * MAX_TH];
+    int tile_x, tile_y;
+    const ViewDesc* v = locate_tile16(bl, blockIdx.x, &tile_x, &tile_y);
+    const int tw = TILE_W + 2 * R, th = TILE_H + 2 * R;
+    const int x0 = tile_x * TILE_W, y0 = tile_y * TILE_H;
+    load_ref_tile16(s_ref, tw, th, v, x0, y0, R);
+    __syncthreads();
+    const int W = v->W, H = v->H;
+    const int ly = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int y = y0 + ly;
+    const int lx = 2 * lane + ((y + color) & 1);
+    const int x = x0 + lx;
+    if (y >= H || x >= W) return;
+    const size_t idx = static_cast<size_t>(y) * W + x;
+    const float dmin = v->dmin, dmax = v->dmax;
+    RefWindow<R, ST> w;
+    load_window<R, ST>(w, s_ref, tw, lx, ly);
+
+    float4 best = v->hyp[idx];
+    float best_cost = v->cost[idx];
+    const float3 ray = view_ray(v->kinv, x, y);
+    float drange = __fmul_rn(__fsub_rn(dmax, dmin), 0.5f);
+    float nrange = 1.0f;
+    for (int i = 0; i < iteration; ++i) {
+        drange = __fmul_rn(drange, sc.iter_decay);
+        nrange = __fmul_rn(nrange, sc.iter_decay);
+    }
+    float4 tried[4];
+    int n_tried = 0;
+    // Candidates 0..3: neighbours L, R, U, D; then refine_steps perturbations.
+    const int n_cand = 4 + sc.refine_steps;
+    for (int cand = 0; cand < n_cand; ++cand) {
+        float4 h;
+        if (cand < 4) {
+            const int nxp = x + (cand == 0 ? -1 : (cand == 1 ? 1 : 0));
+            const int nyp = y + (cand == 2 ? -1 : (cand == 3 ? 1 : 0));
+            if (nxp < 0 || nxp >= W || nyp < 0 || nyp >= H) continue;
+            h = v->hyp[static_cast<size_t>(nyp) * W + nxp];
+            if (h.x < dmin || h.x > dmax) continue;
+            bool dup = same_plane16(h, best);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) dup |= (j < n_tried) && same_plane16(h, tried[j]);
+            if (dup) continue;
+            tried[n_tried++] = h;
+        } else {
+            const int step = cand - 4;
+            const uint4 rr = philox4x32_10(make_uint4(static_cast<uint32_t>(idx), v->view_id,
+                                                      1u + static_cast<uint32_t>(iteration), static_cast<uint32_t>(step)),
+                                           v->seed_lo, v->seed_hi);
+            float cd = __fmaf_rn(__fmaf_rn(u01(rr.x), 2.0f, -1.0f), drange, best.x);
+            cd = fmaxf(dmin, fminf(dmax, cd));
+            const float cx = __fmaf_rn(__fmaf_rn(u01(rr.y), 2.0f, -1.0f), nrange, best.y);
+            const float cy = __fmaf_rn(__fmaf_rn(u01(rr.z), 2.0f, -1.0f), nrange, best.z);
+            const float cz = __fmaf_rn(__fmaf_rn(u01(rr.w), 2.0f, -1.0f), nrange, best.w);
+            float3 cn = normalize3_rn(cx, cy, cz);
+            if (dot3_rn(cn, ray) > 0.0f) cn = make_float3(-cn.x, -cn.y, -cn.z);
+            h = make_float4(cd, cn.x, cn.y, cn.z);
+            drange = __fmul_rn(drange, sc.step_decay);
+            nrange = __fmul_rn(nrange, sc.step_decay);
+        }
+        const float c = cost_f16<R, ST>(w, s_ref, tw, lx, ly, x, y, h.x, h.y, h.z, h.w, v, sc.top_k);
+        if (c < best_cost) {
+            best_cost = c;
+            best = h;
+        }
+    }
+    v->hyp[idx] = best;
+    v->cost[idx] = best_cost;
+}
+
+template <int R, int ST>
+cudaError_t launch_r(const BatchList& bl, const SolveConsts& sc, int iteration, int color, bool full, cudaStream_t st) {
+    if (full)
+        cost16_kernel<R, ST><<<bl.total_tiles, CTA_THREADS, 0, st>>>(bl, sc);
+    else
+        propagate16_kernel<R, ST><<<bl.total_tiles, CTA_THREADS, 0, st>>>(bl, sc, iteration, color);
+    return cudaGetLastError();
+}
+
+cudaError_t dispatch(const BatchList& bl, const SolveConsts& sc, int iteration, int color, bool full,
+                     cudaStream_t st) {
+    if (bl.total_tiles <= 0) return cudaSuccess;
+#define HP_CASE(RR)                                                                       \
+    case RR:                                                                              \
+        return sc.stride == 1 ? launch_r<RR, 1>(bl, sc, iteration, color, full, st)       \
+                              : launch_r<RR, 2>(bl, sc, iteration, color, full, st);
+    switch (sc.radius) {
+        HP_CASE(1)
+        HP_CASE(2)
+        HP_CASE(3)
+        HP_CASE(4)
+        HP_CASE(5)
+        HP_CASE(6)
+        HP_CASE(7)
+        default: return cudaErrorInvalidValue;
+    }
+#undef HP_CASE
+}
+
+}  // namespace
+
+cudaError_t launch_cost_f16(const BatchList& bl, const SolveConsts& sc, cudaStream_t st) {
+    return dispatch(bl, sc, 0, 0, true, st);
+}
+
+cudaError_t launch_propagate_f16(const BatchList& bl, const SolveConsts& sc, int iteration, int color,
+                                 cudaStream_t st) {
+    return dispatch(bl, sc, iteration, color, false, st);
+}
+
+}  // namespace hp

@@ -1,0 +1,95 @@
+// Layout kernels: image conversion on upload and hypothesis (un)packing
+// between the engine's packed float4 planes and the caller's depth / AoS
+// normal / cost maps.  All are HBM-bound streaming kernels: grid-stride loops
+// over a grid sized to the SM count.
+#include "hp_internal.h"
+
+namespace hp {
+
+namespace {
+
+int g_grid_cache = 0;
+int stream_grid() {
+    if (g_grid_cache == 0) {
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        g_grid_cache = sms * 8;
+    }
+    return g_grid_cache;
+}
+
+// u8 / f16 / f32 (tightly packed) -> FP32 and FP16 pitched planes, values in [0, 1].
+__global__ void to_planes_kernel(const void* __restrict__ src, int dtype, int W, int H, float* __restrict__ dst,
+                                 int pitch, __half* __restrict__ dst16, int pitch16) {
+    const size_t n = static_cast<size_t>(W) * H;
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const int y = static_cast<int>(i / W), x = static_cast<int>(i - static_cast<size_t>(y) * W);
+        float v;
+        __half h;
+        if (dtype == HP_DTYPE_U8) {
+            v = __fdiv_rn(static_cast<float>(static_cast<const unsigned char*>(src)[i]), 255.0f);
+            h = __float2half_rn(v);
+        } else if (dtype == HP_DTYPE_F16) {
+            h = static_cast<const __half*>(src)[i];
+            v = __half2float(h);
+        } else {
+            v = static_cast<const float*>(src)[i];
+            h = __float2half_rn(v);
+        }
+        dst[static_cast<size_t>(y) * pitch + x] = v;
+        dst16[static_cast<size_t>(y) * pitch16 + x] = h;
+    }
+}
+
+__global__ void unpack_kernel(const float4* __restrict__ hyp, const float* __restrict__ cost_in, size_t n,
+                              float* __restrict__ depth, float* __restrict__ normal, float* __restrict__ cost) {
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const float4 h = hyp[i];
+        if (depth) depth[i] = h.x;
+        if (normal) {
+            normal[3 * i] = h.y;
+            normal[3 * i + 1] = h.z;
+            normal[3 * i + 2] = h.w;
+        }
+        if (cost) cost[i] = cost_in[i];
+    }
+}
+
+__global__ void pack_kernel(const float* __restrict__ depth, const float* __restrict__ normal,
+                            const float* __restrict__ cost, size_t n, float4* __restrict__ hyp,
+                            float* __restrict__ cost_out) {
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        if (depth && normal) hyp[i] = make_float4(depth[i], normal[3 * i], normal[3 * i + 1], normal[3 * i + 2]);
+        if (cost) cost_out[i] = cost[i];
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_to_f32(const void* src, int dtype, int W, int H, float* dst, int dst_pitch, __half* dst16,
+                          int dst16_pitch, cudaStream_t st) {
+    to_planes_kernel<<<stream_grid(), 256, 0, st>>>(src, dtype, W, H, dst, dst_pitch, dst16, dst16_pitch);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_unpack(const ViewDesc* vh, int view, float* depth, float* normal, float* cost,
+                          cudaStream_t st) {
+    const ViewDesc& v = vh[view];
+    unpack_kernel<<<stream_grid(), 256, 0, st>>>(v.hyp, v.cost, static_cast<size_t>(v.W) * v.H, depth, normal,
+                                                 cost);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pack(const ViewDesc* vh, int view, const float* depth, const float* normal, const float* cost,
+                        cudaStream_t st) {
+    const ViewDesc& v = vh[view];
+    pack_kernel<<<stream_grid(), 256, 0, st>>>(depth, normal, cost, static_cast<size_t>(v.W) * v.H, v.hyp,
+                                               v.cost);
+    return cudaGetLastError();
+}
+
+}  // namespace hp

@@ -1,0 +1,196 @@
+/*
+ * hpmvs.h - C ABI of the B200 PatchMatch multi-view-stereo engine.
+ *
+ * The engine fills the dense-reconstruction stage of the Hemiphoto3D pipeline.
+ * Its call surface follows the reference's
+ *     std::vector<DepthMap> runPatchMatchMVS(images, cameras, sfm, config)
+ * (src/dense_recon/patchmatch_mvs.h:39-44, defined at patchmatch_mvs.cu:1028):
+ * images and cameras in, one depth / normal / cost map per reference view out.
+ * Source views and the depth range, which the reference derives from the SfM
+ * result (selectSourceViews, patchmatch_mvs.cu:74-157), are explicit job inputs.
+ *
+ * Conventions
+ *  - Every entry point returns hp_status; nothing exits the process and no C++
+ *    exception crosses the boundary (the reference calls exit() through
+ *    CUDA_CHECK, src/utils/cuda_utils.cuh:7-15).  hp_ctx_last_error() gives text.
+ *  - Cameras are FP64, row-major, world-to-camera: P_cam = R * P_world + t
+ *    (CameraPose, include/types.h:55-74).
+ *  - Maps are row-major H x W.  Normals are camera-frame, 3 floats per pixel
+ *    (the frame the reference's kernels produce, patchmatch_mvs.cu:213-215).
+ *  - A pointer argument lives in host or device memory as its hp_memory flag
+ *    says; device pointers must belong to the context's device.
+ *  - One context per host thread, or external locking: a context is not
+ *    internally synchronised.  Work is issued on the context's own stream.
+ */
+#ifndef HPMVS_H_
+#define HPMVS_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HP_MAX_SOURCES 8   /* MAX_SRC_VIEWS, patchmatch_mvs.cu:18 */
+#define HP_MAX_RADIUS 7    /* the reference clamps to 5 (patchmatch_mvs.cu:24, :1065-1070) */
+#define HP_MAX_TOP_K 3     /* NCC_TOP_K, patchmatch_mvs.cu:26 */
+
+typedef enum hp_status {
+    HP_OK = 0,
+    HP_ERR_INVALID_ARG = 1,
+    HP_ERR_CUDA = 2,
+    HP_ERR_OUT_OF_MEMORY = 3,
+    HP_ERR_NOT_FOUND = 4,
+    HP_ERR_TIMEOUT = 5,
+    HP_ERR_UNSUPPORTED = 6,
+    HP_ERR_IO = 7,
+    HP_ERR_BUSY = 8,
+    HP_ERR_CANCELLED = 9
+} hp_status;
+
+typedef enum hp_dtype {
+    HP_DTYPE_U8 = 0,   /* 0..255, scaled by 1/255 on upload */
+    HP_DTYPE_F16 = 1,  /* IEEE half in [0,1] */
+    HP_DTYPE_F32 = 2   /* float in [0,1]: ImageData.gray, include/types.h:17 */
+} hp_dtype;
+
+typedef enum hp_precision {
+    /* Plain FP32: per-tap arithmetic and hardware bilinear sampling as in the
+     * reference's computePixelCost (patchmatch_mvs.cu:222-343). */
+    HP_PRECISION_F32 = 0,
+    /* FP16 image storage, FP16 window products with FP32 accumulation and
+     * mean-subtracted variance; FP64 homography setup. */
+    HP_PRECISION_F16ACC = 1
+} hp_precision;
+
+typedef enum hp_memory { HP_MEMORY_HOST = 0, HP_MEMORY_DEVICE = 1 } hp_memory;
+
+typedef struct hp_ctx hp_ctx;
+
+/* World-to-camera pinhole camera; all matrices row-major. */
+typedef struct hp_camera {
+    double K[9];
+    double R[9];
+    double t[3];
+} hp_camera;
+
+/* Solver parameters.  hp_params_default() gives the reference's constants:
+ * radius 5 (mvs_patch_size 11, include/types.h:151), stride 1, top-3 view
+ * selection, 2 refinement steps, ranges x0.6 per iteration and x0.5 per step
+ * (patchmatch_mvs.cu:598-607, :645-646). */
+typedef struct hp_params {
+    int radius;          /* window radius, 1..HP_MAX_RADIUS */
+    int stride;          /* window sampling stride, 1 or 2 */
+    int top_k;           /* sources averaged per pixel, 1..HP_MAX_TOP_K */
+    int precision;       /* hp_precision */
+    int refine_steps;    /* random perturbations per pixel visit, 0..4 */
+    float iter_decay;    /* perturbation range factor per iteration */
+    float step_decay;    /* perturbation range factor per refinement step */
+    int tile_w;          /* pixels per CTA row, 0 = engine choice (autotuned) */
+    int tile_h;          /* rows per CTA, 0 = engine choice */
+} hp_params;
+
+/* One reference view to solve. */
+typedef struct hp_job {
+    int ref_image;                     /* id from hp_image_upload */
+    int num_sources;                   /* 1..HP_MAX_SOURCES */
+    int src_images[HP_MAX_SOURCES];
+    hp_camera ref_cam;
+    hp_camera src_cams[HP_MAX_SOURCES];
+    float depth_min, depth_max;
+    uint64_t seed;                     /* RNG key; with view_id keys Philox streams */
+    uint32_t view_id;
+    int iterations;                    /* red-black iterations (mvs_iterations) */
+    /* When use_coeffs != 0 the per-source homography coefficients below are
+     * used as given instead of the FP64 setup from the cameras: kinv = K_ref^-1
+     * and ab[s] = {A (9), b (3)} with A = K_s R_rel K_ref^-1, b = K_s t_rel
+     * (GPUSourceView, patchmatch_mvs.cu:31-34).  This lets a caller feed the
+     * exact coefficients another implementation used. */
+    int use_coeffs;
+    float kinv[9];
+    float ab[HP_MAX_SOURCES][12];
+} hp_job;
+
+/* Per-view maps, caller-owned. */
+typedef struct hp_maps {
+    int memory;       /* hp_memory of the three pointers */
+    float* depth;     /* H*W */
+    float* normal;    /* H*W*3, camera frame */
+    float* cost;      /* H*W, mean of the top_k lowest 1-NCC, 2 = invalid */
+} hp_maps;
+
+const char* hp_status_string(hp_status s);
+void hp_params_default(hp_params* p);
+/* Library version as "major.minor.patch". */
+const char* hp_version(void);
+
+/* Context: owns a CUDA stream, the uploaded images and solver scratch. */
+hp_status hp_ctx_create(int device, hp_ctx** out);
+hp_status hp_ctx_destroy(hp_ctx* ctx);
+const char* hp_ctx_last_error(const hp_ctx* ctx);
+hp_status hp_ctx_synchronize(hp_ctx* ctx);
+/* Free device memory and the device total, in bytes. */
+hp_status hp_ctx_mem_info(hp_ctx* ctx, size_t* free_bytes, size_t* total_bytes);
+
+/* Replaces createGrayscaleTexture (patchmatch_mvs.cu:789-814): copies a W x H
+ * grayscale image (tightly packed rows) to the device, where it stays until
+ * released.  The FP32 and FP16 device copies the solver needs are made here. */
+hp_status hp_image_upload(hp_ctx* ctx, const void* data, int memory, int width, int height,
+                          int dtype, int* image_id);
+hp_status hp_image_release(hp_ctx* ctx, int image_id);
+hp_status hp_image_size(hp_ctx* ctx, int image_id, int* width, int* height);
+
+/* FP64 homography setup, replacing eigenToGPUCamera + precomputeSourceViews
+ * (patchmatch_mvs.cu:832-884): kinv9 = K_ref^-1, ab[s] = {A, b} per source. */
+hp_status hp_setup_homographies(const hp_camera* ref, const hp_camera* srcs, int num_sources,
+                                double* kinv9, double* ab);
+
+/* Replaces runPatchMatchMVS's per-view body (patchmatch_mvs.cu:1076-1260,
+ * without SfM seeding): random init, initial cost, `iterations` red-black
+ * propagate + refine passes.  out[j] receives job j's maps.  All jobs are
+ * solved as one batch: each half-pass is one launch over every job's pixels. */
+hp_status hp_solve(hp_ctx* ctx, const hp_job* jobs, int num_jobs, const hp_params* params,
+                   hp_maps* out);
+
+/* Replaces launchInitKernel (patchmatch_mvs.cu:890-902): Philox-keyed random
+ * depth in [depth_min, depth_max] and camera-facing unit normal per pixel.
+ * Fills out->depth and out->normal. */
+hp_status hp_init_hypotheses(hp_ctx* ctx, const hp_job* job, const hp_params* params,
+                             hp_maps* out);
+
+/* Replaces launchNCCCostKernel (patchmatch_mvs.cu:904-934): NCC cost with
+ * top-k view selection of the given (depth, normal) hypotheses; writes
+ * maps->cost.  maps->depth / maps->normal are read only. */
+hp_status hp_ncc_cost(hp_ctx* ctx, const hp_job* job, const hp_params* params, hp_maps* maps);
+
+/* Replaces launchPropagateRefineKernel (patchmatch_mvs.cu:936-961): one
+ * red-black half-pass (color 0: (x+y) even, 1: odd) of iteration `iteration`,
+ * in place on maps (depth, normal, cost). */
+hp_status hp_propagate_pass(hp_ctx* ctx, const hp_job* job, const hp_params* params,
+                            hp_maps* maps, int iteration, int color);
+
+/* Replaces geometric_consistency_filter_kernel + its host packing
+ * (patchmatch_mvs.cu:668-781, :1267-1384).  depth and confidence are updated
+ * in place: a pixel with fewer than min_consistent agreeing sources gets 0 in
+ * both.  Reference defaults: depth_tol 0.12, normal_tol_cos cos(180 deg),
+ * min_consistent 2.  All map pointers are in `memory`. */
+hp_status hp_geometric_filter(hp_ctx* ctx, const hp_camera* ref_cam, int width, int height,
+                              float* depth, const float* normal, float* confidence,
+                              int num_sources, const hp_camera* src_cams,
+                              const float* const* src_depths, const float* const* src_normals,
+                              int memory, float depth_tol, float normal_tol_cos,
+                              int min_consistent);
+
+/* Replaces saveDepthMapPFM / loadDepthMapPFM (patchmatch_mvs.cu:990-1022):
+ * 'Pf' (channels 1) or 'PF' (channels 3) little-endian PFM, rows bottom-up. */
+hp_status hp_pfm_write(const char* path, const float* data, int width, int height, int channels);
+/* Reads into `data` (capacity floats); width/height/channels receive the header. */
+hp_status hp_pfm_read(const char* path, float* data, size_t capacity, int* width, int* height,
+                      int* channels);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HPMVS_H_ */

@@ -1,0 +1,642 @@
+/*
+ * pm_oracle.c - CPU restatement of the reference's PatchMatch MVS path.
+ *
+ * TEST INFRASTRUCTURE (the checker and the timed CPU baseline); the engine
+ * never links it.  Built with -ffp-contract=off so every float operation below
+ * rounds exactly as written; fused multiply-adds are spelled fmaf().
+ *
+ * Reference citations are src/dense_recon/patchmatch_mvs.cu:<line>.
+ */
+#include "pm_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+static int g_tex_rounding = 0;
+void orc_set_tex_rounding(int mode) { g_tex_rounding = mode; }
+int orc_get_tex_rounding(void) { return g_tex_rounding; }
+
+int orc_num_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+void orc_set_num_threads(int n) {
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}
+
+/* ---------------------------------------------------------------------------
+ * Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy
+ * as 1, 2, 3", SC'11).  Engine keying: key = (seed lo, seed hi); counter =
+ * (pixel index, view id, phase, block) with phase 0 for initialisation and
+ * 1 + iteration for the refinement draws of that iteration.
+ * ------------------------------------------------------------------------- */
+void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+    const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+    const uint32_t W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+    uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3];
+    uint32_t k0 = key[0], k1 = key[1];
+    for (int r = 0; r < 10; ++r) {
+        uint64_t p0 = (uint64_t)M0 * c0;
+        uint64_t p1 = (uint64_t)M1 * c2;
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        c0 = hi1 ^ c1 ^ k0;
+        c1 = lo1;
+        c2 = hi0 ^ c3 ^ k1;
+        c3 = lo0;
+        k0 += W0;
+        k1 += W1;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+/* Uniform in (0,1): (2*(x>>9)+1) * 2^-24, exactly representable. */
+float orc_u01(uint32_t x) { return (float)(2u * (x >> 9) + 1u) * 5.9604644775390625e-8f; }
+
+static void draw4(uint64_t seed, uint32_t pixel, uint32_t view, uint32_t phase, uint32_t block, float u[4]) {
+    uint32_t ctr[4] = {pixel, view, phase, block};
+    uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    uint32_t r[4];
+    orc_philox4x32_10(ctr, key, r);
+    for (int i = 0; i < 4; ++i) u[i] = orc_u01(r[i]);
+}
+
+/* sin and cos of 2*pi*u for u in (0,1): quadrant reduction then Taylor series
+ * of degree 11 / 12 on |a| <= pi/4, Horner form with fmaf (engine-defined so
+ * host and device agree bit for bit). */
+static void sincos_2pi(float u, float* s_out, float* c_out) {
+    float q = rintf(u * 4.0f);
+    float f = u - q * 0.25f;
+    float a = f * 6.28318530717958647692f;
+    float a2 = a * a;
+    float s = fmaf(a2, -2.50521083854417187751e-8f, 2.75573192239858906526e-6f);
+    s = fmaf(a2, s, -1.98412698412698412698e-4f);
+    s = fmaf(a2, s, 8.33333333333333333333e-3f);
+    s = fmaf(a2, s, -1.66666666666666666667e-1f);
+    s = fmaf(a2 * a, s, a);
+    float c = fmaf(a2, 2.08767569878680989792e-9f, -2.75573192239858906526e-7f);
+    c = fmaf(a2, c, 2.48015873015873015873e-5f);
+    c = fmaf(a2, c, -1.38888888888888888889e-3f);
+    c = fmaf(a2, c, 4.16666666666666666667e-2f);
+    c = fmaf(a2, c, -0.5f);
+    c = fmaf(a2, c, 1.0f);
+    int qi = ((int)q) & 3;
+    float so, co;
+    switch (qi) {
+        case 0: so = s; co = c; break;
+        case 1: so = c; co = -s; break;
+        case 2: so = -s; co = -c; break;
+        default: so = -c; co = s; break;
+    }
+    *s_out = so;
+    *c_out = co;
+}
+
+/* ---------------------------------------------------------------------------
+ * FP64 homography setup (the reference does this in FP32 after an FP64
+ * inverse: eigenToGPUCamera :832-844, precomputeSourceViews :847-884).
+ * ------------------------------------------------------------------------- */
+static void mat3_mul(const double* a, const double* b, double* c) {
+    for (int r = 0; r < 3; ++r)
+        for (int k = 0; k < 3; ++k)
+            c[3 * r + k] = a[3 * r] * b[k] + a[3 * r + 1] * b[3 + k] + a[3 * r + 2] * b[6 + k];
+}
+static int mat3_inv(const double* m, double* inv) {
+    double det = m[0] * (m[4] * m[8] - m[5] * m[7]) - m[1] * (m[3] * m[8] - m[5] * m[6]) +
+                 m[2] * (m[3] * m[7] - m[4] * m[6]);
+    if (fabs(det) < 1e-300) return 1;
+    double id = 1.0 / det;
+    inv[0] = (m[4] * m[8] - m[5] * m[7]) * id;
+    inv[1] = (m[2] * m[7] - m[1] * m[8]) * id;
+    inv[2] = (m[1] * m[5] - m[2] * m[4]) * id;
+    inv[3] = (m[5] * m[6] - m[3] * m[8]) * id;
+    inv[4] = (m[0] * m[8] - m[2] * m[6]) * id;
+    inv[5] = (m[2] * m[3] - m[0] * m[5]) * id;
+    inv[6] = (m[3] * m[7] - m[4] * m[6]) * id;
+    inv[7] = (m[1] * m[6] - m[0] * m[7]) * id;
+    inv[8] = (m[0] * m[4] - m[1] * m[3]) * id;
+    return 0;
+}
+
+int orc_setup_f64(const orc_camera* ref, const orc_camera* srcs, int S, double* kinv9, double* ab) {
+    if (mat3_inv(ref->K, kinv9)) return 1;
+    double RrT[9];
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) RrT[3 * r + c] = ref->R[3 * c + r];
+    for (int s = 0; s < S; ++s) {
+        const orc_camera* cs = &srcs[s];
+        double Rrel[9], tmp[9], A[9];
+        mat3_mul(cs->R, RrT, Rrel);
+        double trel[3];
+        for (int r = 0; r < 3; ++r)
+            trel[r] = cs->t[r] - (Rrel[3 * r] * ref->t[0] + Rrel[3 * r + 1] * ref->t[1] + Rrel[3 * r + 2] * ref->t[2]);
+        mat3_mul(Rrel, kinv9, tmp);
+        mat3_mul(cs->K, tmp, A);
+        double* o = ab + 12 * s;
+        for (int i = 0; i < 9; ++i) o[i] = A[i];
+        for (int r = 0; r < 3; ++r)
+            o[9 + r] = cs->K[3 * r] * trel[0] + cs->K[3 * r + 1] * trel[1] + cs->K[3 * r + 2] * trel[2];
+    }
+    return 0;
+}
+
+int orc_view_set_cameras(orc_view* v, const orc_camera* ref, const orc_camera* srcs) {
+    double ab[ORC_MAX_SOURCES * 12];
+    if (orc_setup_f64(ref, srcs, v->S, v->kinv64, ab)) return 1;
+    for (int i = 0; i < 9; ++i) v->kinv[i] = (float)v->kinv64[i];
+    for (int s = 0; s < v->S; ++s)
+        for (int i = 0; i < 12; ++i) {
+            v->ab64[s][i] = ab[12 * s + i];
+            v->ab[s][i] = (float)ab[12 * s + i];
+        }
+    return 0;
+}
+
+/* ---------------------------------------------------------------------------
+ * Texture unit, linear filter, clamp addressing, unnormalised coordinates
+ * (createGrayscaleTexture :789-814).  The coordinate is converted to fixed
+ * point with 8 fractional bits, the texel-centre offset of 0.5 removed, and
+ * the fractional part used as the 9-bit weight (CUDA C++ Programming Guide,
+ * "Texture Fetching", linear filtering).
+ * ------------------------------------------------------------------------- */
+static inline float texel(const float* img, int W, int H, long x, long y) {
+    if (x < 0) x = 0;
+    if (x > W - 1) x = W - 1;
+    if (y < 0) y = 0;
+    if (y > H - 1) y = H - 1;
+    return img[(size_t)y * W + x];
+}
+
+static inline long to_fixed8(float c) {
+    float s = c * 256.0f; /* exact: power-of-two scale */
+    return g_tex_rounding == 0 ? (long)rintf(s) : (long)floorf(s);
+}
+
+float orc_tex_linear(const float* img, int W, int H, float xc, float yc) {
+    long X = to_fixed8(xc) - 128, Y = to_fixed8(yc) - 128;
+    long i = X >= 0 ? X >> 8 : -((-X + 255) >> 8);
+    long j = Y >= 0 ? Y >> 8 : -((-Y + 255) >> 8);
+    double a = (double)(X - i * 256) / 256.0, b = (double)(Y - j * 256) / 256.0;
+    double t00 = texel(img, W, H, i, j), t10 = texel(img, W, H, i + 1, j);
+    double t01 = texel(img, W, H, i, j + 1), t11 = texel(img, W, H, i + 1, j + 1);
+    return (float)((1 - a) * (1 - b) * t00 + a * (1 - b) * t10 + (1 - a) * b * t01 + a * b * t11);
+}
+
+static inline double bilinear_exact(const float* img, int W, int H, double u, double v) {
+    double fi = floor(u), fj = floor(v);
+    long i = (long)fi, j = (long)fj;
+    double a = u - fi, b = v - fj;
+    double t00 = texel(img, W, H, i, j), t10 = texel(img, W, H, i + 1, j);
+    double t01 = texel(img, W, H, i, j + 1), t11 = texel(img, W, H, i + 1, j + 1);
+    return (1 - a) * (1 - b) * t00 + a * (1 - b) * t10 + (1 - a) * b * t01 + a * b * t11;
+}
+
+static inline double bilinear_q8(const float* img, int W, int H, double u, double v) {
+    /* 8-bit weights from an exact coordinate (FP64 oracle with texture weights). */
+    double fi = floor(u), fj = floor(v);
+    long i = (long)fi, j = (long)fj;
+    double a = (g_tex_rounding == 0 ? nearbyint((u - fi) * 256.0) : floor((u - fi) * 256.0)) / 256.0;
+    double b = (g_tex_rounding == 0 ? nearbyint((v - fj) * 256.0) : floor((v - fj) * 256.0)) / 256.0;
+    double t00 = texel(img, W, H, i, j), t10 = texel(img, W, H, i + 1, j);
+    double t01 = texel(img, W, H, i, j + 1), t11 = texel(img, W, H, i + 1, j + 1);
+    return (1 - a) * (1 - b) * t00 + a * (1 - b) * t10 + (1 - a) * b * t01 + a * b * t11;
+}
+
+/* ---------------------------------------------------------------------------
+ * Cost of one hypothesis at one pixel (computePixelCost :222-343).
+ * Window taps at offsets -r, -r+s, ..., (stride s; the reference has s = 1);
+ * a source needs count >= taps/2 valid taps (:258, :309).  Per source:
+ * cost = 1 - clamp(NCC, -1, 1), or 2 when invalid; the pixel's cost is the
+ * mean of the top_k lowest (:326-342).
+ * ------------------------------------------------------------------------- */
+static inline void topk_insert(float* top, int k, float c) {
+    if (c < top[k - 1]) {
+        top[k - 1] = c;
+        for (int i = k - 2; i >= 0; --i) {
+            if (top[i + 1] < top[i]) {
+                float t = top[i];
+                top[i] = top[i + 1];
+                top[i + 1] = t;
+            } else {
+                break;
+            }
+        }
+    }
+}
+
+/* FP32 arithmetic written as the reference's expressions contract on the GPU
+ * (a*b + c*d + e -> fma(a, b, c*d) + e; x + y*z -> fma(y, z, x)). */
+float orc_pixel_cost_f32(const orc_view* v, int x, int y, float d, float nx, float ny, float nz) {
+    const float* k = v->kinv;
+    const float fx = (float)x, fy = (float)y;
+    const float Px = d * (fmaf(k[0], fx, k[1] * fy) + k[2]);
+    const float Py = d * (fmaf(k[3], fx, k[4] * fy) + k[5]);
+    const float Pz = d * (fmaf(k[6], fx, k[7] * fy) + k[8]);
+    const float ndp = fmaf(nz, Pz, fmaf(nx, Px, ny * Py));
+    if (fabsf(ndp) < 1e-8f) return 2.0f;
+    const float inv_ndp = 1.0f / ndp;
+    const float nK0 = fmaf(k[6], nz, fmaf(k[0], nx, k[3] * ny));
+    const float nK1 = fmaf(k[7], nz, fmaf(k[1], nx, k[4] * ny));
+    const float nK2 = fmaf(k[8], nz, fmaf(k[2], nx, k[5] * ny));
+    const int r = v->radius, st = v->stride;
+    const int n_side = (2 * r) / st + 1;
+    const int min_count = (n_side * n_side) / 2;
+    const float fW = (float)v->W, fH = (float)v->H;
+    float top[3] = {2.0f, 2.0f, 2.0f};
+    const int K = v->top_k < v->S ? v->top_k : v->S;
+    for (int s = 0; s < v->S; ++s) {
+        const float* A = v->ab[s];
+        const float* b = A + 9;
+        float sr = 0.f, ss = 0.f, srr = 0.f, sss = 0.f, srs = 0.f;
+        int count = 0;
+        for (int dy = -r; dy <= r; dy += st) {
+            for (int dx = -r; dx <= r; dx += st) {
+                const float rv = texel(v->ref, v->W, v->H, x + dx, y + dy);
+                const float wpx = fx + (float)dx, wpy = fy + (float)dy;
+                const float qx = fmaf(A[0], wpx, A[1] * wpy) + A[2];
+                const float qy = fmaf(A[3], wpx, A[4] * wpy) + A[5];
+                const float qz = fmaf(A[6], wpx, A[7] * wpy) + A[8];
+                const float sval = fmaf(nK0, wpx, nK1 * wpy) + nK2;
+                const float factor = sval * inv_ndp;
+                const float wz = fmaf(b[2], factor, qz);
+                if (fabsf(wz) < 1e-8f) continue;
+                const float iw = 1.0f / wz;
+                const float u = fmaf(b[0], factor, qx) * iw;
+                const float vv = fmaf(b[1], factor, qy) * iw;
+                if (u < 0.0f || u >= fW - 1.0f || vv < 0.0f || vv >= fH - 1.0f) continue;
+                const float sv = orc_tex_linear(v->src[s], v->W, v->H, u + 0.5f, vv + 0.5f);
+                sr += rv;
+                ss += sv;
+                srr = fmaf(rv, rv, srr);
+                sss = fmaf(sv, sv, sss);
+                srs = fmaf(rv, sv, srs);
+                count++;
+            }
+        }
+        float c;
+        if (count < min_count) {
+            c = 2.0f;
+        } else {
+            const float fc = (float)count;
+            const float num = fmaf(fc, srs, -(sr * ss));
+            const float den_r = fmaf(fc, srr, -(sr * sr));
+            const float den_s = fmaf(fc, sss, -(ss * ss));
+            if (den_r < 1e-6f || den_s < 1e-6f) {
+                c = 2.0f;
+            } else {
+                float ncc = num / (sqrtf(den_r) * sqrtf(den_s));
+                ncc = fmaxf(-1.0f, fminf(1.0f, ncc));
+                c = 1.0f - ncc;
+            }
+        }
+        topk_insert(top, v->top_k, c);
+    }
+    float sum = 0.f;
+    for (int i = 0; i < K; ++i) sum += top[i];
+    return sum / (float)K;
+}
+
+int orc_source_ncc_f64(const orc_view* v, int x, int y, double d, double nx, double ny, double nz, int qw,
+                       double* out_ncc) {
+    const double* k = v->kinv64;
+    const double fx = x, fy = y;
+    const double Px = d * (k[0] * fx + k[1] * fy + k[2]);
+    const double Py = d * (k[3] * fx + k[4] * fy + k[5]);
+    const double Pz = d * (k[6] * fx + k[7] * fy + k[8]);
+    const double ndp = nx * Px + ny * Py + nz * Pz;
+    int mask = 0;
+    for (int s = 0; s < v->S; ++s) out_ncc[s] = -2.0;
+    if (fabs(ndp) < 1e-8) return 0;
+    const double nK0 = k[0] * nx + k[3] * ny + k[6] * nz;
+    const double nK1 = k[1] * nx + k[4] * ny + k[7] * nz;
+    const double nK2 = k[2] * nx + k[5] * ny + k[8] * nz;
+    const int r = v->radius, st = v->stride;
+    const int n_side = (2 * r) / st + 1;
+    const int min_count = (n_side * n_side) / 2;
+    for (int s = 0; s < v->S; ++s) {
+        const double* A = v->ab64[s];
+        const double* b = A + 9;
+        double sr = 0, ss = 0, srr = 0, sss = 0, srs = 0;
+        int count = 0;
+        for (int dy = -r; dy <= r; dy += st) {
+            for (int dx = -r; dx <= r; dx += st) {
+                const double rv = texel(v->ref, v->W, v->H, x + dx, y + dy);
+                const double px = fx + dx, py = fy + dy;
+                const double f = (nK0 * px + nK1 * py + nK2) / ndp;
+                const double wx = A[0] * px + A[1] * py + A[2] + b[0] * f;
+                const double wy = A[3] * px + A[4] * py + A[5] + b[1] * f;
+                const double wz = A[6] * px + A[7] * py + A[8] + b[2] * f;
+                if (fabs(wz) < 1e-8) continue;
+                const double u = wx / wz, vv = wy / wz;
+                if (u < 0.0 || u >= v->W - 1.0 || vv < 0.0 || vv >= v->H - 1.0) continue;
+                const double sv = qw ? bilinear_q8(v->src[s], v->W, v->H, u, vv)
+                                     : bilinear_exact(v->src[s], v->W, v->H, u, vv);
+                sr += rv;
+                ss += sv;
+                srr += rv * rv;
+                sss += sv * sv;
+                srs += rv * sv;
+                count++;
+            }
+        }
+        if (count < min_count) continue;
+        const double n = count;
+        const double mr = sr / n, ms = ss / n;
+        const double vr = srr / n - mr * mr, vs = sss / n - ms * ms, cv = srs / n - mr * ms;
+        /* the reference's guard is den < 1e-6 on n*sum(x^2) - sum(x)^2 = n^2 var */
+        if (vr * n * n < 1e-6 || vs * n * n < 1e-6) continue;
+        double ncc = cv / (sqrt(vr) * sqrt(vs));
+        out_ncc[s] = ncc;
+        mask |= 1 << s;
+    }
+    return mask;
+}
+
+double orc_pixel_cost_f64(const orc_view* v, int x, int y, double d, double nx, double ny, double nz, int qw) {
+    double ncc[ORC_MAX_SOURCES];
+    int mask = orc_source_ncc_f64(v, x, y, d, nx, ny, nz, qw, ncc);
+    double top[3] = {2.0, 2.0, 2.0};
+    const int kk = v->top_k;
+    for (int s = 0; s < v->S; ++s) {
+        double c = 2.0;
+        if (mask & (1 << s)) {
+            double n = ncc[s];
+            if (n > 1) n = 1;
+            if (n < -1) n = -1;
+            c = 1.0 - n;
+        }
+        if (c < top[kk - 1]) {
+            top[kk - 1] = c;
+            for (int i = kk - 2; i >= 0; --i) {
+                if (top[i + 1] < top[i]) {
+                    double t = top[i];
+                    top[i] = top[i + 1];
+                    top[i + 1] = t;
+                } else {
+                    break;
+                }
+            }
+        }
+    }
+    const int K = kk < v->S ? kk : v->S;
+    double sum = 0;
+    for (int i = 0; i < K; ++i) sum += top[i];
+    return sum / K;
+}
+
+void orc_cost_map_f32(const orc_view* v, const float* depth, const float* normal, float* cost) {
+    const int W = v->W, H = v->H;
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int y = 0; y < H; ++y)
+        for (int x = 0; x < W; ++x) {
+            size_t i = (size_t)y * W + x;
+            cost[i] = orc_pixel_cost_f32(v, x, y, depth[i], normal[3 * i], normal[3 * i + 1], normal[3 * i + 2]);
+        }
+}
+
+void orc_cost_map_f64(const orc_view* v, const float* depth, const float* normal, int qw, double* cost) {
+    const int W = v->W, H = v->H;
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int y = 0; y < H; ++y)
+        for (int x = 0; x < W; ++x) {
+            size_t i = (size_t)y * W + x;
+            cost[i] = orc_pixel_cost_f64(v, x, y, depth[i], normal[3 * i], normal[3 * i + 1], normal[3 * i + 2], qw);
+        }
+}
+
+/* ---------------------------------------------------------------------------
+ * Initialisation (init_depth_normal_kernel :164-216): depth uniform in
+ * [dmin, dmax]; normal from theta in [0, 2pi) and cos(phi) in [0, 1), flipped
+ * to face the camera and normalised.  Engine keying and arithmetic.
+ * ------------------------------------------------------------------------- */
+static inline void view_ray(const float* k, int x, int y, float* rx, float* ry, float* rz) {
+    const float fx = (float)x, fy = (float)y;
+    float a = fmaf(k[0], fx, fmaf(k[1], fy, k[2]));
+    float b = fmaf(k[3], fx, fmaf(k[4], fy, k[5]));
+    float c = fmaf(k[6], fx, fmaf(k[7], fy, k[8]));
+    float len = sqrtf(fmaf(a, a, fmaf(b, b, c * c)));
+    if (len > 1e-12f) {
+        a = a / len;
+        b = b / len;
+        c = c / len;
+    }
+    *rx = a;
+    *ry = b;
+    *rz = c;
+}
+
+static inline void normalize3(float* x, float* y, float* z) {
+    float len = sqrtf(fmaf(*x, *x, fmaf(*y, *y, *z * *z)));
+    if (len > 1e-12f) {
+        *x = *x / len;
+        *y = *y / len;
+        *z = *z / len;
+    }
+}
+
+void orc_init(const orc_view* v, float dmin, float dmax, uint64_t seed, uint32_t view_id, float* depth,
+              float* normal) {
+    const int W = v->W, H = v->H;
+#pragma omp parallel for schedule(static)
+    for (int y = 0; y < H; ++y)
+        for (int x = 0; x < W; ++x) {
+            uint32_t idx = (uint32_t)(y * W + x);
+            float u[4];
+            draw4(seed, idx, view_id, 0u, 0u, u);
+            depth[idx] = fmaf(u[0], dmax - dmin, dmin);
+            float rx, ry, rz;
+            view_ray(v->kinv, x, y, &rx, &ry, &rz);
+            float st, ct;
+            sincos_2pi(u[1], &st, &ct);
+            float cp = u[2];
+            float sp = sqrtf(fmaxf(0.0f, fmaf(-cp, cp, 1.0f)));
+            float nx = sp * ct, ny = sp * st, nz = cp;
+            if (fmaf(nx, rx, fmaf(ny, ry, nz * rz)) > 0.0f) {
+                nx = -nx;
+                ny = -ny;
+                nz = -nz;
+            }
+            normalize3(&nx, &ny, &nz);
+            normal[3 * (size_t)idx] = nx;
+            normal[3 * (size_t)idx + 1] = ny;
+            normal[3 * (size_t)idx + 2] = nz;
+        }
+}
+
+/* ---------------------------------------------------------------------------
+ * One red-black half-pass (propagate_and_refine_kernel :519-655): pixels of
+ * the given color try their 4 neighbours' hypotheses (L, R, U, D; skipped
+ * outside the image or outside [dmin, dmax]) and then `refine_steps` random
+ * perturbations of the running best, keeping any strictly lower cost.
+ * Perturbation ranges: depth (dmax-dmin)/2 and normal 1, both x iter_decay
+ * per iteration and x step_decay per step.
+ * ------------------------------------------------------------------------- */
+void orc_propagate_pass(const orc_view* v, float* depth, float* normal, float* cost, float dmin, float dmax,
+                        int iteration, int color, uint64_t seed, uint32_t view_id, const orc_refine* rf) {
+    const int W = v->W, H = v->H;
+    static const int dx4[4] = {-1, 1, 0, 0};
+    static const int dy4[4] = {0, 0, -1, 1};
+#pragma omp parallel for schedule(dynamic, 2)
+    for (int y = 0; y < H; ++y) {
+        for (int x = ((y + color) & 1); x < W; x += 2) {
+            const size_t idx = (size_t)y * W + x;
+            float bd = depth[idx], bnx = normal[3 * idx], bny = normal[3 * idx + 1], bnz = normal[3 * idx + 2];
+            float bc = cost[idx];
+            for (int n = 0; n < 4; ++n) {
+                const int xx = x + dx4[n], yy = y + dy4[n];
+                if (xx < 0 || xx >= W || yy < 0 || yy >= H) continue;
+                const size_t ni = (size_t)yy * W + xx;
+                const float nd = depth[ni];
+                if (nd < dmin || nd > dmax) continue;
+                const float nnx = normal[3 * ni], nny = normal[3 * ni + 1], nnz = normal[3 * ni + 2];
+                const float c = orc_pixel_cost_f32(v, x, y, nd, nnx, nny, nnz);
+                if (c < bc) {
+                    bc = c;
+                    bd = nd;
+                    bnx = nnx;
+                    bny = nny;
+                    bnz = nnz;
+                }
+            }
+            float rx, ry, rz;
+            view_ray(v->kinv, x, y, &rx, &ry, &rz);
+            float drange = (dmax - dmin) * 0.5f;
+            float nrange = 1.0f;
+            for (int i = 0; i < iteration; ++i) {
+                drange *= rf->iter_decay;
+                nrange *= rf->iter_decay;
+            }
+            for (int step = 0; step < rf->refine_steps; ++step) {
+                float u[4];
+                draw4(seed, (uint32_t)idx, view_id, 1u + (uint32_t)iteration, (uint32_t)step, u);
+                float cd = fmaf(fmaf(u[0], 2.0f, -1.0f), drange, bd);
+                cd = fmaxf(dmin, fminf(dmax, cd));
+                float cx = fmaf(fmaf(u[1], 2.0f, -1.0f), nrange, bnx);
+                float cy = fmaf(fmaf(u[2], 2.0f, -1.0f), nrange, bny);
+                float cz = fmaf(fmaf(u[3], 2.0f, -1.0f), nrange, bnz);
+                normalize3(&cx, &cy, &cz);
+                if (fmaf(cx, rx, fmaf(cy, ry, cz * rz)) > 0.0f) {
+                    cx = -cx;
+                    cy = -cy;
+                    cz = -cz;
+                }
+                const float c = orc_pixel_cost_f32(v, x, y, cd, cx, cy, cz);
+                if (c < bc) {
+                    bc = c;
+                    bd = cd;
+                    bnx = cx;
+                    bny = cy;
+                    bnz = cz;
+                }
+                drange *= rf->step_decay;
+                nrange *= rf->step_decay;
+            }
+            depth[idx] = bd;
+            normal[3 * idx] = bnx;
+            normal[3 * idx + 1] = bny;
+            normal[3 * idx + 2] = bnz;
+            cost[idx] = bc;
+        }
+    }
+}
+
+void orc_solve_view(const orc_view* v, float dmin, float dmax, uint64_t seed, uint32_t view_id, int iterations,
+                    const orc_refine* rf, float* depth, float* normal, float* cost) {
+    orc_init(v, dmin, dmax, seed, view_id, depth, normal);
+    orc_cost_map_f32(v, depth, normal, cost);
+    for (int it = 0; it < iterations; ++it) {
+        orc_propagate_pass(v, depth, normal, cost, dmin, dmax, it, 0, seed, view_id, rf);
+        orc_propagate_pass(v, depth, normal, cost, dmin, dmax, it, 1, seed, view_id, rf);
+    }
+}
+
+/* ---------------------------------------------------------------------------
+ * Geometric consistency filter (:668-781), FP32 camera values as the
+ * reference's eigenToGPUCamera casts them (:832-844).
+ * ------------------------------------------------------------------------- */
+void orc_geometric_filter(const orc_camera* ref, int W, int H, float* depth, const float* normal, float* conf,
+                          int S, const orc_camera* srcs, const float* const* src_depths,
+                          const float* const* src_normals, float depth_tol, float normal_tol_cos,
+                          int min_consistent) {
+    double kinv64[9];
+    if (mat3_inv(ref->K, kinv64)) return;
+    float ki[9], R[9], t[3];
+    for (int i = 0; i < 9; ++i) {
+        ki[i] = (float)kinv64[i];
+        R[i] = (float)ref->R[i];
+    }
+    for (int i = 0; i < 3; ++i) t[i] = (float)ref->t[i];
+    float sK[ORC_MAX_SOURCES][9], sR[ORC_MAX_SOURCES][9], st[ORC_MAX_SOURCES][3];
+    for (int s = 0; s < S; ++s) {
+        for (int i = 0; i < 9; ++i) {
+            sK[s][i] = (float)srcs[s].K[i];
+            sR[s][i] = (float)srcs[s].R[i];
+        }
+        for (int i = 0; i < 3; ++i) st[s][i] = (float)srcs[s].t[i];
+    }
+#pragma omp parallel for schedule(static)
+    for (int y = 0; y < H; ++y)
+        for (int x = 0; x < W; ++x) {
+            const size_t idx = (size_t)y * W + x;
+            const float d = depth[idx];
+            if (d <= 0.0f) {
+                conf[idx] = 0.0f;
+                continue;
+            }
+            const float fx = (float)x, fy = (float)y;
+            const float pcx = d * (fmaf(ki[0], fx, ki[1] * fy) + ki[2]);
+            const float pcy = d * (fmaf(ki[3], fx, ki[4] * fy) + ki[5]);
+            const float pcz = d * (fmaf(ki[6], fx, ki[7] * fy) + ki[8]);
+            const float ax = pcx - t[0], ay = pcy - t[1], az = pcz - t[2];
+            const float pwx = fmaf(R[6], az, fmaf(R[0], ax, R[3] * ay));
+            const float pwy = fmaf(R[7], az, fmaf(R[1], ax, R[4] * ay));
+            const float pwz = fmaf(R[8], az, fmaf(R[2], ax, R[5] * ay));
+            const float ncx = normal[3 * idx], ncy = normal[3 * idx + 1], ncz = normal[3 * idx + 2];
+            const float nwx = fmaf(R[6], ncz, fmaf(R[0], ncx, R[3] * ncy));
+            const float nwy = fmaf(R[7], ncz, fmaf(R[1], ncx, R[4] * ncy));
+            const float nwz = fmaf(R[8], ncz, fmaf(R[2], ncx, R[5] * ncy));
+            int consistent = 0;
+            for (int s = 0; s < S; ++s) {
+                const float* Rs = sR[s];
+                const float* Ks = sK[s];
+                const float psx = fmaf(Rs[2], pwz, fmaf(Rs[0], pwx, Rs[1] * pwy)) + st[s][0];
+                const float psy = fmaf(Rs[5], pwz, fmaf(Rs[3], pwx, Rs[4] * pwy)) + st[s][1];
+                const float psz = fmaf(Rs[8], pwz, fmaf(Rs[6], pwx, Rs[7] * pwy)) + st[s][2];
+                if (psz <= 0.0f) continue;
+                const float prx = fmaf(Ks[2], psz, fmaf(Ks[0], psx, Ks[1] * psy));
+                const float pry = fmaf(Ks[5], psz, fmaf(Ks[3], psx, Ks[4] * psy));
+                const float prz = fmaf(Ks[8], psz, fmaf(Ks[6], psx, Ks[7] * psy));
+                const float u = prx / prz, vv = pry / prz;
+                const int ui = (int)rintf(u), vi = (int)rintf(vv);
+                if (ui < 0 || ui >= W || vi < 0 || vi >= H) continue;
+                const size_t sp = (size_t)vi * W + ui;
+                const float ds = src_depths[s][sp];
+                if (ds <= 0.0f) continue;
+                const float err = fabsf(ds - psz) / psz;
+                if (err > depth_tol) continue;
+                const float nsx = src_normals[s][3 * sp], nsy = src_normals[s][3 * sp + 1],
+                            nsz = src_normals[s][3 * sp + 2];
+                const float qx = fmaf(Rs[6], nsz, fmaf(Rs[0], nsx, Rs[3] * nsy));
+                const float qy = fmaf(Rs[7], nsz, fmaf(Rs[1], nsx, Rs[4] * nsy));
+                const float qz = fmaf(Rs[8], nsz, fmaf(Rs[2], nsx, Rs[5] * nsy));
+                const float cosang = fmaf(nwz, qz, fmaf(nwx, qx, nwy * qy));
+                if (cosang < normal_tol_cos) continue;
+                consistent++;
+            }
+            if (consistent < min_consistent) {
+                depth[idx] = 0.0f;
+                conf[idx] = 0.0f;
+            }
+        }
+}

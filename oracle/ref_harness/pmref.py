@@ -1,0 +1,117 @@
+"""ctypes binding of the GPU reference harness (oracle/_ref/libpmref.so) - TEST INFRASTRUCTURE.
+
+libpmref.so is the reference's own src/dense_recon/patchmatch_mvs.cu compiled
+unmodified (see Makefile and ref_harness.cu).  Tests call it as the parity
+anchor; it is only built where the reference tree exists, so callers skip when
+:func:`available` is False.  All arrays are host float32.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "..", "_ref", "libpmref.so")
+
+_lib = None
+
+
+def available() -> bool:
+    return os.path.exists(LIB_PATH)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        L = C.CDLL(LIB_PATH)
+        fp, dp, ip = C.c_void_p, C.c_void_p, C.c_int
+        L.pmref_setup_views.argtypes = [dp, dp, ip, fp, fp]
+        L.pmref_ncc_cost.argtypes = [fp, C.c_void_p, ip, ip, ip, fp, fp, fp, fp, ip, fp]
+        L.pmref_pixel_cost.argtypes = [fp, C.c_void_p, ip, ip, ip, fp, fp, fp, fp, ip, fp]
+        L.pmref_init.argtypes = [fp, ip, ip, C.c_float, C.c_float, C.c_uint64, fp, fp]
+        L.pmref_propagate.argtypes = [fp, C.c_void_p, ip, ip, ip, fp, fp, fp, fp, fp, C.c_float, C.c_float, ip, ip,
+                                      ip, C.c_uint64]
+        L.pmref_solve_view.argtypes = [fp, C.c_void_p, ip, ip, ip, fp, fp, C.c_float, C.c_float, ip, ip, ip, fp, fp,
+                                       fp, C.POINTER(C.c_float)]
+        L.pmref_geometric_filter.argtypes = [fp, fp, fp, dp, fp, fp, dp, ip, ip, ip, C.c_float, C.c_float, ip]
+        for f in ("pmref_setup_views", "pmref_ncc_cost", "pmref_pixel_cost", "pmref_init", "pmref_propagate",
+                  "pmref_solve_view", "pmref_geometric_filter"):
+            getattr(L, f).restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data
+
+
+def _krt(cam):
+    K, R, t = cam
+    return np.concatenate([np.asarray(K, np.float64).ravel(), np.asarray(R, np.float64).ravel(),
+                           np.asarray(t, np.float64).ravel()])
+
+
+def setup_views(ref_cam, src_cams):
+    """(kinv[9], ab[S,12]) float32 exactly as the reference computes them."""
+    r = _krt(ref_cam)
+    s = np.concatenate([_krt(c) for c in src_cams])
+    kinv = np.empty(9, np.float32)
+    ab = np.empty((len(src_cams), 12), np.float32)
+    assert lib().pmref_setup_views(_p(r), _p(s), len(src_cams), _p(kinv), _p(ab)) == 0
+    return kinv, ab
+
+
+class _Images:
+    def __init__(self, ref, srcs):
+        self.ref = np.ascontiguousarray(ref, np.float32)
+        self.srcs = [np.ascontiguousarray(s, np.float32) for s in srcs]
+        self.ptrs = (C.c_void_p * len(self.srcs))(*[s.ctypes.data for s in self.srcs])
+
+
+def ncc_cost(ref, srcs, kinv, ab, depth, normal, radius, kernel="ncc"):
+    """compute_ncc_cost_kernel ('ncc', radius <= 5) or computePixelCost ('pixel') on fixed maps."""
+    im = _Images(ref, srcs)
+    h, w = im.ref.shape
+    cost = np.empty((h, w), np.float32)
+    fn = lib().pmref_ncc_cost if kernel == "ncc" else lib().pmref_pixel_cost
+    kinv = np.ascontiguousarray(kinv, np.float32)
+    ab = np.ascontiguousarray(ab, np.float32)
+    depth = np.ascontiguousarray(depth, np.float32)
+    normal = np.ascontiguousarray(normal, np.float32)
+    st = fn(_p(im.ref), C.cast(im.ptrs, C.c_void_p), len(im.srcs), w, h, _p(kinv), _p(ab), _p(depth), _p(normal),
+            radius, _p(cost))
+    assert st == 0, st
+    return cost
+
+
+def solve_view(ref, srcs, kinv, ab, dmin, dmax, radius, iterations, ref_id):
+    """The reference's per-view solve; returns (depth, normal, cost, gpu_ms)."""
+    im = _Images(ref, srcs)
+    h, w = im.ref.shape
+    depth = np.empty((h, w), np.float32)
+    normal = np.empty((h, w, 3), np.float32)
+    cost = np.empty((h, w), np.float32)
+    ms = C.c_float()
+    kinv = np.ascontiguousarray(kinv, np.float32)
+    ab = np.ascontiguousarray(ab, np.float32)
+    st = lib().pmref_solve_view(_p(im.ref), C.cast(im.ptrs, C.c_void_p), len(im.srcs), w, h, _p(kinv), _p(ab), dmin,
+                                dmax, radius, iterations, ref_id, _p(depth), _p(normal), _p(cost), C.byref(ms))
+    assert st == 0, st
+    return depth, normal, cost, ms.value
+
+
+def geometric_filter(ref_cam, depth, normal, conf, src_cams, src_depths, src_normals, depth_tol=0.12,
+                     normal_tol_cos=-1.0, min_consistent=2):
+    """In place on depth / conf."""
+    S = len(src_cams)
+    h, w = depth.shape
+    r = _krt(ref_cam)
+    s = np.concatenate([_krt(c) for c in src_cams])
+    sd = np.ascontiguousarray(np.stack(src_depths), np.float32)
+    sn = np.ascontiguousarray(np.stack(src_normals), np.float32)
+    assert lib().pmref_geometric_filter(_p(depth), _p(np.ascontiguousarray(normal, np.float32)), _p(conf), _p(r),
+                                        _p(sd), _p(sn), _p(s), S, w, h, depth_tol, normal_tol_cos,
+                                        min_consistent) == 0
