@@ -1,0 +1,417 @@
+#!/usr/bin/env python
+"""Headline benchmark: depth-map Mpix*iter/s of the PatchMatch engine on B200.
+
+Workload (one "step"): the multi-object scene - 20 reference views of
+1920x1080 u8 images, 6 sources each, 15x15 window sampled at stride 2, 12
+red-black iterations, depth range [1, 6] m - solved in one batched hp_solve
+(random init, initial cost, 24 half-pass launches over all 20 views).
+Units per step = 20 * 1920 * 1080 * 12 = 497.7 Mpix*iter.
+
+  value  device-resident: images uploaded once, outputs in device memory,
+         K steps timed with CUDA events on the engine's stream.
+  e2e    through the public API with host buffers: every step uploads the 20
+         images from pinned host memory and reads depth, normal and cost of
+         every view back to pinned host memory.
+
+Inputs (20 x 2.07 Mpix images, 20 x 41 MB of state) exceed the 126 MB L2, so
+no flush between steps is needed.  Multi-GPU (torchrun): views are
+independent, each rank solves its own 20-view batch (weak scaling, no
+collective on the data path); the step time is the max over ranks.
+
+--impl reference times the reference's algorithm on the host cores (the CPU
+restatement in oracle/, all threads): one red-black iteration of a band of
+rows of one view of the same workload per step.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [ROOT, os.path.join(ROOT, "oracle"), os.path.join(ROOT, "oracle", "ref_harness")]
+PKG = "hemiphoto3d-private_b200"
+
+WORKLOAD = dict(name="multi_object_20x1920x1080", views=20, width=1920, height=1080, sources=6, radius=7, stride=2,
+                iterations=12, depth_range=[1.0, 6.0], image_dtype="u8")
+METRIC = "depth-map Mpix*iter/s on 1 B200 (FP16-acc vs plain FP32)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
+    ap.add_argument("--precision", choices=["f32", "f16acc"], default="f32",
+                    help="headline arithmetic; the other is measured too and reported under 'variants'")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-rows", type=int, default=256, help="rows of the CPU-baseline band sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-variants", action="store_true")
+    ap.add_argument("--views", type=int, default=WORKLOAD["views"], help="reduce for profiling captures only")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi sampling (200 ms) during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait(timeout=5)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ------------------------------------------------------------------------------------------------
+def build_scene(views: int):
+    scene = importlib.import_module(PKG + ".scene")
+    return scene.multi_object(n_views=max(views, WORKLOAD["sources"] + 1), n_refs=views)
+
+
+def cpu_sample(s, rows: int, reps: int = 1):
+    """Time one red-black iteration of a band of `rows` rows of view 0 on all host threads.
+    Returns (Mpix*iter/s, seconds, threads, sample description)."""
+    import pm_oracle as po
+    r = 0
+    srcs = s.sources[r]
+    cam = lambda i: (s.views[i].cam.K, s.views[i].cam.R, s.views[i].cam.t)
+    v = po.View(s.views[r].image_f32, [s.views[i].image_f32 for i in srcs], radius=WORKLOAD["radius"],
+                stride=WORKLOAD["stride"], ref_cam=cam(r), src_cams=[cam(i) for i in srcs])
+    H, W = s.views[r].image.shape
+    y0 = (H - rows) // 2
+    dmin, dmax = WORKLOAD["depth_range"]
+    d, n = v.init(dmin, dmax, 42, r)
+    c = np.zeros((H, W), np.float32)
+    v.cost_rows_f32(d, n, c, y0, y0 + rows)
+    best = None
+    for it in range(reps):
+        t = time.perf_counter()
+        v.propagate_rows(d, n, c, dmin, dmax, it, 0, 42, r, y0, y0 + rows)
+        v.propagate_rows(d, n, c, dmin, dmax, it, 1, 42, r, y0, y0 + rows)
+        dt = time.perf_counter() - t
+        best = dt if best is None else min(best, dt)
+    mpix = rows * W / 1e6
+    return mpix / best, best, po.num_threads(), (f"1 red-black iteration of rows [{y0},{y0 + rows}) x {W} of view 0 "
+                                                 f"(r=7, s=2, S=6), {po.num_threads()} threads")
+
+
+def measure_peaks():
+    """On-chip ceilings measured live (lib/libhppeaks.so)."""
+    import ctypes as C
+    path = os.path.join(ROOT, PKG, "lib", "libhppeaks.so")
+    L = C.CDLL(path)
+    out = {}
+    for name, fn, args in [("tex_f32_fetch_per_s", "hpk_tex_fetch_rate", (0,)),
+                           ("tex_f16_fetch_per_s", "hpk_tex_fetch_rate", (1,)),
+                           ("smem_bytes_per_s", "hpk_smem_read_rate", ()), ("fma_per_s", "hpk_fma_rate", ())]:
+        v = C.c_double()
+        f = getattr(L, fn)
+        f.restype = C.c_int
+        rc = f(*args, C.byref(v))
+        out[name] = v.value if rc == 0 else None
+    return out
+
+
+def load_ncu_traffic(kind: str):
+    """DRAM bytes per propagate launch from the committed ncu summary, scaled to this workload."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if not os.path.exists(p):
+        return None
+    try:
+        d = json.load(open(p))
+        e = d.get(kind)
+        return None if e is None else float(e["dram_bytes_per_pixel_visit"])
+    except (ValueError, KeyError, TypeError):
+        return None
+
+
+# ------------------------------------------------------------------------------------------------
+def run_engine(args, rank, world, local_rank):
+    import torch
+    hp = importlib.import_module(PKG)
+    torch.cuda.set_device(local_rank)
+    s = build_scene(args.views)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    H, W = WORKLOAD["height"], WORKLOAD["width"]
+    n_views = args.views
+    units_per_step = n_views * H * W * WORKLOAD["iterations"] / 1e6  # Mpix*iter per rank
+
+    ctx = hp.Context(local_rank)
+    stream = torch.cuda.ExternalStream(ctx.stream_handle, device=local_rank)
+    ids = [ctx.upload(v.image) for v in s.views]
+
+    def make_jobs(id_list):
+        jobs = []
+        for r in range(n_views):
+            srcs = s.sources[r]
+            cam = lambda i: hp.make_camera(s.views[i].cam.K, s.views[i].cam.R, s.views[i].cam.t)
+            jobs.append(hp.make_job(id_list[r], [id_list[i] for i in srcs], cam(r), [cam(i) for i in srcs],
+                                    *WORKLOAD["depth_range"], seed=42 + 1_000_003 * rank,
+                                    view_id=r + 1000 * rank, iterations=WORKLOAD["iterations"]))
+        return jobs
+
+    jobs = make_jobs(ids)
+    dev_maps = []
+    for _ in range(n_views):
+        d = torch.empty(H, W, device="cuda")
+        n = torch.empty(H, W, 3, device="cuda")
+        c = torch.empty(H, W, device="cuda")
+        dev_maps.append(hp.maps_of(d, n, c))
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    def timed(precision, steps, warmup):
+        params = hp.default_params(radius=WORKLOAD["radius"], stride=WORKLOAD["stride"],
+                                   precision=hp.PRECISION_F16ACC if precision == "f16acc" else hp.PRECISION_F32)
+        for _ in range(warmup):
+            ctx.solve(jobs, params, dev_maps)
+        ctx.profile_reset()
+        ctx.set_profiling(True)
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local_rank) as clk:
+            e0.record(stream)
+            for _ in range(steps):
+                ctx.solve(jobs, params, dev_maps)
+            e1.record(stream)
+            e1.synchronize()
+        barrier()
+        ctx.set_profiling(False)
+        ms = e0.elapsed_time(e1)
+        prof = ctx.profile()
+        if dist is not None:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, prof, clk.summary()
+
+    head = args.precision
+    other = "f16acc" if head == "f32" else "f32"
+    ms, prof, clocks = timed(head, args.steps, args.warmup)
+    variants = {}
+    if not args.no_variants:
+        ms2, prof2, clocks2 = timed(other, args.steps, max(1, args.warmup))
+        variants[other] = {"value": world * units_per_step * args.steps / (ms2 / 1e3), "ms_per_step": ms2 / args.steps,
+                           "propagate_ms_per_launch": prof2["propagate"]["device_ms"] / max(1, prof2["propagate"]["timed"]),
+                           "clocks": clocks2}
+
+    # ---- end to end through the public API with pinned host buffers
+    pinned_imgs = [torch.from_numpy(v.image).pin_memory() for v in s.views]
+    host_out = [(torch.empty(H, W).pin_memory(), torch.empty(H, W, 3).pin_memory(), torch.empty(H, W).pin_memory())
+                for _ in range(n_views)]
+    params = hp.default_params(radius=WORKLOAD["radius"], stride=WORKLOAD["stride"],
+                               precision=hp.PRECISION_F16ACC if head == "f16acc" else hp.PRECISION_F32)
+
+    def host_maps(t3):
+        m = hp.Maps(hp.MEMORY_HOST, t3[0].data_ptr(), t3[1].data_ptr(), t3[2].data_ptr())
+        m.arrays = t3
+        return m
+
+    outs_h = [host_maps(t) for t in host_out]
+
+    def upload_pinned(t):
+        import ctypes as C
+        iid = C.c_int()
+        st = hp.lib.hp_image_upload(ctx.handle, t.data_ptr(), hp.MEMORY_HOST, W, H, hp.DTYPE_U8, C.byref(iid))
+        if st != 0:
+            raise hp.HpError(st, "hp_image_upload")
+        return iid.value
+
+    def e2e_step():
+        step_ids = [upload_pinned(t) for t in pinned_imgs]
+        ctx.solve(make_jobs(step_ids), params, outs_h)
+        for i in step_ids:
+            ctx.release(i)
+
+    e2e_step()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.e2e_steps):
+        e2e_step()
+    e1.record(stream)
+    e1.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    barrier()
+    h2d = sum(int(t.numel()) for t in pinned_imgs)
+    d2h = n_views * H * W * (4 + 12 + 4)
+
+    if rank != 0:
+        ctx.close()
+        return None
+
+    # ---- roofline of the dominant kernel (the propagate half-pass)
+    prop_launches = prof["propagate"]["timed"]
+    prop_ms = prof["propagate"]["device_ms"] / max(1, prop_launches)
+    visits = n_views * H * W / 2  # pixel visits per half-pass launch
+    S, N_w = WORKLOAD["sources"], ((2 * WORKLOAD["radius"]) // WORKLOAD["stride"] + 1) ** 2
+    taps_per_visit = 6 * S * N_w  # 4 neighbour + 2 refinement candidates, S sources, N_w taps
+    b_img = 2 if head == "f16acc" else 4
+    # compulsory DRAM bytes per visit: own plane+cost read & write (40), neighbour planes (16),
+    # reference and source images once per launch ((1+S) * 2 visits' worth of pixels * b_img)
+    hbm_bytes_per_visit = 40 + 16 + 2 * (1 + S) * b_img
+    peaks_meas = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    hbm_peak = peaks_meas.get("hbm_gbs")
+    hbm_src = "measured" if hbm_peak else "fallback"
+    hbm_peak = hbm_peak or 6650.0
+    achieved_hbm = visits * hbm_bytes_per_visit / (prop_ms * 1e-3) / 1e9
+    traffic_per_visit = load_ncu_traffic(head)
+    onchip = measure_peaks()
+    tex_peak = onchip.get("tex_f16_fetch_per_s" if head == "f16acc" else "tex_f32_fetch_per_s")
+    fetch_rate = visits * taps_per_visit / (prop_ms * 1e-3)
+    fma_peak = onchip.get("fma_per_s")
+
+    value = world * units_per_step * args.steps / (ms / 1e3)
+    line = {
+        "metric": METRIC,
+        "value": round(value, 2),
+        "unit": "Mpix*iter/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms / args.steps, 3),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f16acc" if head == "f16acc" else "f32",
+        "data": "synthetic: seeded planes+spheres scene, renderer ground truth (no dataset)",
+        "config": {"workload": WORKLOAD["name"], "views_per_gpu": n_views, "width": W, "height": H,
+                   "sources": S, "window": f"{2 * WORKLOAD['radius'] + 1}x{2 * WORKLOAD['radius'] + 1}",
+                   "stride": WORKLOAD["stride"], "iterations": WORKLOAD["iterations"],
+                   "depth_range": WORKLOAD["depth_range"], "images": "u8", "parallelism": f"views/{world} ranks",
+                   "mpix_iter_per_step": round(units_per_step * world, 3),
+                   "l2": "inputs larger than L2 (20 x 2.07 Mpix images + 830 MB state per step), no flush"},
+        "e2e": {"value": round(world * units_per_step * args.e2e_steps / (e2e_ms / 1e3), 2), "unit": "Mpix*iter/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": args.e2e_steps},
+        "roofline": {"bound": "hbm", "achieved": round(achieved_hbm, 2), "peak": hbm_peak, "unit": "GB/s",
+                     "frac": round(achieved_hbm / hbm_peak, 5), "peak_source": hbm_src,
+                     "traffic": None if traffic_per_visit is None else round(traffic_per_visit * visits),
+                     "kernel": "propagate half-pass", "ms_per_launch": round(prop_ms, 4),
+                     "algorithmic_bytes_per_launch": int(visits * hbm_bytes_per_visit),
+                     "note": "compulsory DRAM bytes; HBM does not bind this kernel - see roofline_tex"},
+        "roofline_tex": {"bound": "texture-filter fetches", "achieved": round(fetch_rate / 1e9, 2),
+                         "peak": None if tex_peak is None else round(tex_peak / 1e9, 2), "unit": "Gfetch/s",
+                         "frac": None if not tex_peak else round(fetch_rate / tex_peak, 4),
+                         "peak_source": "measured live (L1-resident bilinear fetch microbenchmark)",
+                         "algorithmic_fetches_per_launch": int(visits * taps_per_visit)},
+        "roofline_fp32": {"achieved_fma_equiv": None if fma_peak is None else round(fetch_rate * 14 / 1e12, 3),
+                          "peak_fma": None if fma_peak is None else round(fma_peak / 1e12, 3), "unit": "TFMA/s",
+                          "note": "~14 FMA-equivalent issue slots per tap on the FP32 path (28 ops)"},
+        "onchip_peaks": onchip,
+        "gpu_launches": int(sum(v["launches"] for v in prof.values())),
+        "kernel_launches": {k: v["launches"] for k, v in prof.items()},
+        "clocks": clocks,
+        "variants": variants,
+    }
+    # CPU baseline (rank 0, N = 1)
+    if world == 1 and not args.no_cpu_baseline:
+        rate, secs, thr, desc = cpu_sample(s, args.cpu_rows)
+        line["cpu_baseline"] = {"value": round(rate, 4), "unit": "Mpix*iter/s", "cores": thr, "kind": "port",
+                                "sample": desc, "seconds": round(secs, 2)}
+    ctx.close()
+    return line
+
+
+def run_reference(args, rank, world):
+    """The reference's algorithm on the host cores (CPU restatement, all threads)."""
+    if rank != 0:
+        return None
+    s = build_scene(1)
+    rates = []
+    desc = thr = None
+    for i in range(args.warmup + args.steps):
+        rate, secs, thr, desc = cpu_sample(s, args.cpu_rows)
+        if i >= args.warmup:
+            rates.append(rate)
+    v = float(np.median(rates))
+    return {
+        "impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": "Mpix*iter/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic: seeded planes+spheres scene",
+        "config": {"workload": WORKLOAD["name"], "sources": WORKLOAD["sources"], "window": "15x15", "stride": 2,
+                   "images": "u8"},
+        "cpu_baseline": {"value": round(v, 4), "unit": "Mpix*iter/s", "cores": thr, "kind": "port", "sample": desc},
+        "e2e": {"value": round(v, 4), "unit": "Mpix*iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != args.gpus:
+        print(f"warning: --gpus {args.gpus} but WORLD_SIZE {world}", file=sys.stderr)
+    if args.impl == "reference":
+        line = run_reference(args, rank, world)
+        if line:
+            print(json.dumps(line))
+        return
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        line = run_engine(args, rank, world, local_rank)
+        if line:
+            print(json.dumps(line))
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

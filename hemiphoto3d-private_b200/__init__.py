@@ -66,6 +66,17 @@ class Maps(C.Structure):
     _fields_ = [("memory", C.c_int), ("depth", C.c_void_p), ("normal", C.c_void_p), ("cost", C.c_void_p)]
 
 
+KERNEL_KINDS = ("init", "cost", "propagate", "other")
+
+
+class Profile(C.Structure):
+    _fields_ = [("launches", C.c_uint64 * 4), ("device_ms", C.c_double * 4), ("timed", C.c_uint64 * 4)]
+
+    def as_dict(self):
+        return {k: {"launches": int(self.launches[i]), "device_ms": float(self.device_ms[i]),
+                    "timed": int(self.timed[i])} for i, k in enumerate(KERNEL_KINDS)}
+
+
 def _load() -> C.CDLL:
     if not os.path.exists(LIB_PATH):
         raise ImportError(
@@ -81,6 +92,10 @@ def _load() -> C.CDLL:
         "hp_ctx_last_error": (C.c_char_p, [C.c_void_p]),
         "hp_ctx_synchronize": (C.c_int, [C.c_void_p]),
         "hp_ctx_mem_info": (C.c_int, [C.c_void_p, P(C.c_size_t), P(C.c_size_t)]),
+        "hp_ctx_stream": (C.c_int, [C.c_void_p, P(C.c_void_p)]),
+        "hp_ctx_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
+        "hp_ctx_profile": (C.c_int, [C.c_void_p, P(Profile)]),
+        "hp_ctx_profile_reset": (C.c_int, [C.c_void_p]),
         "hp_image_upload": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, P(C.c_int)]),
         "hp_image_release": (C.c_int, [C.c_void_p, C.c_int]),
         "hp_image_size": (C.c_int, [C.c_void_p, C.c_int, P(C.c_int), P(C.c_int)]),
@@ -107,7 +122,8 @@ lib = _load()
 #: Every exported entry point of include/hpmvs.h (checked against the .so by the tests).
 EXPORTS = (
     "hp_status_string", "hp_params_default", "hp_version", "hp_ctx_create", "hp_ctx_destroy",
-    "hp_ctx_last_error", "hp_ctx_synchronize", "hp_ctx_mem_info", "hp_image_upload", "hp_image_release",
+    "hp_ctx_last_error", "hp_ctx_synchronize", "hp_ctx_mem_info", "hp_ctx_stream", "hp_ctx_set_profiling",
+    "hp_ctx_profile", "hp_ctx_profile_reset", "hp_image_upload", "hp_image_release",
     "hp_image_size", "hp_setup_homographies", "hp_solve", "hp_init_hypotheses", "hp_ncc_cost",
     "hp_propagate_pass", "hp_geometric_filter", "hp_pfm_write", "hp_pfm_read",
 )
@@ -200,6 +216,24 @@ class Context:
         f, t = C.c_size_t(), C.c_size_t()
         self._check(lib.hp_ctx_mem_info(self._h, C.byref(f), C.byref(t)), "hp_ctx_mem_info")
         return f.value, t.value
+
+    @property
+    def stream_handle(self) -> int:
+        """The context's cudaStream_t as an integer (e.g. for torch.cuda.ExternalStream)."""
+        s = C.c_void_p()
+        self._check(lib.hp_ctx_stream(self._h, C.byref(s)), "hp_ctx_stream")
+        return s.value or 0
+
+    def set_profiling(self, on: bool):
+        self._check(lib.hp_ctx_set_profiling(self._h, int(bool(on))), "hp_ctx_set_profiling")
+
+    def profile(self) -> dict:
+        p = Profile()
+        self._check(lib.hp_ctx_profile(self._h, C.byref(p)), "hp_ctx_profile")
+        return p.as_dict()
+
+    def profile_reset(self):
+        self._check(lib.hp_ctx_profile_reset(self._h), "hp_ctx_profile_reset")
 
     def upload(self, img) -> int:
         """Upload a grayscale image (numpy u8/f16/f32 on host, or a contiguous torch CUDA tensor)."""

@@ -67,9 +67,49 @@ struct hp_ctx {
     DevBuf descs;   // ViewDesc array
     DevBuf lists;   // active-view lists and tile prefixes
     DevBuf staging; // host-memory results pass through here
+    // Profiler: launch counts always; with profiling on, CUDA events bracket
+    // each launch and are read back at the next synchronisation point.
+    bool profiling = false;
+    hp_profile prof{};
+    std::vector<cudaEvent_t> events;
+    std::vector<std::pair<int, size_t>> pending;  // (kind, index of the start event)
+    size_t events_used = 0;
 };
 
 namespace {
+
+// Run one launch, counted under `kind` and, when profiling, bracketed by events.
+template <class F>
+cudaError_t counted(hp_ctx* ctx, int kind, F&& launch) {
+    ctx->prof.launches[kind]++;
+    if (!ctx->profiling) return launch();
+    while (ctx->events.size() < ctx->events_used + 2) {
+        cudaEvent_t e;
+        cudaError_t err = cudaEventCreate(&e);
+        if (err != cudaSuccess) return err;
+        ctx->events.push_back(e);
+    }
+    const size_t i = ctx->events_used;
+    ctx->events_used += 2;
+    cudaEventRecord(ctx->events[i], ctx->stream);
+    cudaError_t err = launch();
+    cudaEventRecord(ctx->events[i + 1], ctx->stream);
+    ctx->pending.emplace_back(kind, i);
+    return err;
+}
+
+// Fold completed event pairs into the profile (call after a stream sync).
+void flush_profile(hp_ctx* ctx) {
+    for (auto& pk : ctx->pending) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, ctx->events[pk.second], ctx->events[pk.second + 1]) == cudaSuccess) {
+            ctx->prof.device_ms[pk.first] += ms;
+            ctx->prof.timed[pk.first]++;
+        }
+    }
+    ctx->pending.clear();
+    ctx->events_used = 0;
+}
 
 hp_status fail(hp_ctx* c, hp_status s, const char* fmt, ...) {
     if (c) {
@@ -266,6 +306,7 @@ hp_status prepare(hp_ctx* ctx, const hp_job* jobs, int n, Prepared* P) {
                             ctx->stream));
     // The staging vectors above are pageable: the copies complete before return.
     HP_CUDA(cudaStreamSynchronize(ctx->stream));
+    flush_profile(ctx);
     return HP_OK;
 }
 
@@ -287,19 +328,22 @@ hp_status export_maps(hp_ctx* ctx, const Prepared& P, int k, hp_maps* m, bool wa
     float* nrm = want_depth_normal ? m->normal : nullptr;
     float* c = want_cost ? m->cost : nullptr;
     if (m->memory == HP_MEMORY_DEVICE) {
-        HP_CUDA(hp::launch_unpack(P.host.data(), k, d, nrm, c, ctx->stream));
+        HP_CUDA(counted(ctx, HP_KERNEL_OTHER, [&] { return hp::launch_unpack(P.host.data(), k, d, nrm, c, ctx->stream); }));
         return HP_OK;
     }
     HP_CUDA(ctx->staging.ensure(px * 5 * sizeof(float)));
     float* sd = static_cast<float*>(ctx->staging.p);
     float* sn = sd + px;
     float* sc = sn + 3 * px;
-    HP_CUDA(hp::launch_unpack(P.host.data(), k, d ? sd : nullptr, nrm ? sn : nullptr, c ? sc : nullptr,
-                              ctx->stream));
+    HP_CUDA(counted(ctx, HP_KERNEL_OTHER, [&] {
+        return hp::launch_unpack(P.host.data(), k, d ? sd : nullptr, nrm ? sn : nullptr, c ? sc : nullptr,
+                                 ctx->stream);
+    }));
     if (d) HP_CUDA(cudaMemcpyAsync(d, sd, px * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
     if (nrm) HP_CUDA(cudaMemcpyAsync(nrm, sn, 3 * px * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
     if (c) HP_CUDA(cudaMemcpyAsync(c, sc, px * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
     HP_CUDA(cudaStreamSynchronize(ctx->stream));
+    flush_profile(ctx);
     return HP_OK;
 }
 
@@ -310,7 +354,9 @@ hp_status import_maps(hp_ctx* ctx, const Prepared& P, int k, const hp_maps* m, b
     if (!m->depth || !m->normal || (with_cost && !m->cost))
         return fail(ctx, HP_ERR_INVALID_ARG, "maps: depth/normal%s pointer is null", with_cost ? "/cost" : "");
     if (m->memory == HP_MEMORY_DEVICE) {
-        HP_CUDA(hp::launch_pack(P.host.data(), k, m->depth, m->normal, with_cost ? m->cost : nullptr, ctx->stream));
+        HP_CUDA(counted(ctx, HP_KERNEL_OTHER, [&] {
+            return hp::launch_pack(P.host.data(), k, m->depth, m->normal, with_cost ? m->cost : nullptr, ctx->stream);
+        }));
         return HP_OK;
     }
     HP_CUDA(ctx->staging.ensure(px * 5 * sizeof(float)));
@@ -320,23 +366,29 @@ hp_status import_maps(hp_ctx* ctx, const Prepared& P, int k, const hp_maps* m, b
     HP_CUDA(cudaMemcpyAsync(sd, m->depth, px * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
     HP_CUDA(cudaMemcpyAsync(sn, m->normal, 3 * px * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
     if (with_cost) HP_CUDA(cudaMemcpyAsync(sc, m->cost, px * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
-    HP_CUDA(hp::launch_pack(P.host.data(), k, sd, sn, with_cost ? sc : nullptr, ctx->stream));
+    HP_CUDA(counted(ctx, HP_KERNEL_OTHER,
+                    [&] { return hp::launch_pack(P.host.data(), k, sd, sn, with_cost ? sc : nullptr, ctx->stream); }));
     HP_CUDA(cudaStreamSynchronize(ctx->stream));
+    flush_profile(ctx);
     return HP_OK;
 }
 
 hp_status launch_cost(hp_ctx* ctx, const hp::BatchList& bl, const hp_params* p) {
     hp::SolveConsts sc = consts_of(p);
-    cudaError_t e = p->precision == HP_PRECISION_F16ACC ? hp::launch_cost_f16(bl, sc, ctx->stream)
-                                                        : hp::launch_cost_f32(bl, sc, ctx->stream);
+    cudaError_t e = counted(ctx, HP_KERNEL_COST, [&] {
+        return p->precision == HP_PRECISION_F16ACC ? hp::launch_cost_f16(bl, sc, ctx->stream)
+                                                   : hp::launch_cost_f32(bl, sc, ctx->stream);
+    });
     HP_CUDA(e);
     return HP_OK;
 }
 
 hp_status launch_pass(hp_ctx* ctx, const hp::BatchList& bl, const hp_params* p, int it, int color) {
     hp::SolveConsts sc = consts_of(p);
-    cudaError_t e = p->precision == HP_PRECISION_F16ACC ? hp::launch_propagate_f16(bl, sc, it, color, ctx->stream)
-                                                        : hp::launch_propagate_f32(bl, sc, it, color, ctx->stream);
+    cudaError_t e = counted(ctx, HP_KERNEL_PROPAGATE, [&] {
+        return p->precision == HP_PRECISION_F16ACC ? hp::launch_propagate_f16(bl, sc, it, color, ctx->stream)
+                                                   : hp::launch_propagate_f32(bl, sc, it, color, ctx->stream);
+    });
     HP_CUDA(e);
     return HP_OK;
 }
@@ -428,6 +480,7 @@ hp_status hp_ctx_destroy(hp_ctx* ctx) {
         ctx->descs.release();
         ctx->lists.release();
         ctx->staging.release();
+        for (cudaEvent_t e : ctx->events) cudaEventDestroy(e);
         cudaStreamDestroy(ctx->stream);
     }
     delete ctx;
@@ -440,6 +493,7 @@ hp_status hp_ctx_synchronize(hp_ctx* ctx) {
     if (!ctx) return HP_ERR_INVALID_ARG;
     DeviceGuard g(ctx->device);
     HP_CUDA(cudaStreamSynchronize(ctx->stream));
+    flush_profile(ctx);
     return HP_OK;
 }
 
@@ -447,6 +501,39 @@ hp_status hp_ctx_mem_info(hp_ctx* ctx, size_t* free_bytes, size_t* total_bytes) 
     if (!ctx || !free_bytes || !total_bytes) return HP_ERR_INVALID_ARG;
     DeviceGuard g(ctx->device);
     HP_CUDA(cudaMemGetInfo(free_bytes, total_bytes));
+    return HP_OK;
+}
+
+hp_status hp_ctx_stream(hp_ctx* ctx, void** stream) {
+    if (!ctx || !stream) return HP_ERR_INVALID_ARG;
+    *stream = static_cast<void*>(ctx->stream);
+    return HP_OK;
+}
+
+hp_status hp_ctx_set_profiling(hp_ctx* ctx, int enable) {
+    if (!ctx) return HP_ERR_INVALID_ARG;
+    DeviceGuard g(ctx->device);
+    HP_CUDA(cudaStreamSynchronize(ctx->stream));
+    flush_profile(ctx);
+    ctx->profiling = enable != 0;
+    return HP_OK;
+}
+
+hp_status hp_ctx_profile(hp_ctx* ctx, hp_profile* out) {
+    if (!ctx || !out) return HP_ERR_INVALID_ARG;
+    DeviceGuard g(ctx->device);
+    HP_CUDA(cudaStreamSynchronize(ctx->stream));
+    flush_profile(ctx);
+    *out = ctx->prof;
+    return HP_OK;
+}
+
+hp_status hp_ctx_profile_reset(hp_ctx* ctx) {
+    if (!ctx) return HP_ERR_INVALID_ARG;
+    DeviceGuard g(ctx->device);
+    HP_CUDA(cudaStreamSynchronize(ctx->stream));
+    flush_profile(ctx);
+    ctx->prof = hp_profile{};
     return HP_OK;
 }
 
@@ -489,8 +576,10 @@ hp_status hp_image_upload(hp_ctx* ctx, const void* data, int memory, int width, 
     }
     HP_UP(cudaMallocPitch(reinterpret_cast<void**>(&im.f32), &im.pitch32, width * sizeof(float), height));
     HP_UP(cudaMallocPitch(reinterpret_cast<void**>(&im.f16), &im.pitch16, width * sizeof(__half), height));
-    HP_UP(hp::launch_to_f32(src, dtype, width, height, im.f32, static_cast<int>(im.pitch32 / sizeof(float)), im.f16,
-                            static_cast<int>(im.pitch16 / sizeof(__half)), ctx->stream));
+    HP_UP(counted(ctx, HP_KERNEL_OTHER, [&] {
+        return hp::launch_to_f32(src, dtype, width, height, im.f32, static_cast<int>(im.pitch32 / sizeof(float)),
+                                 im.f16, static_cast<int>(im.pitch16 / sizeof(__half)), ctx->stream);
+    }));
     cudaChannelFormatDesc d32 = cudaCreateChannelDesc<float>();
     cudaChannelFormatDesc d16 = cudaCreateChannelDescHalf();
     HP_UP(cudaMallocArray(&im.arr32, &d32, width, height));
@@ -565,7 +654,7 @@ hp_status hp_solve(hp_ctx* ctx, const hp_job* jobs, int num_jobs, const hp_param
     Prepared P;
     if ((st = prepare(ctx, jobs, num_jobs, &P)) != HP_OK) return st;
     hp::BatchList all = batch_of(P, 0);
-    HP_CUDA(hp::launch_init(all, ctx->stream));
+    HP_CUDA(counted(ctx, HP_KERNEL_INIT, [&] { return hp::launch_init(all, ctx->stream); }));
     if ((st = launch_cost(ctx, all, params)) != HP_OK) return st;
     for (int it = 0; it < P.max_iter; ++it) {
         hp::BatchList bl = batch_of(P, 1 + it);
@@ -575,6 +664,7 @@ hp_status hp_solve(hp_ctx* ctx, const hp_job* jobs, int num_jobs, const hp_param
     for (int k = 0; k < num_jobs; ++k)
         if ((st = export_maps(ctx, P, k, &out[k], true, true)) != HP_OK) return st;
     HP_CUDA(cudaStreamSynchronize(ctx->stream));
+    flush_profile(ctx);
     return HP_OK;
 }
 
@@ -586,9 +676,10 @@ hp_status hp_init_hypotheses(hp_ctx* ctx, const hp_job* job, const hp_params* pa
     DeviceGuard g(ctx->device);
     Prepared P;
     if ((st = prepare(ctx, job, 1, &P)) != HP_OK) return st;
-    HP_CUDA(hp::launch_init(batch_of(P, 0), ctx->stream));
+    HP_CUDA(counted(ctx, HP_KERNEL_INIT, [&] { return hp::launch_init(batch_of(P, 0), ctx->stream); }));
     if ((st = export_maps(ctx, P, 0, out, true, false)) != HP_OK) return st;
     HP_CUDA(cudaStreamSynchronize(ctx->stream));
+    flush_profile(ctx);
     return HP_OK;
 }
 
@@ -604,6 +695,7 @@ hp_status hp_ncc_cost(hp_ctx* ctx, const hp_job* job, const hp_params* params, h
     if ((st = launch_cost(ctx, batch_of(P, 0), params)) != HP_OK) return st;
     if ((st = export_maps(ctx, P, 0, maps, false, true)) != HP_OK) return st;
     HP_CUDA(cudaStreamSynchronize(ctx->stream));
+    flush_profile(ctx);
     return HP_OK;
 }
 
@@ -622,6 +714,7 @@ hp_status hp_propagate_pass(hp_ctx* ctx, const hp_job* job, const hp_params* par
     if ((st = launch_pass(ctx, batch_of(P, 0), params, iteration, color)) != HP_OK) return st;
     if ((st = export_maps(ctx, P, 0, maps, true, true)) != HP_OK) return st;
     HP_CUDA(cudaStreamSynchronize(ctx->stream));
+    flush_profile(ctx);
     return HP_OK;
 }
 
@@ -665,7 +758,8 @@ hp_status hp_geometric_filter(hp_ctx* ctx, const hp_camera* ref_cam, int width, 
             a.src_depth[s] = src_depths[s];
             a.src_normal[s] = src_normals[s];
         }
-        HP_CUDA(hp::launch_geometric_filter(a, depth, normal, confidence, ctx->stream));
+        HP_CUDA(counted(ctx, HP_KERNEL_OTHER,
+                        [&] { return hp::launch_geometric_filter(a, depth, normal, confidence, ctx->stream); }));
         HP_CUDA(cudaStreamSynchronize(ctx->stream));
         return HP_OK;
     }
@@ -686,10 +780,11 @@ hp_status hp_geometric_filter(hp_ctx* ctx, const hp_camera* ref_cam, int width, 
         a.src_depth[s] = dd;
         a.src_normal[s] = dd + px;
     }
-    HP_CUDA(hp::launch_geometric_filter(a, sd, sn, sc, ctx->stream));
+    HP_CUDA(counted(ctx, HP_KERNEL_OTHER, [&] { return hp::launch_geometric_filter(a, sd, sn, sc, ctx->stream); }));
     HP_CUDA(cudaMemcpyAsync(depth, sd, px * 4, cudaMemcpyDeviceToHost, ctx->stream));
     HP_CUDA(cudaMemcpyAsync(confidence, sc, px * 4, cudaMemcpyDeviceToHost, ctx->stream));
     HP_CUDA(cudaStreamSynchronize(ctx->stream));
+    flush_profile(ctx);
     return HP_OK;
 }
 

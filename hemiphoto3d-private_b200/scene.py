@@ -12,7 +12,7 @@ Workloads (all sizes, counts and ranges as stated):
   plane_sphere   5 views 640x480 u8, fx 500; plane z=3 + sphere r=0.5 at z=2.5;
                  2 m arc, 10 deg spacing; depth [1, 4]; r=5, s=2, S=4, 8 iterations
   multi_object   20 views 1920x1080 u8, fx 1500; 3 spheres + 2 tilted planes
-                 (seeded) before a background plane; arc +-30 deg; depth [1, 6];
+                 (seeded) before a background plane at z=4.5; arc +-30 deg; depth [1, 6];
                  r=7, s=2, S=6, 12 iterations
   precision      32 views 3000x2000 FP16 + N(0, 0.01), fx 2400, multi_object
                  layout; r=7, S=8, 12 iterations
@@ -272,7 +272,7 @@ def multi_object(seed: int = 11, w: int = 1920, h: int = 1080, n_views: int = 20
     K = intrinsics(f, w, h)
     angles = list(np.linspace(-30.0, 30.0, n_views))
     cams = arc_cameras(n_views, angles, 3.0, K)
-    objs = _random_layout(rng, 3, 2, 5.0)
+    objs = _random_layout(rng, 3, 2, 4.5)
     tpm = f / 3.5
     views = build_views(objs, cams, w, h, albedo(seed), tpm, dtype, rng, noise)
     refs = list(range(n_views if n_refs is None else n_refs))

@@ -132,6 +132,33 @@ const char* hp_ctx_last_error(const hp_ctx* ctx);
 hp_status hp_ctx_synchronize(hp_ctx* ctx);
 /* Free device memory and the device total, in bytes. */
 hp_status hp_ctx_mem_info(hp_ctx* ctx, size_t* free_bytes, size_t* total_bytes);
+/* The context's CUDA stream (a cudaStream_t), for callers that order their own
+ * work or timing events against the engine's.  No reference counterpart: the
+ * reference runs everything on the default stream. */
+hp_status hp_ctx_stream(hp_ctx* ctx, void** stream);
+
+/* Kernel kinds counted by the context profiler. */
+typedef enum hp_kernel_kind {
+    HP_KERNEL_INIT = 0,      /* hypothesis initialisation */
+    HP_KERNEL_COST = 1,      /* full-map cost */
+    HP_KERNEL_PROPAGATE = 2, /* red-black propagate + refine half-pass */
+    HP_KERNEL_OTHER = 3,     /* layout, conversion and filter kernels */
+    HP_KERNEL_KINDS = 4
+} hp_kernel_kind;
+
+typedef struct hp_profile {
+    uint64_t launches[HP_KERNEL_KINDS];  /* every kernel launch the context issued */
+    double device_ms[HP_KERNEL_KINDS];   /* summed CUDA-event time, while profiling was on */
+    uint64_t timed[HP_KERNEL_KINDS];     /* launches that device_ms covers */
+} hp_profile;
+
+/* Tracing: with profiling on, every init / cost / propagate launch is
+ * bracketed by CUDA events on the context stream and its device time summed.
+ * Launch counts are kept always.  The reference has only printf progress
+ * lines (patchmatch_mvs.cu:1083-1087). */
+hp_status hp_ctx_set_profiling(hp_ctx* ctx, int enable);
+hp_status hp_ctx_profile(hp_ctx* ctx, hp_profile* out);
+hp_status hp_ctx_profile_reset(hp_ctx* ctx);
 
 /* Replaces createGrayscaleTexture (patchmatch_mvs.cu:789-814): copies a W x H
  * grayscale image (tightly packed rows) to the device, where it stays until

@@ -45,8 +45,8 @@ typedef struct orc_view {
     int radius, stride, top_k;
 } orc_view;
 
-/* Texture-filter emulation: how the hardware turns a coordinate into 8-bit
- * fixed point.  0 = round to nearest, 1 = truncate toward -inf. */
+/* Texture-filter emulation: how a coordinate becomes 8-bit fixed point.
+ * 0 = round half up (measured on B200, the default), 1 = truncate. */
 void orc_set_tex_rounding(int mode);
 int orc_get_tex_rounding(void);
 
@@ -69,6 +69,8 @@ int orc_source_ncc_f64(const orc_view* v, int x, int y, double d, double nx, dou
 
 /* Whole-map costs of fixed hypotheses.  normal is AoS (3 floats per pixel). */
 void orc_cost_map_f32(const orc_view* v, const float* depth, const float* normal, float* cost);
+/* Rows [y0, y1) only (bounded samples for the CPU baseline). */
+void orc_cost_rows_f32(const orc_view* v, const float* depth, const float* normal, float* cost, int y0, int y1);
 void orc_cost_map_f64(const orc_view* v, const float* depth, const float* normal, int quantized_weights,
                       double* cost);
 
@@ -83,6 +85,10 @@ typedef struct orc_refine {
 
 void orc_propagate_pass(const orc_view* v, float* depth, float* normal, float* cost, float dmin, float dmax,
                         int iteration, int color, uint64_t seed, uint32_t view_id, const orc_refine* rf);
+
+void orc_propagate_rows(const orc_view* v, float* depth, float* normal, float* cost, float dmin, float dmax,
+                        int iteration, int color, uint64_t seed, uint32_t view_id, const orc_refine* rf, int y0,
+                        int y1);
 
 /* init + initial cost + `iterations` red-black iterations. */
 void orc_solve_view(const orc_view* v, float dmin, float dmax, uint64_t seed, uint32_t view_id,

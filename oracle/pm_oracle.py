@@ -66,6 +66,9 @@ def lib():
                                                 C.c_double, C.c_int]),
             "orc_cost_map_f32": (None, [P(OrcView), fp, fp, fp]),
             "orc_cost_map_f64": (None, [P(OrcView), fp, fp, C.c_int, dp]),
+            "orc_cost_rows_f32": (None, [P(OrcView), fp, fp, fp, C.c_int, C.c_int]),
+            "orc_propagate_rows": (None, [P(OrcView), fp, fp, fp, C.c_float, C.c_float, C.c_int, C.c_int, C.c_uint64,
+                                          C.c_uint32, P(OrcRefine), C.c_int, C.c_int]),
             "orc_init": (None, [P(OrcView), C.c_float, C.c_float, C.c_uint64, C.c_uint32, fp, fp]),
             "orc_propagate_pass": (None, [P(OrcView), fp, fp, fp, C.c_float, C.c_float, C.c_int, C.c_int, C.c_uint64,
                                           C.c_uint32, P(OrcRefine)]),
@@ -142,6 +145,15 @@ class View:
         lib().orc_cost_map_f64(C.byref(self.c), _fp(depth), _fp(normal), int(quantized),
                                cost.ctypes.data_as(C.POINTER(C.c_double)))
         return cost
+
+    def cost_rows_f32(self, depth, normal, cost, y0, y1):
+        lib().orc_cost_rows_f32(C.byref(self.c), _fp(depth), _fp(normal), _fp(cost), y0, y1)
+
+    def propagate_rows(self, depth, normal, cost, dmin, dmax, iteration, color, seed, view_id, y0, y1,
+                       refine_steps=2, iter_decay=0.6, step_decay=0.5):
+        rf = OrcRefine(refine_steps, iter_decay, step_decay)
+        lib().orc_propagate_rows(C.byref(self.c), _fp(depth), _fp(normal), _fp(cost), dmin, dmax, iteration, color,
+                                 seed, view_id, C.byref(rf), y0, y1)
 
     def pixel_cost_f32(self, x, y, d, n):
         return lib().orc_pixel_cost_f32(C.byref(self.c), x, y, d, *map(float, n))

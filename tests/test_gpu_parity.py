@@ -1,0 +1,156 @@
+"""Parity of the CUDA path (through the C ABI) with the reference's own kernels,
+the CPU oracle and the FP64 oracle.  Tolerances are written in each test."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import cam_of, err_stats, oracle_view
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx(hp):
+    with hp.Context(0) as c:
+        yield c
+
+
+@pytest.fixture(scope="module")
+def ids_full(ctx, full_scene):
+    return [ctx.upload(v.image) for v in full_scene.views]
+
+
+@pytest.fixture(scope="module")
+def pmref():
+    import pmref as m
+    if not m.available():
+        pytest.skip("reference harness not built (needs the reference tree at build time)")
+    return m
+
+
+def job_for(hp, scene, ids, r, coeffs=None, iterations=8, seed=42):
+    srcs = scene.sources[r]
+    return hp.make_job(ids[r], [ids[i] for i in srcs], hp.make_camera(*cam_of(scene, r)),
+                       [hp.make_camera(*cam_of(scene, i)) for i in srcs], *scene.depth_range, seed=seed,
+                       view_id=r, iterations=iterations, coeffs=coeffs)
+
+
+def engine_cost(hp, ctx, job, params, d, n):
+    c = np.zeros(d.shape, np.float32)
+    ctx.ncc_cost(job, params, hp.maps_of(d.copy(), n.copy(), c))
+    return c
+
+
+def hypotheses(hp, ctx, scene, ids, r):
+    job = job_for(hp, scene, ids, r)
+    m, d, n, _ = hp.host_maps(scene.height, scene.width)
+    ctx.init_hypotheses(job, hp.default_params(), m)
+    return {"rand": (d, n), "gt": (scene.views[r].depth_gt.astype(np.float32),
+                                   np.ascontiguousarray(scene.views[r].normal_gt, np.float32))}
+
+
+@pytest.mark.parametrize("radius,kernel", [(5, "ncc"), (3, "ncc"), (7, "pixel")])
+@pytest.mark.parametrize("r", [0, 2])
+def test_fp32_cost_matches_reference_kernel(hp, ctx, ids_full, full_scene, pmref, radius, kernel, r):
+    """On identical fixed hypotheses and identical homography coefficients the FP32 cost
+    equals the reference's compute_ncc_cost_kernel (radius <= 5) / computePixelCost (radius 7).
+    Bound: |cost - reference| <= 1e-5 everywhere; in practice every pixel is bit-identical."""
+    s = full_scene
+    srcs = s.sources[r]
+    kinv, ab = pmref.setup_views(cam_of(s, r), [cam_of(s, i) for i in srcs])
+    job = job_for(hp, s, ids_full, r, coeffs=(kinv, ab))
+    p = hp.default_params(radius=radius, stride=1)
+    for tag, (d, n) in hypotheses(hp, ctx, s, ids_full, r).items():
+        ce = engine_cost(hp, ctx, job, p, d, n)
+        cr = pmref.ncc_cost(s.views[r].image_f32, [s.views[i].image_f32 for i in srcs], kinv, ab, d, n, radius,
+                            kernel)
+        st = err_stats(ce, cr)
+        assert st["max"] <= 1e-5, (tag, st)
+        assert st["exact"] >= 0.999, (tag, st)
+
+
+def test_fp32_cost_vs_cpu_oracle(hp, ctx, ids_full, full_scene, po):
+    """Engine FP32 (FP64 homography setup) vs the CPU restatement with the same coefficients.
+    IEEE vs approximate division moves a few texture weights by 1/256; each such flip weighs
+    more in a sparser window, so the bound scales with the tap count: stride 1 (121 taps)
+    p90 <= 5e-6, p99 <= 5e-5; stride 2 (36 taps) p90 <= 1e-5, p99 <= 1e-4."""
+    s, r = full_scene, 1
+    job = job_for(hp, s, ids_full, r)
+    for stride, p90, p99 in ((1, 5e-6, 5e-5), (2, 1e-5, 1e-4)):
+        p = hp.default_params(radius=5, stride=stride)
+        v = oracle_view(po, s, r, radius=5, stride=stride)
+        for tag, (d, n) in hypotheses(hp, ctx, s, ids_full, r).items():
+            st = err_stats(engine_cost(hp, ctx, job, p, d, n), v.cost_map_f32(d, n))
+            assert st["p90"] <= p90 and st["p99"] <= p99 and st["max"] <= 5e-2, (stride, tag, st)
+
+
+@pytest.mark.parametrize("radius,stride", [(5, 1), (5, 2), (7, 2), (3, 1)])
+def test_fp16acc_cost_vs_fp64_oracle(hp, ctx, ids_full, full_scene, po, radius, stride):
+    """FP16-storage / FP32-accumulate cost vs exact FP64 math: |err| <= 1e-3 on ground-truth
+    planes everywhere, and on >= 99.9% of random hypotheses (the rest are validity flips at
+    the count / contrast thresholds, where FP32 flips too)."""
+    s, r = full_scene, 2
+    job = job_for(hp, s, ids_full, r)
+    p = hp.default_params(radius=radius, stride=stride, precision=hp.PRECISION_F16ACC)
+    v = oracle_view(po, s, r, radius=radius, stride=stride)
+    for tag, (d, n) in hypotheses(hp, ctx, s, ids_full, r).items():
+        c16 = engine_cost(hp, ctx, job, p, d, n)
+        c64 = v.cost_map_f64(d, n, quantized=False)
+        e = np.abs(c16 - c64)
+        if tag == "gt":
+            assert e.max() <= 1e-3, err_stats(c16, c64)
+        assert (e <= 1e-3).mean() >= 0.999, (tag, err_stats(c16, c64))
+
+
+def test_init_bit_exact_vs_oracle(hp, ctx, ids_full, full_scene, po):
+    s = full_scene
+    for r in (0, 3):
+        job = job_for(hp, s, ids_full, r, seed=77)
+        m, d, n, _ = hp.host_maps(s.height, s.width)
+        ctx.init_hypotheses(job, hp.default_params(), m)
+        od, on = oracle_view(po, s, r).init(*s.depth_range, 77, r)
+        assert np.array_equal(d, od) and np.array_equal(n, on)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_one_pass_matches_oracle(hp, ctx, ids_full, full_scene, po, precision):
+    """One red-black half-pass from identical state: the same candidates are drawn (bit-exact
+    RNG and refinement arithmetic); adoption decisions agree except where two candidates' costs
+    are within rounding of each other."""
+    s, r = full_scene, 0
+    job = job_for(hp, s, ids_full, r)
+    p = hp.default_params(radius=5, stride=2, precision=precision)
+    d, n = hypotheses(hp, ctx, s, ids_full, r)["rand"]
+    c = engine_cost(hp, ctx, job, p, d, n)
+    v = oracle_view(po, s, r, radius=5, stride=2)
+    for it, color in [(0, 0), (3, 1)]:
+        dd, nn, cc = d.copy(), n.copy(), c.copy()
+        ctx.propagate_pass(job, p, hp.maps_of(dd, nn, cc), it, color)
+        od, on, oc = d.copy(), n.copy(), c.copy()
+        v.propagate_pass(od, on, oc, *s.depth_range, it, color, 42, r)
+        same = dd == od
+        assert same.mean() >= (0.9999 if precision == 0 else 0.995), same.mean()
+        assert np.array_equal(nn[same], on[same])
+        other = np.ones_like(same)
+        other[(np.add.outer(np.arange(s.height), np.arange(s.width)) + color) % 2 == 0] = False
+        assert np.array_equal(dd[other], d[other]), "the other color must be untouched"
+
+
+def test_filter_matches_reference_kernel(hp, ctx, full_scene, pmref):
+    s = full_scene
+    rng = np.random.default_rng(3)
+    maps = {}
+    for i in (1, 2, 3):
+        d = s.views[i].depth_gt * (1 + rng.normal(0, 0.08, s.views[i].depth_gt.shape))
+        maps[i] = (np.ascontiguousarray(d, np.float32), np.ascontiguousarray(s.views[i].normal_gt, np.float32))
+    for cos_tol in (-1.0, float(np.cos(np.radians(30)))):
+        de, ce = maps[2][0].copy(), np.full(maps[2][0].shape, 0.5, np.float32)
+        ctx.geometric_filter(hp.make_camera(*cam_of(s, 2)), de, maps[2][1], ce,
+                             [hp.make_camera(*cam_of(s, 1)), hp.make_camera(*cam_of(s, 3))],
+                             [maps[1][0], maps[3][0]], [maps[1][1], maps[3][1]], 0.12, cos_tol, 2)
+        dr, cr = maps[2][0].copy(), np.full(maps[2][0].shape, 0.5, np.float32)
+        pmref.geometric_filter(cam_of(s, 2), dr, maps[2][1], cr, [cam_of(s, 1), cam_of(s, 3)],
+                               [maps[1][0], maps[3][0]], [maps[1][1], maps[3][1]], 0.12, cos_tol, 2)
+        assert (de == dr).mean() >= 0.9999 and (ce == cr).mean() >= 0.9999
+        assert 0.05 < (de == 0).mean() < 0.95, "the test maps exercise both outcomes"
