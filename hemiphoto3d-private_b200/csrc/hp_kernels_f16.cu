@@ -1,21 +1,23 @@
 // FP16-storage / FP32-accumulate PatchMatch kernels for sm_100a.
 //
-// Same algorithm as the FP32 path (init is shared; cost, propagation and
-// refinement follow src/dense_recon/patchmatch_mvs.cu:222-343 and :519-655),
-// re-derived for throughput:
+// Same algorithm as the FP32 path (initialisation is shared; cost,
+// propagation and refinement follow src/dense_recon/patchmatch_mvs.cu:222-343
+// and :519-655), re-derived for throughput:
 //  - Sources are FP16 textures (half the texel bytes of FP32); the hardware
 //    linear filter returns FP32.
 //  - Per (candidate, source) the plane-induced homography is folded into one
 //    3x3 H = A + b (K^-T n)^T / (n.P), with the +0.5 texel-centre offset folded
-//    into its first two rows; taps then step w += s*H[:,0] along a row: three
-//    adds, one reciprocal and two multiplies per tap instead of ~25 operations.
+//    into its first two rows; along a window row a tap is w += s*H[:,0]: three
+//    adds, one reciprocal and two multiplies instead of ~25 operations.  Each
+//    row issues all its texture fetches before consuming them.
 //  - If the warped window's four corners lie inside the valid source region
 //    (the warp of a rectangle with one-signed depth is the convex quad of its
 //    corners) every tap is valid and the per-tap bounds tests are skipped.
-//  - The reference window is mean-subtracted per pixel once per visit and,
-//    for windows of up to 64 taps, held in registers as half2 pairs.  Window
-//    sums use mean-shifted values (compensated variance): FP16 products and
-//    per-row FP16 partial sums, flushed into FP32 accumulators every row.
+//  - The reference window is mean-subtracted per pixel once per visit and kept
+//    in shared memory as half2 pairs ([pair][thread], conflict-free) for
+//    windows of up to 64 taps.  Window sums use mean-shifted values
+//    (compensated variance): FP16 products and per-row FP16 partial sums,
+//    flushed into FP32 accumulators every row.
 //  - Windows touching the source border take a checked FP32 path with the
 //    reference's validity rules (|w_z| >= 1e-8, u in [0, W-1), v in [0, H-1),
 //    count >= taps/2) on mean-shifted sums.
@@ -23,6 +25,10 @@
 
 #include "hp_internal.h"
 #include "hp_rng.cuh"
+
+#ifndef HP_F16_MIN_BLOCKS
+#define HP_F16_MIN_BLOCKS 3
+#endif
 
 namespace hp {
 
@@ -55,48 +61,50 @@ __device__ __forceinline__ void load_ref_tile16(float* s_ref, int tw, int th, co
     }
 }
 
-// Per-pixel reference window, mean-subtracted.
 template <int R, int ST>
-struct RefWindow {
+struct Win {
     static constexpr int SIDE = (2 * R) / ST + 1;
     static constexpr int N = SIDE * SIDE;
-    static constexpr int PAIRS = (SIDE + 1) / 2;          // half2 per row (last may be half-empty)
-    static constexpr bool IN_REGS = SIDE * PAIRS <= 32;
-    __half2 q[IN_REGS ? SIDE * PAIRS : 1];
-    float mean;     // window mean
-    float ssd;      // sum (r - mean)^2
+    static constexpr int PAIRS = (SIDE + 1) / 2;  // half2 per row (the last may be half empty)
+    static constexpr bool IN_SMEM = SIDE * PAIRS <= 32;
+};
+constexpr int WIN_PAIRS_MAX = 32;
+
+// Per-pixel window statistics; the mean-subtracted window itself goes to s_win.
+struct RefStats {
+    float mean;  // window mean (the shift of every sum)
+    float ssd;   // sum (r - mean)^2
 };
 
 template <int R, int ST>
-__device__ __forceinline__ void load_window(RefWindow<R, ST>& w, const float* s_ref, int tw, int lx, int ly) {
-    constexpr int SIDE = RefWindow<R, ST>::SIDE;
+__device__ __forceinline__ RefStats load_window(__half2* s_win, const float* s_ref, int tw, int lx, int ly) {
+    constexpr int SIDE = Win<R, ST>::SIDE;
     float sum = 0.f;
-#pragma unroll
+#pragma unroll 1
     for (int i = 0; i < SIDE; ++i)
 #pragma unroll
         for (int j = 0; j < SIDE; ++j) sum += s_ref[(ly + i * ST) * tw + lx + j * ST];
-    const float mean = sum * (1.0f / RefWindow<R, ST>::N);
+    const float mean = sum * (1.0f / Win<R, ST>::N);
     float ssd = 0.f;
-#pragma unroll
+#pragma unroll 1
     for (int i = 0; i < SIDE; ++i)
 #pragma unroll
         for (int j = 0; j < SIDE; ++j) {
             const float d = s_ref[(ly + i * ST) * tw + lx + j * ST] - mean;
             ssd = fmaf(d, d, ssd);
         }
-    w.mean = mean;
-    w.ssd = ssd;
-    if constexpr (RefWindow<R, ST>::IN_REGS) {
-        constexpr int PAIRS = RefWindow<R, ST>::PAIRS;
-#pragma unroll
+    if constexpr (Win<R, ST>::IN_SMEM) {
+        constexpr int PAIRS = Win<R, ST>::PAIRS;
+#pragma unroll 1
         for (int i = 0; i < SIDE; ++i)
 #pragma unroll
             for (int p = 0; p < PAIRS; ++p) {
                 const float a = s_ref[(ly + i * ST) * tw + lx + (2 * p) * ST] - mean;
                 const float b = (2 * p + 1 < SIDE) ? s_ref[(ly + i * ST) * tw + lx + (2 * p + 1) * ST] - mean : 0.f;
-                w.q[i * PAIRS + p] = __floats2half2_rn(a, b);
+                s_win[(i * PAIRS + p) * CTA_THREADS + threadIdx.x] = __floats2half2_rn(a, b);
             }
     }
+    return RefStats{mean, ssd};
 }
 
 // Approximate reciprocal (PTX rcp.approx.ftz.f32, ~1 ulp): the warped-coordinate
@@ -114,12 +122,12 @@ struct Plane {
 // Checked FP32 evaluation of one source (border windows): reference validity
 // rules, mean-shifted sums.  Returns the source cost (1 - NCC or 2).
 template <int R, int ST>
-__device__ float source_cost_checked(const Plane& P, cudaTextureObject_t tex, const RefWindow<R, ST>& w,
-                                     const float* s_ref, int tw, int lx, int ly, int x, int y, float fW, float fH) {
-    constexpr int SIDE = RefWindow<R, ST>::SIDE;
+__device__ __noinline__ float source_cost_checked(const Plane& P, cudaTextureObject_t tex, float c0,
+                                                  const float* s_ref, int tw, int lx, int ly, int x, int y, float fW,
+                                                  float fH) {
+    constexpr int SIDE = Win<R, ST>::SIDE;
     float sr = 0.f, ss = 0.f, srr = 0.f, sss = 0.f, srs = 0.f;
     int count = 0;
-    const float c0 = w.mean;
     for (int i = 0; i < SIDE; ++i) {
         const float py = static_cast<float>(y - R + i * ST);
         for (int j = 0; j < SIDE; ++j) {
@@ -140,7 +148,7 @@ __device__ float source_cost_checked(const Plane& P, cudaTextureObject_t tex, co
             ++count;
         }
     }
-    if (count < RefWindow<R, ST>::N / 2) return 2.0f;
+    if (count < Win<R, ST>::N / 2) return 2.0f;
     const float n = static_cast<float>(count);
     const float num = fmaf(n, srs, -sr * ss);
     const float dr = fmaf(n, srr, -sr * sr);
@@ -153,41 +161,45 @@ __device__ float source_cost_checked(const Plane& P, cudaTextureObject_t tex, co
 // Fast path: all taps valid.  Sums of e = s - mean and products (r - mean) e
 // in FP16 per row, flushed to FP32.
 template <int R, int ST>
-__device__ __forceinline__ float source_cost_fast(const Plane& P, cudaTextureObject_t tex, const RefWindow<R, ST>& w,
-                                                  const float* s_ref, int tw, int lx, int ly, int x, int y) {
-    constexpr int SIDE = RefWindow<R, ST>::SIDE;
-    constexpr int PAIRS = RefWindow<R, ST>::PAIRS;
-    const float c0 = w.mean;
-    const __half2 c0h = __float2half2_rn(c0);
+__device__ __forceinline__ float source_cost_fast(const Plane& P, cudaTextureObject_t tex, RefStats st,
+                                                  const __half2* s_win, const float* s_ref, int tw, int lx, int ly,
+                                                  int x, int y) {
+    constexpr int SIDE = Win<R, ST>::SIDE;
+    constexpr int PAIRS = Win<R, ST>::PAIRS;
+    const float c0 = st.mean;
     float s1 = 0.f, s2 = 0.f, s3 = 0.f;
     const float sx0 = static_cast<float>(x - R), sy0 = static_cast<float>(y - R);
     const float hx0 = P.h[0] * ST, hx1 = P.h[3] * ST, hx2 = P.h[6] * ST;
-#pragma unroll
+    const float rx0 = fmaf(P.h[0], sx0, P.h[2]), rx1 = fmaf(P.h[3], sx0, P.h[5]), rx2 = fmaf(P.h[6], sx0, P.h[8]);
+#pragma unroll 1
     for (int i = 0; i < SIDE; ++i) {
         const float py = sy0 + static_cast<float>(i * ST);
-        float wx = fmaf(P.h[0], sx0, fmaf(P.h[1], py, P.h[2]));
-        float wy = fmaf(P.h[3], sx0, fmaf(P.h[4], py, P.h[5]));
-        float wz = fmaf(P.h[6], sx0, fmaf(P.h[7], py, P.h[8]));
+        float wx = fmaf(P.h[1], py, rx0);
+        float wy = fmaf(P.h[4], py, rx1);
+        float wz = fmaf(P.h[7], py, rx2);
+        float smp[2 * PAIRS];
+#pragma unroll
+        for (int j = 0; j < SIDE; ++j) {
+            const float iz = rcp_approx(wz);
+            smp[j] = tex2D<float>(tex, wx * iz, wy * iz);
+            wx += hx0;
+            wy += hx1;
+            wz += hx2;
+        }
+        if constexpr (SIDE & 1) smp[SIDE] = c0;  // pads the last pair: e = 0
         __half2 a1 = __float2half2_rn(0.f), a2 = a1, a3 = a1;
 #pragma unroll
         for (int p = 0; p < PAIRS; ++p) {
-            float iz = rcp_approx(wz);
-            const float sa = tex2D<float>(tex, wx * iz, wy * iz);
-            wx += hx0; wy += hx1; wz += hx2;
-            float sb = 0.f;
-            if (2 * p + 1 < SIDE) {
-                iz = rcp_approx(wz);
-                sb = tex2D<float>(tex, wx * iz, wy * iz);
-                wx += hx0; wy += hx1; wz += hx2;
-            }
-            __half2 e = __hsub2(__floats2half2_rn(sa, sb), c0h);
-            if (2 * p + 1 >= SIDE) e = __halves2half2(__low2half(e), __float2half_rn(0.f));
+            // The shift is subtracted in FP32 and only the small residual is
+            // rounded to FP16 (rounding the sample first would cost ~2.4e-4).
+            const __half2 e = __floats2half2_rn(smp[2 * p] - c0, smp[2 * p + 1] - c0);
             __half2 rq;
-            if constexpr (RefWindow<R, ST>::IN_REGS) {
-                rq = w.q[i * PAIRS + p];
+            if constexpr (Win<R, ST>::IN_SMEM) {
+                rq = s_win[(i * PAIRS + p) * CTA_THREADS];  // s_win points at the pixel's column
             } else {
-                const float ra = s_ref[(ly + i * ST) * tw + lx + (2 * p) * ST] - c0;
-                const float rb = (2 * p + 1 < SIDE) ? s_ref[(ly + i * ST) * tw + lx + (2 * p + 1) * ST] - c0 : 0.f;
+                const float* row = s_ref + (ly + i * ST) * tw + lx;
+                const float ra = row[(2 * p) * ST] - c0;
+                const float rb = (2 * p + 1 < SIDE) ? row[(2 * p + 1) * ST] - c0 : 0.f;
                 rq = __floats2half2_rn(ra, rb);
             }
             a1 = __hadd2(a1, e);
@@ -199,9 +211,9 @@ __device__ __forceinline__ float source_cost_fast(const Plane& P, cudaTextureObj
         s2 += f2.x + f2.y;
         s3 += f3.x + f3.y;
     }
-    constexpr float n = static_cast<float>(RefWindow<R, ST>::N);
+    constexpr float n = static_cast<float>(Win<R, ST>::N);
     // n*sum(r^2)-sum(r)^2 = n*ssd, n*sum(s^2)-sum(s)^2 = n*s2 - s1^2, cov numerator n*s3 (sum(r - mean) = 0).
-    const float dr = n * w.ssd;
+    const float dr = n * st.ssd;
     const float ds = fmaf(n, s2, -s1 * s1);
     if (dr < 1e-6f || ds < 1e-6f) return 2.0f;
     const float ncc = fmaxf(-1.0f, fminf(1.0f, n * s3 * rsqrtf(dr) * rsqrtf(ds)));
@@ -209,8 +221,8 @@ __device__ __forceinline__ float source_cost_fast(const Plane& P, cudaTextureObj
 }
 
 template <int R, int ST>
-__device__ __forceinline__ float cost_f16(const RefWindow<R, ST>& w, const float* s_ref, int tw, int lx, int ly,
-                                          int x, int y, float d, float cnx, float cny, float cnz,
+__device__ __forceinline__ float cost_f16(RefStats st, const __half2* s_win, const float* s_ref, int tw, int lx,
+                                          int ly, int x, int y, float d, float cnx, float cny, float cnz,
                                           const ViewDesc* __restrict__ v, int topk) {
     const float* k = v->kinv;
     const float fx = static_cast<float>(x), fy = static_cast<float>(y);
@@ -224,8 +236,8 @@ __device__ __forceinline__ float cost_f16(const RefWindow<R, ST>& w, const float
     const float m1 = fmaf(k[1], cnx, fmaf(k[4], cny, k[7] * cnz)) * ind;
     const float m2 = fmaf(k[2], cnx, fmaf(k[5], cny, k[8] * cnz)) * ind;
     const float fW = static_cast<float>(v->W), fH = static_cast<float>(v->H);
-    const float xa = static_cast<float>(x - R), xb = static_cast<float>(x - R + (RefWindow<R, ST>::SIDE - 1) * ST);
-    const float ya = static_cast<float>(y - R), yb = static_cast<float>(y - R + (RefWindow<R, ST>::SIDE - 1) * ST);
+    const float xa = static_cast<float>(x - R), xb = static_cast<float>(x - R + (Win<R, ST>::SIDE - 1) * ST);
+    const float ya = static_cast<float>(y - R), yb = static_cast<float>(y - R + (Win<R, ST>::SIDE - 1) * ST);
     float top0 = 2.0f, top1 = 2.0f, top2 = 2.0f;
     const int S = v->S;
     for (int s = 0; s < S; ++s) {
@@ -254,8 +266,8 @@ __device__ __forceinline__ float cost_f16(const RefWindow<R, ST>& w, const float
                      vv >= 0.501f && vv < fH - 0.501f;
         }
         const cudaTextureObject_t tex = v->src_tex16[s];
-        const float c = inside ? source_cost_fast<R, ST>(P, tex, w, s_ref, tw, lx, ly, x, y)
-                               : source_cost_checked<R, ST>(P, tex, w, s_ref, tw, lx, ly, x, y, fW, fH);
+        const float c = inside ? source_cost_fast<R, ST>(P, tex, st, s_win, s_ref, tw, lx, ly, x, y)
+                               : source_cost_checked<R, ST>(P, tex, st.mean, s_ref, tw, lx, ly, x, y, fW, fH);
         if (c < top2) {
             top2 = c;
             if (top2 < top1) {
@@ -277,11 +289,12 @@ __device__ __forceinline__ bool same_plane16(float4 a, float4 b) {
 }
 
 template <int R, int ST>
-__global__ void __launch_bounds__(CTA_THREADS) cost16_kernel(BatchList bl, SolveConsts sc) {
+__global__ void __launch_bounds__(CTA_THREADS, HP_F16_MIN_BLOCKS) cost16_kernel(BatchList bl, SolveConsts sc) {
     __shared__ float s_ref[MAX_TW * MAX_TH];
+    __shared__ __half2 s_win[Win<R, ST>::IN_SMEM ? WIN_PAIRS_MAX * CTA_THREADS : 1];
     int tile_x, tile_y;
     const ViewDesc* v = locate_tile16(bl, blockIdx.x, &tile_x, &tile_y);
-    const int tw = TILE_W + 2 * R, th = TILE_H + 2 * R;
+    constexpr int tw = TILE_W + 2 * R, th = TILE_H + 2 * R;
     const int x0 = tile_x * TILE_W, y0 = tile_y * TILE_H;
     load_ref_tile16(s_ref, tw, th, v, x0, y0, R);
     __syncthreads();
@@ -291,37 +304,113 @@ __global__ void __launch_bounds__(CTA_THREADS) cost16_kernel(BatchList bl, Solve
     for (int j = 0; j < 2; ++j) {
         const int lx = 2 * lane + j, x = x0 + lx;
         if (x >= v->W) continue;
-        RefWindow<R, ST> w;
-        load_window<R, ST>(w, s_ref, tw, lx, ly);
+        const RefStats st = load_window<R, ST>(s_win, s_ref, tw, lx, ly);
         const size_t idx = static_cast<size_t>(y) * v->W + x;
         const float4 h = v->hyp[idx];
-        v->cost[idx] = cost_f16<R, ST>(w, s_ref, tw, lx, ly, x, y, h.x, h.y, h.z, h.w, v, sc.top_k);
+        v->cost[idx] = cost_f16<R, ST>(st, s_win + threadIdx.x, s_ref, tw, lx, ly, x, y, h.x, h.y, h.z, h.w, v,
+                                       sc.top_k);
     }
 }
 
+// One red-black half-pass.  The neighbour phase is compacted per warp exactly
+// as in the FP32 kernel (see propagate_kernel there): lanes list the
+// neighbour planes they must score, the warp scores the union 32 items at a
+// time (an item borrows its owner's window statistics by shuffle and the
+// owner's column of s_win), and owners fold the costs in L, R, U, D order.
 template <int R, int ST>
-__global__ void __launch_bounds__(CTA_THREADS) propagate16_kernel(BatchList bl, SolveConsts sc, int iteration,
-                                                                  int color) {
+__global__ void __launch_bounds__(CTA_THREADS, HP_F16_MIN_BLOCKS) propagate16_kernel(BatchList bl, SolveConsts sc,
+                                                                                     int iteration, int color) {
+    constexpr int WARPS = CTA_THREADS / 32;
     __shared__ float s_ref[MAX_TW * MAX_TH];
+    __shared__ __half2 s_win[Win<R, ST>::IN_SMEM ? WIN_PAIRS_MAX * CTA_THREADS : 1];
+    __shared__ float s_cost[WARPS][32 * 4];
+    __shared__ unsigned char s_items[WARPS][32 * 4];
     int tile_x, tile_y;
     const ViewDesc* v = locate_tile16(bl, blockIdx.x, &tile_x, &tile_y);
-    const int tw = TILE_W + 2 * R, th = TILE_H + 2 * R;
+    constexpr int tw = TILE_W + 2 * R, th = TILE_H + 2 * R;
     const int x0 = tile_x * TILE_W, y0 = tile_y * TILE_H;
     load_ref_tile16(s_ref, tw, th, v, x0, y0, R);
     __syncthreads();
     const int W = v->W, H = v->H;
     const int ly = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int y = y0 + ly;
-    const int lx = 2 * lane + ((y + color) & 1);
+    if (y >= H) return;  // uniform per warp
+    const int parity = (y + color) & 1;
+    const int lx = 2 * lane + parity;
     const int x = x0 + lx;
-    if (y >= H || x >= W) return;
+    const bool active = x < W;
     const size_t idx = static_cast<size_t>(y) * W + x;
     const float dmin = v->dmin, dmax = v->dmax;
-    RefWindow<R, ST> w;
-    load_window<R, ST>(w, s_ref, tw, lx, ly);
-
-    float4 best = v->hyp[idx];
-    float best_cost = v->cost[idx];
+    RefStats st{0.f, 0.f};
+    float4 best = make_float4(0.f, 0.f, 0.f, 0.f);
+    float best_cost = 0.f;
+    unsigned need = 0;
+    if (active) {
+        st = load_window<R, ST>(s_win, s_ref, tw, lx, ly);
+        best = v->hyp[idx];
+        best_cost = v->cost[idx];
+#pragma unroll
+        for (int cand = 0; cand < 4; ++cand) {
+            const int nxp = x + (cand == 0 ? -1 : (cand == 1 ? 1 : 0));
+            const int nyp = y + (cand == 2 ? -1 : (cand == 3 ? 1 : 0));
+            if (nxp < 0 || nxp >= W || nyp < 0 || nyp >= H) continue;
+            const float4 h = v->hyp[static_cast<size_t>(nyp) * W + nxp];
+            if (h.x < dmin || h.x > dmax) continue;
+            bool dup = same_plane16(h, best);
+            for (int j = 0; j < cand && !dup; ++j) {
+                if (need & (1u << j)) {
+                    const int jx = x + (j == 0 ? -1 : (j == 1 ? 1 : 0));
+                    const int jy = y + (j == 2 ? -1 : (j == 3 ? 1 : 0));
+                    dup = same_plane16(h, v->hyp[static_cast<size_t>(jy) * W + jx]);
+                }
+            }
+            if (!dup) need |= 1u << cand;
+        }
+    }
+    const int cnt = __popc(need);
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    {
+        int k = incl - cnt;
+        for (int cand = 0; cand < 4; ++cand)
+            if (need & (1u << cand)) s_items[ly][k++] = static_cast<unsigned char>((lane << 2) | cand);
+    }
+    __syncwarp();
+    for (int base = 0; base < total; base += 32) {
+        const int w = base + lane;
+        const int item = w < total ? s_items[ly][w] : 0;
+        const int owner = item >> 2, cand = item & 3;
+        RefStats ost;
+        ost.mean = __shfl_sync(0xffffffffu, st.mean, owner);
+        ost.ssd = __shfl_sync(0xffffffffu, st.ssd, owner);
+        if (w < total) {
+            const int olx = 2 * owner + parity, ox = x0 + olx;
+            const int nxp = ox + (cand == 0 ? -1 : (cand == 1 ? 1 : 0));
+            const int nyp = y + (cand == 2 ? -1 : (cand == 3 ? 1 : 0));
+            const float4 h = v->hyp[static_cast<size_t>(nyp) * W + nxp];
+            s_cost[ly][item] = cost_f16<R, ST>(ost, s_win + ly * 32 + owner, s_ref, tw, olx, ly, ox, y, h.x, h.y,
+                                               h.z, h.w, v, sc.top_k);
+        }
+    }
+    __syncwarp();
+    if (!active) return;
+#pragma unroll
+    for (int cand = 0; cand < 4; ++cand) {
+        if (need & (1u << cand)) {
+            const float c = s_cost[ly][(lane << 2) | cand];
+            if (c < best_cost) {
+                const int nxp = x + (cand == 0 ? -1 : (cand == 1 ? 1 : 0));
+                const int nyp = y + (cand == 2 ? -1 : (cand == 3 ? 1 : 0));
+                best_cost = c;
+                best = v->hyp[static_cast<size_t>(nyp) * W + nxp];
+            }
+        }
+    }
     const float3 ray = view_ray(v->kinv, x, y);
     float drange = __fmul_rn(__fsub_rn(dmax, dmin), 0.5f);
     float nrange = 1.0f;
@@ -329,44 +418,25 @@ __global__ void __launch_bounds__(CTA_THREADS) propagate16_kernel(BatchList bl, 
         drange = __fmul_rn(drange, sc.iter_decay);
         nrange = __fmul_rn(nrange, sc.iter_decay);
     }
-    float4 tried[4];
-    int n_tried = 0;
-    // Candidates 0..3: neighbours L, R, U, D; then refine_steps perturbations.
-    const int n_cand = 4 + sc.refine_steps;
-    for (int cand = 0; cand < n_cand; ++cand) {
-        float4 h;
-        if (cand < 4) {
-            const int nxp = x + (cand == 0 ? -1 : (cand == 1 ? 1 : 0));
-            const int nyp = y + (cand == 2 ? -1 : (cand == 3 ? 1 : 0));
-            if (nxp < 0 || nxp >= W || nyp < 0 || nyp >= H) continue;
-            h = v->hyp[static_cast<size_t>(nyp) * W + nxp];
-            if (h.x < dmin || h.x > dmax) continue;
-            bool dup = same_plane16(h, best);
-#pragma unroll
-            for (int j = 0; j < 4; ++j) dup |= (j < n_tried) && same_plane16(h, tried[j]);
-            if (dup) continue;
-            tried[n_tried++] = h;
-        } else {
-            const int step = cand - 4;
-            const uint4 rr = philox4x32_10(make_uint4(static_cast<uint32_t>(idx), v->view_id,
-                                                      1u + static_cast<uint32_t>(iteration), static_cast<uint32_t>(step)),
-                                           v->seed_lo, v->seed_hi);
-            float cd = __fmaf_rn(__fmaf_rn(u01(rr.x), 2.0f, -1.0f), drange, best.x);
-            cd = fmaxf(dmin, fminf(dmax, cd));
-            const float cx = __fmaf_rn(__fmaf_rn(u01(rr.y), 2.0f, -1.0f), nrange, best.y);
-            const float cy = __fmaf_rn(__fmaf_rn(u01(rr.z), 2.0f, -1.0f), nrange, best.z);
-            const float cz = __fmaf_rn(__fmaf_rn(u01(rr.w), 2.0f, -1.0f), nrange, best.w);
-            float3 cn = normalize3_rn(cx, cy, cz);
-            if (dot3_rn(cn, ray) > 0.0f) cn = make_float3(-cn.x, -cn.y, -cn.z);
-            h = make_float4(cd, cn.x, cn.y, cn.z);
-            drange = __fmul_rn(drange, sc.step_decay);
-            nrange = __fmul_rn(nrange, sc.step_decay);
-        }
-        const float c = cost_f16<R, ST>(w, s_ref, tw, lx, ly, x, y, h.x, h.y, h.z, h.w, v, sc.top_k);
+    for (int step = 0; step < sc.refine_steps; ++step) {
+        const uint4 rr = philox4x32_10(make_uint4(static_cast<uint32_t>(idx), v->view_id,
+                                                  1u + static_cast<uint32_t>(iteration), static_cast<uint32_t>(step)),
+                                       v->seed_lo, v->seed_hi);
+        float cd = __fmaf_rn(__fmaf_rn(u01(rr.x), 2.0f, -1.0f), drange, best.x);
+        cd = fmaxf(dmin, fminf(dmax, cd));
+        const float cx = __fmaf_rn(__fmaf_rn(u01(rr.y), 2.0f, -1.0f), nrange, best.y);
+        const float cy = __fmaf_rn(__fmaf_rn(u01(rr.z), 2.0f, -1.0f), nrange, best.z);
+        const float cz = __fmaf_rn(__fmaf_rn(u01(rr.w), 2.0f, -1.0f), nrange, best.w);
+        float3 cn = normalize3_rn(cx, cy, cz);
+        if (dot3_rn(cn, ray) > 0.0f) cn = make_float3(-cn.x, -cn.y, -cn.z);
+        const float c = cost_f16<R, ST>(st, s_win + threadIdx.x, s_ref, tw, lx, ly, x, y, cd, cn.x, cn.y, cn.z, v,
+                                        sc.top_k);
         if (c < best_cost) {
             best_cost = c;
-            best = h;
+            best = make_float4(cd, cn.x, cn.y, cn.z);
         }
+        drange = __fmul_rn(drange, sc.step_decay);
+        nrange = __fmul_rn(nrange, sc.step_decay);
     }
     v->hyp[idx] = best;
     v->cost[idx] = best_cost;
@@ -384,6 +454,7 @@ cudaError_t launch_r(const BatchList& bl, const SolveConsts& sc, int iteration, 
 cudaError_t dispatch(const BatchList& bl, const SolveConsts& sc, int iteration, int color, bool full,
                      cudaStream_t st) {
     if (bl.total_tiles <= 0) return cudaSuccess;
+    if (sc.stride != 1 && sc.stride != 2) return cudaErrorInvalidValue;
 #define HP_CASE(RR)                                                                       \
     case RR:                                                                              \
         return sc.stride == 1 ? launch_r<RR, 1>(bl, sc, iteration, color, full, st)       \

@@ -5,17 +5,26 @@
 // src/dense_recon/patchmatch_mvs.cu:222-343) samples sources through the
 // texture unit's linear filter, whose weights carry only 8 fractional bits; a
 // warped coordinate that moves by one ulp can flip a weight by 1/256 and the
-// cost by ~1e-5.  To hold the 1e-5 bound this file keeps the reference's
-// per-tap arithmetic - the same expressions in the same order, built with the
-// reference's --use_fast_math - and samples sources with tex2D on the same
-// filter configuration.  Everything around the taps is this engine's own:
-// packed float4 hypotheses, a shared-memory reference tile, red-black
-// compaction (every thread owns a pixel of the active color), duplicate-
-// candidate elimination, batched multi-view launches and counter-based RNG.
-// Engine-defined arithmetic outside the taps uses explicitly rounded
+// cost by ~1e-5.  To hold the 1e-5 bound this file reproduces the reference's
+// per-tap rounding exactly - the operation sequence its --use_fast_math build
+// executes, pinned with explicitly rounded intrinsics (see cost_f32) - and
+// samples sources with tex2D on the same filter configuration; the per-pixel
+// plane setup and the NCC finalisation keep the reference's expressions in a
+// translation unit built with the same flags.  The result is bit-identical to
+// the reference's compute_ncc_cost_kernel.  Everything around the arithmetic
+// is this engine's own: packed float4 hypotheses, a shared-memory reference
+// tile, red-black compaction (every thread owns a pixel of the active color),
+// row-batched texture fetches, duplicate-candidate elimination, batched
+// multi-view launches and counter-based RNG.  Engine-defined arithmetic
+// outside the taps (initialisation, refinement) uses explicitly rounded
 // intrinsics so the CPU restatement reproduces it bit for bit.
 #include "hp_internal.h"
 #include "hp_rng.cuh"
+
+// Resident CTAs per SM the cost kernels are register-budgeted for.
+#ifndef HP_F32_MIN_BLOCKS
+#define HP_F32_MIN_BLOCKS 2
+#endif
 
 namespace hp {
 
@@ -52,18 +61,33 @@ __device__ __forceinline__ void load_ref_tile(float* s_ref, int tw, int th, cons
     }
 }
 
+// Approximate reciprocal (PTX rcp.approx.ftz.f32): the instruction the
+// reference's fast-math build uses for 1.0f / w_z.
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 // Cost of hypothesis (d, n) at pixel (x, y): per-source NCC over the window,
-// top_k lowest of (1 - NCC) averaged.  One out-of-line body so the full-map
-// kernel and the propagate kernel round identically.  The sampling stride ST
-// is a compile-time constant: with a run-time stride the fast-math build
-// reassociates the warp arithmetic differently from the reference's unit-
-// stride loop and ~30% of costs move by an ulp-driven 1e-5; with ST = 1 the
-// loop has the reference's shape and the costs are bit-identical to it.
-template <int ST>
-__device__ __noinline__ float cost_f32(const float* __restrict__ s_ref, int tw, int lx, int ly, int x, int y,
-                                       float d, float cnx, float cny, float cnz, const ViewDesc* __restrict__ v,
-                                       int r, int topk) {
-    constexpr int st = ST;
+// top_k lowest of (1 - NCC) averaged (computePixelCost, :222-343).
+//
+// Per tap the warp arithmetic is pinned with explicitly rounded intrinsics to
+// the operation sequence the reference compiles to (found by a bit-exact
+// search against its kernels on B200):
+//   q = fma(a0, x, a1*y) + a2,  f = s * inv(n.P),  w_z = fma(b2, f, q_z),
+//   u = fma(b0, f, q_x) * rcp(w_z),  sums accumulated with fma in tap order.
+// Because nothing is left to the compiler's reassociation, the taps can be
+// restructured for throughput: each window row issues all its texture
+// fetches before consuming any (SIDE fetches in flight per thread), the
+// row-invariant products a1*y are computed once per row (the same rounded
+// value), and samples are accumulated in tap order, skipping invalid taps
+// exactly as the reference's `continue`s do.
+template <int R, int ST>
+__device__ __forceinline__ float cost_f32(const float* __restrict__ s_ref, int tw, int lx, int ly, int x, int y,
+                                          float d, float cnx, float cny, float cnz, const ViewDesc* __restrict__ v,
+                                          int topk) {
+    constexpr int SIDE = (2 * R) / ST + 1;
     const float ki0 = v->kinv[0], ki1 = v->kinv[1], ki2 = v->kinv[2];
     const float ki3 = v->kinv[3], ki4 = v->kinv[4], ki5 = v->kinv[5];
     const float ki6 = v->kinv[6], ki7 = v->kinv[7], ki8 = v->kinv[8];
@@ -79,44 +103,55 @@ __device__ __noinline__ float cost_f32(const float* __restrict__ s_ref, int tw, 
     const float nK0 = ki0 * cnx + ki3 * cny + ki6 * cnz;
     const float nK1 = ki1 * cnx + ki4 * cny + ki7 * cnz;
     const float nK2 = ki2 * cnx + ki5 * cny + ki8 * cnz;
+    constexpr int min_count = (SIDE * SIDE) / 2;
+    const float fw1 = static_cast<float>(v->W) - 1.0f;
+    const float fh1 = static_cast<float>(v->H) - 1.0f;
 
-    const int side = (2 * r) / st + 1;
-    const int min_count = (side * side) / 2;
-    const float fwidth = static_cast<float>(v->W);
-    const float fheight = static_cast<float>(v->H);
-
-    // Loop shape, coefficient reads and the top-k array are kept as the
-    // reference writes them: the fast-math build then rounds every tap exactly
-    // as the reference does (verified bit-for-bit on the GPU).
     float top[3] = {2.0f, 2.0f, 2.0f};
     const int S = v->S;
     for (int s = 0; s < S; ++s) {
         const float* A = v->ab[s];
+        const float a0 = A[0], a1 = A[1], a2 = A[2], a3 = A[3], a4 = A[4], a5 = A[5];
+        const float a6 = A[6], a7 = A[7], a8 = A[8], b0 = A[9], b1 = A[10], b2 = A[11];
+        const cudaTextureObject_t tex = v->src_tex[s];
         float sum_ref = 0.0f, sum_src = 0.0f, sum_ref2 = 0.0f, sum_src2 = 0.0f, sum_rs = 0.0f;
         int count = 0;
-        for (int dy = -r; dy <= r; dy += st) {
-            for (int dx = -r; dx <= r; dx += st) {
-                const float ref_val = s_ref[(ly + r + dy) * tw + (lx + r + dx)];
-                const float wpx = fx + static_cast<float>(dx);
-                const float wpy = fy + static_cast<float>(dy);
-                const float qx = A[0] * wpx + A[1] * wpy + A[2];
-                const float qy = A[3] * wpx + A[4] * wpy + A[5];
-                const float qz = A[6] * wpx + A[7] * wpy + A[8];
-                const float sval = nK0 * wpx + nK1 * wpy + nK2;
-                const float factor = sval * inv_n_dot_P;
-                const float wz = qz + A[11] * factor;
-                if (fabsf(wz) < 1e-8f) continue;
-                const float inv_wz = 1.0f / wz;
-                const float src_u = (qx + A[9] * factor) * inv_wz;
-                const float src_v = (qy + A[10] * factor) * inv_wz;
-                if (src_u < 0.0f || src_u >= fwidth - 1.0f || src_v < 0.0f || src_v >= fheight - 1.0f) continue;
-                const float src_val = tex2D<float>(v->src_tex[s], src_u + 0.5f, src_v + 0.5f);
-                sum_ref += ref_val;
-                sum_src += src_val;
-                sum_ref2 += ref_val * ref_val;
-                sum_src2 += src_val * src_val;
-                sum_rs += ref_val * src_val;
-                count++;
+#pragma unroll 1
+        for (int i = 0; i < SIDE; ++i) {
+            const float wpy = fy + static_cast<float>(i * ST - R);
+            const float tqx = __fmul_rn(a1, wpy), tqy = __fmul_rn(a4, wpy), tqz = __fmul_rn(a7, wpy);
+            const float tsv = __fmul_rn(nK1, wpy);
+            float smp[SIDE];
+            unsigned ok = 0;
+#pragma unroll
+            for (int j = 0; j < SIDE; ++j) {
+                const float wpx = fx + static_cast<float>(j * ST - R);
+                const float qx = __fadd_rn(__fmaf_rn(a0, wpx, tqx), a2);
+                const float qy = __fadd_rn(__fmaf_rn(a3, wpx, tqy), a5);
+                const float qz = __fadd_rn(__fmaf_rn(a6, wpx, tqz), a8);
+                const float sval = __fadd_rn(__fmaf_rn(nK0, wpx, tsv), nK2);
+                const float factor = __fmul_rn(sval, inv_n_dot_P);
+                const float wz = __fmaf_rn(b2, factor, qz);
+                const float iw = rcp_approx(wz);
+                const float u = __fmul_rn(__fmaf_rn(b0, factor, qx), iw);
+                const float vv = __fmul_rn(__fmaf_rn(b1, factor, qy), iw);
+                const bool skip = fabsf(wz) < 1e-8f || u < 0.0f || u >= fw1 || vv < 0.0f || vv >= fh1;
+                ok |= static_cast<unsigned>(!skip) << j;
+                smp[j] = tex2D<float>(tex, __fadd_rn(u, 0.5f), __fadd_rn(vv, 0.5f));
+            }
+            const float* rrow = s_ref + (ly + i * ST) * tw + lx;
+#pragma unroll
+            for (int j = 0; j < SIDE; ++j) {
+                if (ok & (1u << j)) {
+                    const float rv = rrow[j * ST];
+                    const float sv = smp[j];
+                    sum_ref = __fadd_rn(sum_ref, rv);
+                    sum_src = __fadd_rn(sum_src, sv);
+                    sum_ref2 = __fmaf_rn(rv, rv, sum_ref2);
+                    sum_src2 = __fmaf_rn(sv, sv, sum_src2);
+                    sum_rs = __fmaf_rn(rv, sv, sum_rs);
+                    count++;
+                }
             }
         }
         float c;
@@ -192,14 +227,14 @@ __global__ void __launch_bounds__(CTA_THREADS) init_kernel(BatchList bl) {
 
 // Full-map cost of the current hypotheses (compute_ncc_cost_kernel,
 // patchmatch_mvs.cu:349-513).  Each thread owns a horizontal pixel pair.
-template <int ST>
-__global__ void __launch_bounds__(CTA_THREADS) cost_kernel(BatchList bl, SolveConsts sc) {
+template <int R, int ST>
+__global__ void __launch_bounds__(CTA_THREADS, HP_F32_MIN_BLOCKS) cost_kernel(BatchList bl, SolveConsts sc) {
     __shared__ float s_ref[MAX_TW * MAX_TH];
     int tile_x, tile_y;
     const ViewDesc* v = locate_tile(bl, blockIdx.x, &tile_x, &tile_y);
-    const int r = sc.radius, tw = TILE_W + 2 * r, th = TILE_H + 2 * r;
+    constexpr int tw = TILE_W + 2 * R, th = TILE_H + 2 * R;
     const int x0 = tile_x * TILE_W, y0 = tile_y * TILE_H;
-    load_ref_tile(s_ref, tw, th, v, x0, y0, r);
+    load_ref_tile(s_ref, tw, th, v, x0, y0, R);
     __syncthreads();
     const int ly = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int y = y0 + ly;
@@ -209,60 +244,116 @@ __global__ void __launch_bounds__(CTA_THREADS) cost_kernel(BatchList bl, SolveCo
         if (x >= v->W) continue;
         const size_t idx = static_cast<size_t>(y) * v->W + x;
         const float4 h = v->hyp[idx];
-        v->cost[idx] = cost_f32<ST>(s_ref, tw, lx, ly, x, y, h.x, h.y, h.z, h.w, v, r, sc.top_k);
+        v->cost[idx] = cost_f32<R, ST>(s_ref, tw, lx, ly, x, y, h.x, h.y, h.z, h.w, v, sc.top_k);
     }
 }
 
 // One red-black half-pass (propagate_and_refine_kernel, patchmatch_mvs.cu:519-655).
 // Thread (ly, lane) owns pixel x0 + 2*lane + ((y + color) & 1) of row y0 + ly:
 // every thread has work, where the reference idles half its grid.
-template <int ST>
-__global__ void __launch_bounds__(CTA_THREADS) propagate_kernel(BatchList bl, SolveConsts sc, int iteration,
-                                                                int color) {
+//
+// Neighbour phase (L, R, U, D; :551-580), compacted per warp.  Each lane lists
+// the neighbour planes it must score: in range, and not bit-identical to its
+// current plane or to an earlier listed neighbour (such a candidate cannot win:
+// same pixel, same plane, same arithmetic, same cost).  Lanes skip different
+// candidates, so scoring them lane by lane would leave warps half idle while
+// every texture instruction still costs nearly a full warp's worth of filter
+// throughput.  Instead the warp writes the union of its (pixel, neighbour) items
+// to a list in shared memory and scores it 32 items at a time, then each owner
+// folds its costs in L, R, U, D order with the same strict-less rule - the
+// result is that of the sequential loop.  The refinement perturbations
+// (:583-648) follow per lane: every lane has exactly refine_steps of them.
+template <int R, int ST>
+__global__ void __launch_bounds__(CTA_THREADS, HP_F32_MIN_BLOCKS) propagate_kernel(BatchList bl, SolveConsts sc,
+                                                                                   int iteration, int color) {
+    constexpr int WARPS = CTA_THREADS / 32;
     __shared__ float s_ref[MAX_TW * MAX_TH];
+    __shared__ float s_cost[WARPS][32 * 4];
+    __shared__ unsigned char s_items[WARPS][32 * 4];
     int tile_x, tile_y;
     const ViewDesc* v = locate_tile(bl, blockIdx.x, &tile_x, &tile_y);
-    const int r = sc.radius, tw = TILE_W + 2 * r, th = TILE_H + 2 * r;
+    constexpr int tw = TILE_W + 2 * R, th = TILE_H + 2 * R;
     const int x0 = tile_x * TILE_W, y0 = tile_y * TILE_H;
-    load_ref_tile(s_ref, tw, th, v, x0, y0, r);
+    load_ref_tile(s_ref, tw, th, v, x0, y0, R);
     __syncthreads();
     const int W = v->W, H = v->H;
     const int ly = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int y = y0 + ly;
-    const int lx = 2 * lane + ((y + color) & 1);
+    if (y >= H) return;  // uniform per warp
+    const int parity = (y + color) & 1;
+    const int lx = 2 * lane + parity;
     const int x = x0 + lx;
-    if (y >= H || x >= W) return;
+    const bool active = x < W;
     const size_t idx = static_cast<size_t>(y) * W + x;
     const float dmin = v->dmin, dmax = v->dmax;
 
-    float4 best = v->hyp[idx];
-    float best_cost = v->cost[idx];
-
-    // Neighbour hypotheses, left, right, up, down (patchmatch_mvs.cu:551-580).
-    // A candidate bit-identical to the current best or to one already tried
-    // at this visit cannot win (its cost is the same number), so it is skipped.
-    float4 tried[4];
-    int n_tried = 0;
+    float4 best = make_float4(0.f, 0.f, 0.f, 0.f);
+    float best_cost = 0.f;
+    unsigned need = 0;
+    if (active) {
+        best = v->hyp[idx];
+        best_cost = v->cost[idx];
 #pragma unroll
-    for (int n = 0; n < 4; ++n) {
-        const int nxp = x + (n == 0 ? -1 : (n == 1 ? 1 : 0));
-        const int nyp = y + (n == 2 ? -1 : (n == 3 ? 1 : 0));
-        if (nxp < 0 || nxp >= W || nyp < 0 || nyp >= H) continue;
-        const float4 h = v->hyp[static_cast<size_t>(nyp) * W + nxp];
-        if (h.x < dmin || h.x > dmax) continue;
-        bool dup = same_plane(h, best);
+        for (int cand = 0; cand < 4; ++cand) {
+            const int nxp = x + (cand == 0 ? -1 : (cand == 1 ? 1 : 0));
+            const int nyp = y + (cand == 2 ? -1 : (cand == 3 ? 1 : 0));
+            if (nxp < 0 || nxp >= W || nyp < 0 || nyp >= H) continue;
+            const float4 h = v->hyp[static_cast<size_t>(nyp) * W + nxp];
+            if (h.x < dmin || h.x > dmax) continue;
+            bool dup = same_plane(h, best);
+            for (int j = 0; j < cand && !dup; ++j) {
+                if (need & (1u << j)) {
+                    const int jx = x + (j == 0 ? -1 : (j == 1 ? 1 : 0));
+                    const int jy = y + (j == 2 ? -1 : (j == 3 ? 1 : 0));
+                    dup = same_plane(h, v->hyp[static_cast<size_t>(jy) * W + jx]);
+                }
+            }
+            if (!dup) need |= 1u << cand;
+        }
+    }
+    // Warp-wide exclusive scan of the item counts; owners write their items.
+    const int cnt = __popc(need);
+    int incl = cnt;
 #pragma unroll
-        for (int j = 0; j < 4; ++j) dup |= (j < n_tried) && same_plane(h, tried[j]);
-        if (dup) continue;
-        tried[n_tried++] = h;
-        const float c = cost_f32<ST>(s_ref, tw, lx, ly, x, y, h.x, h.y, h.z, h.w, v, r, sc.top_k);
-        if (c < best_cost) {
-            best_cost = c;
-            best = h;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    {
+        int k = incl - cnt;
+        for (int cand = 0; cand < 4; ++cand)
+            if (need & (1u << cand)) s_items[ly][k++] = static_cast<unsigned char>((lane << 2) | cand);
+    }
+    __syncwarp();
+    for (int base = 0; base < total; base += 32) {
+        const int w = base + lane;
+        if (w < total) {
+            const int item = s_items[ly][w];
+            const int owner = item >> 2, cand = item & 3;
+            const int olx = 2 * owner + parity, ox = x0 + olx;
+            const int nxp = ox + (cand == 0 ? -1 : (cand == 1 ? 1 : 0));
+            const int nyp = y + (cand == 2 ? -1 : (cand == 3 ? 1 : 0));
+            const float4 h = v->hyp[static_cast<size_t>(nyp) * W + nxp];
+            s_cost[ly][item] = cost_f32<R, ST>(s_ref, tw, olx, ly, ox, y, h.x, h.y, h.z, h.w, v, sc.top_k);
+        }
+    }
+    __syncwarp();
+    if (!active) return;
+#pragma unroll
+    for (int cand = 0; cand < 4; ++cand) {
+        if (need & (1u << cand)) {
+            const float c = s_cost[ly][(lane << 2) | cand];
+            if (c < best_cost) {
+                const int nxp = x + (cand == 0 ? -1 : (cand == 1 ? 1 : 0));
+                const int nyp = y + (cand == 2 ? -1 : (cand == 3 ? 1 : 0));
+                best_cost = c;
+                best = v->hyp[static_cast<size_t>(nyp) * W + nxp];
+            }
         }
     }
 
-    // Random refinement around the running best (patchmatch_mvs.cu:583-648).
+    // Random refinement around the running best.
     const float3 ray = view_ray(v->kinv, x, y);
     float drange = __fmul_rn(__fsub_rn(dmax, dmin), 0.5f);
     float nrange = 1.0f;
@@ -281,7 +372,7 @@ __global__ void __launch_bounds__(CTA_THREADS) propagate_kernel(BatchList bl, So
         const float cz = __fmaf_rn(__fmaf_rn(u01(rr.w), 2.0f, -1.0f), nrange, best.w);
         float3 cn = normalize3_rn(cx, cy, cz);
         if (dot3_rn(cn, ray) > 0.0f) cn = make_float3(-cn.x, -cn.y, -cn.z);
-        const float c = cost_f32<ST>(s_ref, tw, lx, ly, x, y, cd, cn.x, cn.y, cn.z, v, r, sc.top_k);
+        const float c = cost_f32<R, ST>(s_ref, tw, lx, ly, x, y, cd, cn.x, cn.y, cn.z, v, sc.top_k);
         if (c < best_cost) {
             best_cost = c;
             best = make_float4(cd, cn.x, cn.y, cn.z);
@@ -293,6 +384,37 @@ __global__ void __launch_bounds__(CTA_THREADS) propagate_kernel(BatchList bl, So
     v->cost[idx] = best_cost;
 }
 
+template <int R, int ST>
+cudaError_t launch_rs(const BatchList& bl, const SolveConsts& sc, int iteration, int color, bool full,
+                      cudaStream_t st) {
+    if (full)
+        cost_kernel<R, ST><<<bl.total_tiles, CTA_THREADS, 0, st>>>(bl, sc);
+    else
+        propagate_kernel<R, ST><<<bl.total_tiles, CTA_THREADS, 0, st>>>(bl, sc, iteration, color);
+    return cudaGetLastError();
+}
+
+cudaError_t dispatch_f32(const BatchList& bl, const SolveConsts& sc, int iteration, int color, bool full,
+                         cudaStream_t st) {
+    if (bl.total_tiles <= 0) return cudaSuccess;
+    if (sc.stride != 1 && sc.stride != 2) return cudaErrorInvalidValue;
+#define HP_CASE(RR)                                                                  \
+    case RR:                                                                         \
+        return sc.stride == 1 ? launch_rs<RR, 1>(bl, sc, iteration, color, full, st) \
+                              : launch_rs<RR, 2>(bl, sc, iteration, color, full, st);
+    switch (sc.radius) {
+        HP_CASE(1)
+        HP_CASE(2)
+        HP_CASE(3)
+        HP_CASE(4)
+        HP_CASE(5)
+        HP_CASE(6)
+        HP_CASE(7)
+        default: return cudaErrorInvalidValue;
+    }
+#undef HP_CASE
+}
+
 }  // namespace
 
 cudaError_t launch_init(const BatchList& bl, cudaStream_t st) {
@@ -302,26 +424,12 @@ cudaError_t launch_init(const BatchList& bl, cudaStream_t st) {
 }
 
 cudaError_t launch_cost_f32(const BatchList& bl, const SolveConsts& sc, cudaStream_t st) {
-    if (bl.total_tiles <= 0) return cudaSuccess;
-    if (sc.stride == 1)
-        cost_kernel<1><<<bl.total_tiles, CTA_THREADS, 0, st>>>(bl, sc);
-    else if (sc.stride == 2)
-        cost_kernel<2><<<bl.total_tiles, CTA_THREADS, 0, st>>>(bl, sc);
-    else
-        return cudaErrorInvalidValue;
-    return cudaGetLastError();
+    return dispatch_f32(bl, sc, 0, 0, true, st);
 }
 
 cudaError_t launch_propagate_f32(const BatchList& bl, const SolveConsts& sc, int iteration, int color,
                                  cudaStream_t st) {
-    if (bl.total_tiles <= 0) return cudaSuccess;
-    if (sc.stride == 1)
-        propagate_kernel<1><<<bl.total_tiles, CTA_THREADS, 0, st>>>(bl, sc, iteration, color);
-    else if (sc.stride == 2)
-        propagate_kernel<2><<<bl.total_tiles, CTA_THREADS, 0, st>>>(bl, sc, iteration, color);
-    else
-        return cudaErrorInvalidValue;
-    return cudaGetLastError();
+    return dispatch_f32(bl, sc, iteration, color, false, st);
 }
 
 }  // namespace hp

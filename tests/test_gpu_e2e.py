@@ -91,6 +91,19 @@ def test_deterministic_and_batch_invariant(hp, ctx, ids_full, full_scene, precis
         assert np.array_equal(a, b) and np.array_equal(a, c)
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_stored_cost_equals_recomputed_cost(hp, ctx, ids_full, full_scene, precision):
+    """The cost a solve stores for a pixel is bit-identical to what the full-map cost kernel
+    computes for the final plane.  The propagate kernel relies on this when it skips a neighbour
+    plane equal to the current one: re-scoring it could not produce a lower number."""
+    s = full_scene
+    p = hp.default_params(radius=5, stride=2, precision=precision)
+    d, n, c = solve(hp, ctx, s, ids_full, [2], p, iterations=3)[0]
+    again = np.zeros_like(c)
+    ctx.ncc_cost(job_for(hp, s, ids_full, 2), p, hp.maps_of(d, n, again))
+    assert np.array_equal(c, again)
+
+
 def test_uneven_iterations_in_one_batch(hp, ctx, ids_full, full_scene):
     s = full_scene
     p = hp.default_params(radius=5, stride=2)
