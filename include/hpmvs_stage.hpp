@@ -1,0 +1,147 @@
+// hpmvs_stage.hpp - header-only C++ adapter: the reference's dense stage
+//     std::vector<DepthMap> runPatchMatchMVS(images, cameras, sfm, config)
+// (src/dense_recon/patchmatch_mvs.h:39-44) implemented on the B200 engine's
+// C ABI (hpmvs.h).  It is meant to be included by the reference's
+// patchmatch_mvs.cu, whose data model (types.h: ImageData, CameraPose,
+// DepthMap, PipelineConfig; sfm/camera_pose.h: SfMResult) and host-side
+// selectSourceViews it uses; it compiles wherever those headers do.
+//
+// Behaviour follows runPatchMatchMVS (:1028-1388): sources and depth range from
+// selectSourceViews, radius (mvs_patch_size - 1) / 2 (clamped to the engine's
+// 1..7 instead of the reference's 1..5), per-view seed 42 + 1e6 * ref_id,
+// confidence 1 - cost / 2, then the in-place geometric filter (tolerance 0.12,
+// normal check off, 2 agreeing views) when iterations > 0 and >= 2 maps, PFM
+// depth per view when save_intermediate.  Not done: the SfM-point seeding of
+// the initial hypotheses (:1111-1177).  Errors are reported by return value
+// (an empty vector and `*status`), never by exit().
+#pragma once
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "hpmvs.h"
+
+namespace hpmvs_stage {
+
+inline hp_camera to_hp_camera(const CameraPose& c) {
+    hp_camera h;
+    for (int r = 0; r < 3; ++r) {
+        for (int k = 0; k < 3; ++k) {
+            h.K[3 * r + k] = c.K(r, k);
+            h.R[3 * r + k] = c.R(r, k);
+        }
+        h.t[r] = c.t(r);
+    }
+    return h;
+}
+
+inline std::vector<DepthMap> runPatchMatchMVS(const std::vector<ImageData>& images,
+                                              const std::vector<CameraPose>& cameras, const SfMResult& sfm,
+                                              const PipelineConfig& config, hp_status* status = nullptr) {
+    hp_status st_local = HP_OK;
+    hp_status& st = status ? *status : st_local;
+    std::vector<DepthMap> maps;
+    const int num_sources = std::min(HP_MAX_SOURCES, std::max(3, sfm.num_registered - 1));
+    std::vector<MVSViewParams> views = selectSourceViews(sfm, num_sources);
+
+    hp_ctx* ctx = nullptr;
+    if ((st = hp_ctx_create(config.gpu_id, &ctx)) != HP_OK) return maps;
+    std::vector<int> ids(images.size(), -1);
+    auto upload = [&](int i) -> bool {
+        if (ids[i] >= 0) return true;
+        const cv::Mat& g = images[i].gray;  // CV_32F in [0, 1]
+        st = hp_image_upload(ctx, g.data, HP_MEMORY_HOST, g.cols, g.rows, HP_DTYPE_F32, &ids[i]);
+        return st == HP_OK;
+    };
+
+    hp_params params;
+    hp_params_default(&params);
+    params.radius = std::min(HP_MAX_RADIUS, std::max(1, (config.mvs_patch_size - 1) / 2));
+
+    std::vector<hp_job> jobs;
+    std::vector<const MVSViewParams*> solved;
+    for (const MVSViewParams& vp : views) {
+        if (vp.source_views.empty()) continue;  // :1089-1092
+        if (!upload(vp.ref_image_id)) break;
+        hp_job j;
+        std::memset(&j, 0, sizeof j);
+        j.ref_image = ids[vp.ref_image_id];
+        j.ref_cam = to_hp_camera(cameras[vp.ref_image_id]);
+        j.num_sources = static_cast<int>(std::min<size_t>(vp.source_views.size(), HP_MAX_SOURCES));
+        for (int s = 0; s < j.num_sources; ++s) {
+            const int id = vp.source_views[s].image_id;
+            if (!upload(id)) break;
+            j.src_images[s] = ids[id];
+            j.src_cams[s] = to_hp_camera(cameras[id]);
+        }
+        if (st != HP_OK) break;
+        j.depth_min = vp.depth_min;
+        j.depth_max = vp.depth_max;
+        j.seed = 42ull + static_cast<uint64_t>(vp.ref_image_id) * 1000000ull;  // :1106
+        j.view_id = static_cast<uint32_t>(vp.ref_image_id);
+        j.iterations = config.mvs_iterations;
+        jobs.push_back(j);
+        solved.push_back(&vp);
+    }
+    std::vector<hp_maps> out(jobs.size());
+    for (size_t k = 0; st == HP_OK && k < jobs.size(); ++k) {
+        const ImageData& img = images[solved[k]->ref_image_id];
+        DepthMap dm;
+        dm.image_id = solved[k]->ref_image_id;
+        dm.width = img.width;
+        dm.height = img.height;
+        dm.depth = cv::Mat(img.height, img.width, CV_32F);
+        dm.normal = cv::Mat(img.height, img.width, CV_32FC3);
+        dm.confidence = cv::Mat(img.height, img.width, CV_32F);
+        maps.push_back(dm);
+        out[k].memory = HP_MEMORY_HOST;
+        out[k].depth = reinterpret_cast<float*>(maps.back().depth.data);
+        out[k].normal = reinterpret_cast<float*>(maps.back().normal.data);
+        out[k].cost = reinterpret_cast<float*>(maps.back().confidence.data);  // converted below
+    }
+    if (st == HP_OK && !jobs.empty())
+        st = hp_solve(ctx, jobs.data(), static_cast<int>(jobs.size()), &params, out.data());
+    if (st == HP_OK) {
+        for (DepthMap& dm : maps) {  // confidence = 1 - cost / 2 (:1246-1252)
+            float* c = reinterpret_cast<float*>(dm.confidence.data);
+            for (int p = 0; p < dm.width * dm.height; ++p) c[p] = 1.0f - c[p] * 0.5f;
+        }
+        if (config.mvs_iterations > 0 && maps.size() >= 2) {  // :1267-1384, in place, in view order
+            for (size_t k = 0; st == HP_OK && k < maps.size(); ++k) {
+                std::vector<hp_camera> cams;
+                std::vector<const float*> sd, sn;
+                for (const SourceViewInfo& sv : solved[k]->source_views) {
+                    for (size_t m = 0; m < maps.size(); ++m)
+                        if (maps[m].image_id == sv.image_id && maps[m].width == maps[k].width &&
+                            maps[m].height == maps[k].height && cams.size() < HP_MAX_SOURCES) {
+                            cams.push_back(to_hp_camera(cameras[sv.image_id]));
+                            sd.push_back(reinterpret_cast<const float*>(maps[m].depth.data));
+                            sn.push_back(reinterpret_cast<const float*>(maps[m].normal.data));
+                        }
+                }
+                if (cams.size() < 2) continue;
+                hp_camera ref = to_hp_camera(cameras[maps[k].image_id]);
+                st = hp_geometric_filter(ctx, &ref, maps[k].width, maps[k].height,
+                                         reinterpret_cast<float*>(maps[k].depth.data),
+                                         reinterpret_cast<const float*>(maps[k].normal.data),
+                                         reinterpret_cast<float*>(maps[k].confidence.data),
+                                         static_cast<int>(cams.size()), cams.data(), sd.data(), sn.data(),
+                                         HP_MEMORY_HOST, 0.12f, -1.0f /* cos(180 deg): normal check off */, 2);
+            }
+        }
+        if (config.save_intermediate && !config.output_path.empty()) {
+            const std::string dir = config.output_path.substr(0, config.output_path.find_last_of('/'));
+            for (const DepthMap& dm : maps)
+                hp_pfm_write((dir + "/depth_" + std::to_string(dm.image_id) + ".pfm").c_str(),
+                             reinterpret_cast<const float*>(dm.depth.data), dm.width, dm.height, 1);
+        }
+    }
+    hp_ctx_destroy(ctx);
+    if (st != HP_OK) maps.clear();
+    return maps;
+}
+
+}  // namespace hpmvs_stage
