@@ -107,6 +107,8 @@ def _load() -> C.CDLL:
         "hp_geometric_filter": (C.c_int, [C.c_void_p, P(Camera), C.c_int, C.c_int, C.c_void_p, C.c_void_p,
                                           C.c_void_p, C.c_int, P(Camera), P(C.c_void_p), P(C.c_void_p),
                                           C.c_int, C.c_float, C.c_float, C.c_int]),
+        "hp_solve_static": (C.c_int, [C.c_int, C.c_void_p, P(Job), C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                      P(C.c_ulonglong), P(Params), P(Maps)]),
         "hp_pfm_write": (C.c_int, [C.c_char_p, C.c_void_p, C.c_int, C.c_int, C.c_int]),
         "hp_pfm_read": (C.c_int, [C.c_char_p, C.c_void_p, C.c_size_t, P(C.c_int), P(C.c_int), P(C.c_int)]),
     }
@@ -125,8 +127,23 @@ EXPORTS = (
     "hp_ctx_last_error", "hp_ctx_synchronize", "hp_ctx_mem_info", "hp_ctx_stream", "hp_ctx_set_profiling",
     "hp_ctx_profile", "hp_ctx_profile_reset", "hp_image_upload", "hp_image_release",
     "hp_image_size", "hp_setup_homographies", "hp_solve", "hp_init_hypotheses", "hp_ncc_cost",
-    "hp_propagate_pass", "hp_geometric_filter", "hp_pfm_write", "hp_pfm_read",
+    "hp_propagate_pass", "hp_geometric_filter", "hp_pfm_write", "hp_pfm_read", "hp_solve_static",
 )
+STATIC_MAX_PIXELS = 1280 * 1024  # HP_STATIC_MAX_PIXELS
+
+
+def solve_static(job: Job, params: Params, ref_image, src_textures: Sequence[int], out: Maps, device: int = 0,
+                 stream: int = 0):
+    """hp_solve_static: the single-view FP32 solve for callers that cannot let the library allocate device
+    memory.  ``ref_image`` is a contiguous device FP32 tensor (H, W); ``src_textures`` are texture-object
+    handles over the FP32 source images (linear filter, clamp, unnormalised coordinates); ``out`` holds device
+    maps.  No device memory is allocated: the state lives in a fixed array of HP_STATIC_MAX_PIXELS pixels."""
+    h, w = ref_image.shape
+    tex = (C.c_ulonglong * len(src_textures))(*src_textures)
+    st = lib.hp_solve_static(device, stream or None, C.byref(job), int(ref_image.data_ptr()), w, w, h, tex,
+                             C.byref(params), C.byref(out))
+    if st != OK:
+        raise HpError(st, "hp_solve_static")
 
 
 def default_params(**kw) -> Params:

@@ -209,6 +209,36 @@ hp_status hp_geometric_filter(hp_ctx* ctx, const hp_camera* ref_cam, int width, 
                               int memory, float depth_tol, float normal_tol_cos,
                               int min_consistent);
 
+/* Largest view hp_solve_static accepts (width * height), fixed by its
+ * statically sized device scratch: 20 bytes per pixel, 26.2 MB in all. */
+#define HP_STATIC_MAX_PIXELS (1280 * 1024)
+
+/* No counterpart in the reference.  The single-view FP32 solve of hp_solve
+ * (random init, initial cost, `iterations` red-black passes, same kernels and
+ * results) for callers that must not have the library allocate device memory:
+ * applications whose device memory is owned by their own pool or budget, or
+ * latency-critical loops that cannot afford cudaMalloc/cudaFree and the
+ * synchronisation they bring.  It calls no allocation routine: the plane
+ * state, costs and launch descriptors live in one file-scope device array of
+ * fixed size that every GPU loading the library holds until exit, so views
+ * larger than HP_STATIC_MAX_PIXELS are rejected with HP_ERR_UNSUPPORTED.
+ *   device, stream    where to run (stream may be NULL); waits for completion
+ *   job               cameras or use_coeffs, depth range, seed, view_id,
+ *                     iterations, num_sources (its image ids are ignored)
+ *   ref_image         device FP32 reference image, values in [0,1], row pitch
+ *                     ref_pitch floats
+ *   src_textures      num_sources cudaTextureObject_t over the FP32 source
+ *                     images (same size): linear filter, clamp addressing,
+ *                     unnormalised coordinates, element read mode
+ *   params            precision must be HP_PRECISION_F32
+ *   out               device maps (memory HP_MEMORY_DEVICE)
+ * The first call on a device looks up the scratch array's address; make it
+ * before any stream capture.  All calls share the one array, so calls that
+ * overlap in time (several host threads) race: serialise them. */
+hp_status hp_solve_static(int device, void* stream, const hp_job* job, const float* ref_image, int ref_pitch,
+                          int width, int height, const unsigned long long* src_textures, const hp_params* params,
+                          hp_maps* out);
+
 /* Replaces saveDepthMapPFM / loadDepthMapPFM (patchmatch_mvs.cu:990-1022):
  * 'Pf' (channels 1) or 'PF' (channels 3) little-endian PFM, rows bottom-up. */
 hp_status hp_pfm_write(const char* path, const float* data, int width, int height, int channels);
