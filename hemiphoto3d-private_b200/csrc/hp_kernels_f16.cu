@@ -18,9 +18,9 @@
 //    windows of up to 64 taps.  Window sums use mean-shifted values
 //    (compensated variance): FP16 products and per-row FP16 partial sums,
 //    flushed into FP32 accumulators every row.
-//  - Windows touching the source border take a checked FP32 path with the
+//  - Windows touching the source border mask invalid taps per the
 //    reference's validity rules (|w_z| >= 1e-8, u in [0, W-1), v in [0, H-1),
-//    count >= taps/2) on mean-shifted sums.
+//    count >= taps/2), vectorised like the fast path.
 #include <cuda_fp16.h>
 
 #include "hp_internal.h"
@@ -83,15 +83,15 @@ __device__ __forceinline__ RefStats load_window(__half2* s_win, const float* s_r
 #pragma unroll 1
     for (int i = 0; i < SIDE; ++i)
 #pragma unroll
-        for (int j = 0; j < SIDE; ++j) sum += s_ref[(ly + i * ST) * tw + lx + j * ST];
-    const float mean = sum * (1.0f / Win<R, ST>::N);
+        for (int j = 0; j < SIDE; ++j) sum = __fadd_rn(sum, s_ref[(ly + i * ST) * tw + lx + j * ST]);
+    const float mean = __fmul_rn(sum, 1.0f / Win<R, ST>::N);
     float ssd = 0.f;
 #pragma unroll 1
     for (int i = 0; i < SIDE; ++i)
 #pragma unroll
         for (int j = 0; j < SIDE; ++j) {
-            const float d = s_ref[(ly + i * ST) * tw + lx + j * ST] - mean;
-            ssd = fmaf(d, d, ssd);
+            const float d = __fsub_rn(s_ref[(ly + i * ST) * tw + lx + j * ST], mean);
+            ssd = __fmaf_rn(d, d, ssd);
         }
     if constexpr (Win<R, ST>::IN_SMEM) {
         constexpr int PAIRS = Win<R, ST>::PAIRS;
@@ -99,8 +99,9 @@ __device__ __forceinline__ RefStats load_window(__half2* s_win, const float* s_r
         for (int i = 0; i < SIDE; ++i)
 #pragma unroll
             for (int p = 0; p < PAIRS; ++p) {
-                const float a = s_ref[(ly + i * ST) * tw + lx + (2 * p) * ST] - mean;
-                const float b = (2 * p + 1 < SIDE) ? s_ref[(ly + i * ST) * tw + lx + (2 * p + 1) * ST] - mean : 0.f;
+                const float a = __fsub_rn(s_ref[(ly + i * ST) * tw + lx + (2 * p) * ST], mean);
+                const float b =
+                    (2 * p + 1 < SIDE) ? __fsub_rn(s_ref[(ly + i * ST) * tw + lx + (2 * p + 1) * ST], mean) : 0.f;
                 s_win[(i * PAIRS + p) * CTA_THREADS + threadIdx.x] = __floats2half2_rn(a, b);
             }
     }
@@ -119,105 +120,110 @@ struct Plane {
     float h[9];  // homography with the +0.5 texel offset folded into rows 0, 1
 };
 
-// Checked FP32 evaluation of one source (border windows): reference validity
-// rules, mean-shifted sums.  Returns the source cost (1 - NCC or 2).
-template <int R, int ST>
-__device__ __noinline__ float source_cost_checked(const Plane& P, cudaTextureObject_t tex, float c0,
-                                                  const float* s_ref, int tw, int lx, int ly, int x, int y, float fW,
-                                                  float fH) {
-    constexpr int SIDE = Win<R, ST>::SIDE;
-    float sr = 0.f, ss = 0.f, srr = 0.f, sss = 0.f, srs = 0.f;
-    int count = 0;
-    for (int i = 0; i < SIDE; ++i) {
-        const float py = static_cast<float>(y - R + i * ST);
-        for (int j = 0; j < SIDE; ++j) {
-            const float px = static_cast<float>(x - R + j * ST);
-            const float wz = fmaf(P.h[6], px, fmaf(P.h[7], py, P.h[8]));
-            if (fabsf(wz) < 1e-8f) continue;
-            const float iz = __frcp_rn(wz);
-            const float u = fmaf(P.h[0], px, fmaf(P.h[1], py, P.h[2])) * iz;  // = u_ref + 0.5
-            const float v = fmaf(P.h[3], px, fmaf(P.h[4], py, P.h[5])) * iz;
-            if (u < 0.5f || u >= fW - 0.5f || v < 0.5f || v >= fH - 0.5f) continue;
-            const float sv = tex2D<float>(tex, u, v) - c0;
-            const float rv = s_ref[(ly + i * ST) * tw + lx + j * ST] - c0;
-            sr += rv;
-            ss += sv;
-            srr = fmaf(rv, rv, srr);
-            sss = fmaf(sv, sv, sss);
-            srs = fmaf(rv, sv, srs);
-            ++count;
-        }
-    }
-    if (count < Win<R, ST>::N / 2) return 2.0f;
-    const float n = static_cast<float>(count);
-    const float num = fmaf(n, srs, -sr * ss);
-    const float dr = fmaf(n, srr, -sr * sr);
-    const float ds = fmaf(n, sss, -ss * ss);
-    if (dr < 1e-6f || ds < 1e-6f) return 2.0f;
-    const float ncc = fmaxf(-1.0f, fminf(1.0f, num * rsqrtf(dr) * rsqrtf(ds)));
-    return 1.0f - ncc;
-}
-
-// Fast path: all taps valid.  Sums of e = s - mean and products (r - mean) e
-// in FP16 per row, flushed to FP32.
-template <int R, int ST>
-__device__ __forceinline__ float source_cost_fast(const Plane& P, cudaTextureObject_t tex, RefStats st,
-                                                  const __half2* s_win, const float* s_ref, int tw, int lx, int ly,
-                                                  int x, int y) {
+// Cost (1 - NCC, or 2 when invalid) of one source.  Sums of e = s - mean and
+// products (r - mean) e are formed in FP16 per window row and flushed to FP32.
+// CHECK = false assumes every tap is valid (the caller's corner test proved
+// it); CHECK = true applies the reference's validity rules per tap
+// (|w_z| >= 1e-8, u in [0, W-1), v in [0, H-1), count >= taps/2) by masking
+// the tap's terms.  Each lane picks its form from its own corner test, so a
+// pixel's cost never depends on which other pixels share its warp.
+template <int R, int ST, bool CHECK>
+__device__ __forceinline__ float source_cost(const Plane& P, cudaTextureObject_t tex, RefStats st,
+                                             const __half2* s_win, const float* s_ref, int tw, int lx, int ly, int x,
+                                             int y, float fW, float fH) {
     constexpr int SIDE = Win<R, ST>::SIDE;
     constexpr int PAIRS = Win<R, ST>::PAIRS;
+    constexpr int N = Win<R, ST>::N;
     const float c0 = st.mean;
-    float s1 = 0.f, s2 = 0.f, s3 = 0.f;
+    float s1 = 0.f, s2 = 0.f, s3 = 0.f, r1 = 0.f, r2 = 0.f;
+    int count = 0;
     const float sx0 = static_cast<float>(x - R), sy0 = static_cast<float>(y - R);
-    const float hx0 = P.h[0] * ST, hx1 = P.h[3] * ST, hx2 = P.h[6] * ST;
-    const float rx0 = fmaf(P.h[0], sx0, P.h[2]), rx1 = fmaf(P.h[3], sx0, P.h[5]), rx2 = fmaf(P.h[6], sx0, P.h[8]);
+    const float hx0 = __fmul_rn(P.h[0], ST), hx1 = __fmul_rn(P.h[3], ST), hx2 = __fmul_rn(P.h[6], ST);
+    const float rx0 = __fmaf_rn(P.h[0], sx0, P.h[2]), rx1 = __fmaf_rn(P.h[3], sx0, P.h[5]);
+    const float rx2 = __fmaf_rn(P.h[6], sx0, P.h[8]);
 #pragma unroll 1
     for (int i = 0; i < SIDE; ++i) {
-        const float py = sy0 + static_cast<float>(i * ST);
-        float wx = fmaf(P.h[1], py, rx0);
-        float wy = fmaf(P.h[4], py, rx1);
-        float wz = fmaf(P.h[7], py, rx2);
+        const float py = __fadd_rn(sy0, static_cast<float>(i * ST));
+        float wx = __fmaf_rn(P.h[1], py, rx0);
+        float wy = __fmaf_rn(P.h[4], py, rx1);
+        float wz = __fmaf_rn(P.h[7], py, rx2);
         float smp[2 * PAIRS];
+        unsigned ok = (1u << SIDE) - 1u;
 #pragma unroll
         for (int j = 0; j < SIDE; ++j) {
             const float iz = rcp_approx(wz);
-            smp[j] = tex2D<float>(tex, wx * iz, wy * iz);
-            wx += hx0;
-            wy += hx1;
-            wz += hx2;
+            const float u = __fmul_rn(wx, iz), v = __fmul_rn(wy, iz);  // texel-centre offset already folded in
+            if constexpr (CHECK) {
+                const bool skip = fabsf(wz) < 1e-8f || u < 0.5f || u >= fW - 0.5f || v < 0.5f || v >= fH - 0.5f;
+                ok &= ~(static_cast<unsigned>(skip) << j);
+            }
+            smp[j] = tex2D<float>(tex, u, v);
+            wx = __fadd_rn(wx, hx0);
+            wy = __fadd_rn(wy, hx1);
+            wz = __fadd_rn(wz, hx2);
         }
         if constexpr (SIDE & 1) smp[SIDE] = c0;  // pads the last pair: e = 0
-        __half2 a1 = __float2half2_rn(0.f), a2 = a1, a3 = a1;
+        __half2 a1 = __float2half2_rn(0.f), a2 = a1, a3 = a1, a4 = a1, a5 = a1;
 #pragma unroll
         for (int p = 0; p < PAIRS; ++p) {
             // The shift is subtracted in FP32 and only the small residual is
             // rounded to FP16 (rounding the sample first would cost ~2.4e-4).
-            const __half2 e = __floats2half2_rn(smp[2 * p] - c0, smp[2 * p + 1] - c0);
+            float ea = __fsub_rn(smp[2 * p], c0), eb = __fsub_rn(smp[2 * p + 1], c0);
             __half2 rq;
             if constexpr (Win<R, ST>::IN_SMEM) {
                 rq = s_win[(i * PAIRS + p) * CTA_THREADS];  // s_win points at the pixel's column
             } else {
                 const float* row = s_ref + (ly + i * ST) * tw + lx;
-                const float ra = row[(2 * p) * ST] - c0;
-                const float rb = (2 * p + 1 < SIDE) ? row[(2 * p + 1) * ST] - c0 : 0.f;
+                const float ra = __fsub_rn(row[(2 * p) * ST], c0);
+                const float rb = (2 * p + 1 < SIDE) ? __fsub_rn(row[(2 * p + 1) * ST], c0) : 0.f;
                 rq = __floats2half2_rn(ra, rb);
             }
+            if constexpr (CHECK) {
+                const bool va = (ok >> (2 * p)) & 1u;
+                const bool vb = (2 * p + 1 < SIDE) && ((ok >> (2 * p + 1)) & 1u);
+                ea = va ? ea : 0.f;
+                eb = vb ? eb : 0.f;
+                // Bitwise mask (exact; a multiply by 1 would not preserve FP16 subnormals).
+                unsigned bits;
+                memcpy(&bits, &rq, sizeof bits);
+                bits &= (va ? 0x0000ffffu : 0u) | (vb ? 0xffff0000u : 0u);
+                memcpy(&rq, &bits, sizeof bits);
+            }
+            const __half2 e = __floats2half2_rn(ea, eb);
             a1 = __hadd2(a1, e);
             a2 = __hfma2(e, e, a2);
             a3 = __hfma2(rq, e, a3);
+            if constexpr (CHECK) {
+                a4 = __hadd2(a4, rq);
+                a5 = __hfma2(rq, rq, a5);
+            }
         }
         const float2 f1 = __half22float2(a1), f2 = __half22float2(a2), f3 = __half22float2(a3);
-        s1 += f1.x + f1.y;
-        s2 += f2.x + f2.y;
-        s3 += f3.x + f3.y;
+        s1 = __fadd_rn(s1, __fadd_rn(f1.x, f1.y));
+        s2 = __fadd_rn(s2, __fadd_rn(f2.x, f2.y));
+        s3 = __fadd_rn(s3, __fadd_rn(f3.x, f3.y));
+        if constexpr (CHECK) {
+            const float2 f4 = __half22float2(a4), f5 = __half22float2(a5);
+            r1 = __fadd_rn(r1, __fadd_rn(f4.x, f4.y));
+            r2 = __fadd_rn(r2, __fadd_rn(f5.x, f5.y));
+            count += __popc(ok);
+        }
     }
-    constexpr float n = static_cast<float>(Win<R, ST>::N);
-    // n*sum(r^2)-sum(r)^2 = n*ssd, n*sum(s^2)-sum(s)^2 = n*s2 - s1^2, cov numerator n*s3 (sum(r - mean) = 0).
-    const float dr = n * st.ssd;
-    const float ds = fmaf(n, s2, -s1 * s1);
+    float n = static_cast<float>(N), dr, num;
+    if (!CHECK || count == N) {
+        // n*sum(r^2)-sum(r)^2 = n*ssd and the covariance numerator is n*s3 (sum(r - mean) = 0).
+        dr = __fmul_rn(n, st.ssd);
+        num = __fmul_rn(n, s3);
+    } else {
+        if (count < N / 2) return 2.0f;
+        n = static_cast<float>(count);
+        dr = __fmaf_rn(n, r2, -__fmul_rn(r1, r1));
+        num = __fmaf_rn(n, s3, -__fmul_rn(r1, s1));
+    }
+    const float ds = __fmaf_rn(n, s2, -__fmul_rn(s1, s1));
     if (dr < 1e-6f || ds < 1e-6f) return 2.0f;
-    const float ncc = fmaxf(-1.0f, fminf(1.0f, n * s3 * rsqrtf(dr) * rsqrtf(ds)));
-    return 1.0f - ncc;
+    const float ncc = fmaxf(-1.0f, fminf(1.0f, __fmul_rn(__fmul_rn(num, rsqrtf(dr)), rsqrtf(ds))));
+    return __fsub_rn(1.0f, ncc);
 }
 
 template <int R, int ST>
@@ -226,15 +232,15 @@ __device__ __forceinline__ float cost_f16(RefStats st, const __half2* s_win, con
                                           const ViewDesc* __restrict__ v, int topk) {
     const float* k = v->kinv;
     const float fx = static_cast<float>(x), fy = static_cast<float>(y);
-    const float Px = d * fmaf(k[0], fx, fmaf(k[1], fy, k[2]));
-    const float Py = d * fmaf(k[3], fx, fmaf(k[4], fy, k[5]));
-    const float Pz = d * fmaf(k[6], fx, fmaf(k[7], fy, k[8]));
-    const float ndp = fmaf(cnx, Px, fmaf(cny, Py, cnz * Pz));
+    const float Px = __fmul_rn(d, __fmaf_rn(k[0], fx, __fmaf_rn(k[1], fy, k[2])));
+    const float Py = __fmul_rn(d, __fmaf_rn(k[3], fx, __fmaf_rn(k[4], fy, k[5])));
+    const float Pz = __fmul_rn(d, __fmaf_rn(k[6], fx, __fmaf_rn(k[7], fy, k[8])));
+    const float ndp = __fmaf_rn(cnx, Px, __fmaf_rn(cny, Py, __fmul_rn(cnz, Pz)));
     if (fabsf(ndp) < 1e-8f) return 2.0f;
     const float ind = __frcp_rn(ndp);
-    const float m0 = fmaf(k[0], cnx, fmaf(k[3], cny, k[6] * cnz)) * ind;
-    const float m1 = fmaf(k[1], cnx, fmaf(k[4], cny, k[7] * cnz)) * ind;
-    const float m2 = fmaf(k[2], cnx, fmaf(k[5], cny, k[8] * cnz)) * ind;
+    const float m0 = __fmul_rn(__fmaf_rn(k[0], cnx, __fmaf_rn(k[3], cny, __fmul_rn(k[6], cnz))), ind);
+    const float m1 = __fmul_rn(__fmaf_rn(k[1], cnx, __fmaf_rn(k[4], cny, __fmul_rn(k[7], cnz))), ind);
+    const float m2 = __fmul_rn(__fmaf_rn(k[2], cnx, __fmaf_rn(k[5], cny, __fmul_rn(k[8], cnz))), ind);
     const float fW = static_cast<float>(v->W), fH = static_cast<float>(v->H);
     const float xa = static_cast<float>(x - R), xb = static_cast<float>(x - R + (Win<R, ST>::SIDE - 1) * ST);
     const float ya = static_cast<float>(y - R), yb = static_cast<float>(y - R + (Win<R, ST>::SIDE - 1) * ST);
@@ -243,31 +249,33 @@ __device__ __forceinline__ float cost_f16(RefStats st, const __half2* s_win, con
     for (int s = 0; s < S; ++s) {
         const float* A = v->ab[s];
         Plane P;
-        P.h[6] = fmaf(A[11], m0, A[6]);
-        P.h[7] = fmaf(A[11], m1, A[7]);
-        P.h[8] = fmaf(A[11], m2, A[8]);
-        P.h[0] = fmaf(0.5f, P.h[6], fmaf(A[9], m0, A[0]));
-        P.h[1] = fmaf(0.5f, P.h[7], fmaf(A[9], m1, A[1]));
-        P.h[2] = fmaf(0.5f, P.h[8], fmaf(A[9], m2, A[2]));
-        P.h[3] = fmaf(0.5f, P.h[6], fmaf(A[10], m0, A[3]));
-        P.h[4] = fmaf(0.5f, P.h[7], fmaf(A[10], m1, A[4]));
-        P.h[5] = fmaf(0.5f, P.h[8], fmaf(A[10], m2, A[5]));
+        P.h[6] = __fmaf_rn(A[11], m0, A[6]);
+        P.h[7] = __fmaf_rn(A[11], m1, A[7]);
+        P.h[8] = __fmaf_rn(A[11], m2, A[8]);
+        P.h[0] = __fmaf_rn(0.5f, P.h[6], __fmaf_rn(A[9], m0, A[0]));
+        P.h[1] = __fmaf_rn(0.5f, P.h[7], __fmaf_rn(A[9], m1, A[1]));
+        P.h[2] = __fmaf_rn(0.5f, P.h[8], __fmaf_rn(A[9], m2, A[2]));
+        P.h[3] = __fmaf_rn(0.5f, P.h[6], __fmaf_rn(A[10], m0, A[3]));
+        P.h[4] = __fmaf_rn(0.5f, P.h[7], __fmaf_rn(A[10], m1, A[4]));
+        P.h[5] = __fmaf_rn(0.5f, P.h[8], __fmaf_rn(A[10], m2, A[5]));
         // Corner test (margin 1e-3 px): one-signed depth and all four corners inside.
         bool inside = true;
         float zsign = 0.f;
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             const float px = (c & 1) ? xb : xa, py = (c & 2) ? yb : ya;
-            const float wz = fmaf(P.h[6], px, fmaf(P.h[7], py, P.h[8]));
-            const float u = fmaf(P.h[0], px, fmaf(P.h[1], py, P.h[2])) / wz;
-            const float vv = fmaf(P.h[3], px, fmaf(P.h[4], py, P.h[5])) / wz;
+            const float wz = __fmaf_rn(P.h[6], px, __fmaf_rn(P.h[7], py, P.h[8]));
+            const float u = __fdiv_rn(__fmaf_rn(P.h[0], px, __fmaf_rn(P.h[1], py, P.h[2])), wz);
+            const float vv = __fdiv_rn(__fmaf_rn(P.h[3], px, __fmaf_rn(P.h[4], py, P.h[5])), wz);
             if (c == 0) zsign = wz;
-            inside = inside && (fabsf(wz) > 1e-6f) && (wz * zsign > 0.f) && u >= 0.501f && u < fW - 0.501f &&
+            inside = inside && (fabsf(wz) > 1e-6f) && (__fmul_rn(wz, zsign) > 0.f) && u >= 0.501f && u < fW - 0.501f &&
                      vv >= 0.501f && vv < fH - 0.501f;
         }
         const cudaTextureObject_t tex = v->src_tex16[s];
-        const float c = inside ? source_cost_fast<R, ST>(P, tex, st, s_win, s_ref, tw, lx, ly, x, y)
-                               : source_cost_checked<R, ST>(P, tex, st.mean, s_ref, tw, lx, ly, x, y, fW, fH);
+        // Per-lane choice: a pixel's cost depends only on its own window and plane.
+        const float c = inside
+                            ? source_cost<R, ST, false>(P, tex, st, s_win, s_ref, tw, lx, ly, x, y, fW, fH)
+                            : source_cost<R, ST, true>(P, tex, st, s_win, s_ref, tw, lx, ly, x, y, fW, fH);
         if (c < top2) {
             top2 = c;
             if (top2 < top1) {
@@ -278,9 +286,9 @@ __device__ __forceinline__ float cost_f16(RefStats st, const __half2* s_win, con
     }
     const int kk = min(topk, S);
     float sum = top0;
-    if (kk > 1) sum += top1;
-    if (kk > 2) sum += top2;
-    return sum / static_cast<float>(kk);
+    if (kk > 1) sum = __fadd_rn(sum, top1);
+    if (kk > 2) sum = __fadd_rn(sum, top2);
+    return __fdiv_rn(sum, static_cast<float>(kk));
 }
 
 __device__ __forceinline__ bool same_plane16(float4 a, float4 b) {
