@@ -66,15 +66,32 @@ class Maps(C.Structure):
     _fields_ = [("memory", C.c_int), ("depth", C.c_void_p), ("normal", C.c_void_p), ("cost", C.c_void_p)]
 
 
-KERNEL_KINDS = ("init", "cost", "propagate", "other")
+KERNEL_KINDS = ("init", "cost", "propagate", "other", "persistent")
 
 
 class Profile(C.Structure):
-    _fields_ = [("launches", C.c_uint64 * 4), ("device_ms", C.c_double * 4), ("timed", C.c_uint64 * 4)]
+    _fields_ = [("launches", C.c_uint64 * 5), ("device_ms", C.c_double * 5), ("timed", C.c_uint64 * 5)]
 
     def as_dict(self):
         return {k: {"launches": int(self.launches[i]), "device_ms": float(self.device_ms[i]),
                     "timed": int(self.timed[i])} for i, k in enumerate(KERNEL_KINDS)}
+
+
+SCHEDULE_AUTO, SCHEDULE_PER_PASS, SCHEDULE_PERSISTENT = 0, 1, 2
+
+
+class PlanOptions(C.Structure):
+    _fields_ = [("schedule", C.c_int), ("ctas_per_sm", C.c_int), ("use_graph", C.c_int),
+                ("wait_limit_ms", C.c_int), ("debug_stall_view", C.c_int), ("debug_stall_tile", C.c_int)]
+
+
+class PlanInfo(C.Structure):
+    _fields_ = [("schedule", C.c_int), ("ctas_per_sm", C.c_int), ("grid", C.c_int), ("max_ctas_per_sm", C.c_int),
+                ("tickets", C.c_int), ("launches_per_run", C.c_int), ("views", C.c_int), ("use_graph", C.c_int),
+                ("state_bytes", C.c_uint64), ("pixel_iterations", C.c_double), ("tuned_ms", C.c_float)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 def _load() -> C.CDLL:
@@ -109,6 +126,17 @@ def _load() -> C.CDLL:
                                           C.c_int, C.c_float, C.c_float, C.c_int]),
         "hp_solve_static": (C.c_int, [C.c_int, C.c_void_p, P(Job), C.c_void_p, C.c_int, C.c_int, C.c_int,
                                       P(C.c_ulonglong), P(Params), P(Maps)]),
+        "hp_plan_options_default": (None, [P(PlanOptions)]),
+        "hp_plan_create": (C.c_int, [C.c_void_p, P(Job), C.c_int, P(Params), P(PlanOptions), P(Maps),
+                                     P(C.c_void_p)]),
+        "hp_plan_run": (C.c_int, [C.c_void_p]),
+        "hp_plan_launch": (C.c_int, [C.c_void_p]),
+        "hp_plan_wait": (C.c_int, [C.c_void_p]),
+        "hp_plan_tune": (C.c_int, [C.c_void_p, C.c_int, P(PlanInfo)]),
+        "hp_plan_get_info": (C.c_int, [C.c_void_p, P(PlanInfo)]),
+        "hp_plan_destroy": (C.c_int, [C.c_void_p]),
+        "hp_schedule_build": (C.c_int, [C.c_int, P(C.c_int), P(C.c_int), P(C.c_int), C.c_int, P(C.c_int),
+                                        P(C.c_int), P(C.c_int), P(C.c_int)]),
         "hp_pfm_write": (C.c_int, [C.c_char_p, C.c_void_p, C.c_int, C.c_int, C.c_int]),
         "hp_pfm_read": (C.c_int, [C.c_char_p, C.c_void_p, C.c_size_t, P(C.c_int), P(C.c_int), P(C.c_int)]),
     }
@@ -128,6 +156,8 @@ EXPORTS = (
     "hp_ctx_profile", "hp_ctx_profile_reset", "hp_image_upload", "hp_image_release",
     "hp_image_size", "hp_setup_homographies", "hp_solve", "hp_init_hypotheses", "hp_ncc_cost",
     "hp_propagate_pass", "hp_geometric_filter", "hp_pfm_write", "hp_pfm_read", "hp_solve_static",
+    "hp_plan_options_default", "hp_plan_create", "hp_plan_run", "hp_plan_launch", "hp_plan_wait", "hp_plan_tune",
+    "hp_plan_get_info", "hp_plan_destroy", "hp_schedule_build",
 )
 STATIC_MAX_PIXELS = 1280 * 1024  # HP_STATIC_MAX_PIXELS
 
@@ -300,6 +330,79 @@ class Context:
         self._check(lib.hp_geometric_filter(self._h, C.byref(ref_cam), w, h, _ptr(depth), _ptr(normal),
                                             _ptr(confidence), n, cams, dps, nps, _mem(depth), depth_tol,
                                             normal_tol_cos, min_consistent), "hp_geometric_filter")
+
+
+def plan_options(**kw) -> PlanOptions:
+    o = PlanOptions()
+    lib.hp_plan_options_default(C.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+class Plan:
+    """A batched solve prepared once (hp_plan): jobs, params and output maps bound at creation."""
+
+    def __init__(self, ctx: "Context", jobs: Sequence[Job], params: Params, outs: Sequence[Maps],
+                 options: PlanOptions | None = None):
+        self.ctx = ctx
+        self._outs = list(outs)  # keep the Maps (and their arrays) alive
+        jarr = (Job * len(jobs))(*jobs)
+        marr = (Maps * len(outs))(*outs)
+        h = C.c_void_p()
+        opts = options if options is not None else plan_options()
+        ctx._check(lib.hp_plan_create(ctx.handle, jarr, len(jobs), C.byref(params), C.byref(opts), marr, C.byref(h)),
+                   "hp_plan_create")
+        self._h = h
+
+    def run(self):
+        self.ctx._check(lib.hp_plan_run(self._h), "hp_plan_run")
+
+    def launch(self):
+        self.ctx._check(lib.hp_plan_launch(self._h), "hp_plan_launch")
+
+    def wait(self):
+        self.ctx._check(lib.hp_plan_wait(self._h), "hp_plan_wait")
+
+    def tune(self, repeats: int = 3) -> dict:
+        info = PlanInfo()
+        self.ctx._check(lib.hp_plan_tune(self._h, repeats, C.byref(info)), "hp_plan_tune")
+        return info.as_dict()
+
+    def info(self) -> dict:
+        info = PlanInfo()
+        self.ctx._check(lib.hp_plan_get_info(self._h, C.byref(info)), "hp_plan_get_info")
+        return info.as_dict()
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.hp_plan_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def schedule_build(tiles: Sequence[int], stage_begin: Sequence[int], stage_end: Sequence[int]):
+    """The persistent ticket order (hp_schedule_build): arrays (entry_ticket[n+1], entry_view[n], entry_stage[n])."""
+    n = len(tiles)
+    cap = sum(max(0, e - b) for b, e in zip(stage_begin, stage_end)) + 1
+    arr = lambda xs: (C.c_int * max(1, len(xs)))(*xs)
+    et, ev, es, ne = (C.c_int * (cap + 1))(), (C.c_int * cap)(), (C.c_int * cap)(), C.c_int()
+    st = lib.hp_schedule_build(n, arr(tiles), arr(stage_begin), arr(stage_end), cap, et, ev, es, C.byref(ne))
+    if st != OK:
+        raise HpError(st, "hp_schedule_build")
+    k = ne.value
+    return np.array(et[:k + 1]), np.array(ev[:k]), np.array(es[:k])
 
 
 def make_job(ref_image: int, src_images: Sequence[int], ref_cam: Camera, src_cams: Sequence[Camera],

@@ -20,129 +20,11 @@
 #include <string>
 #include <vector>
 
-#include "hp_internal.h"
+#include "hp_host.h"
 
-
-namespace {
-
-struct Image {
-    int W = 0, H = 0;
-    float* f32 = nullptr;
-    size_t pitch32 = 0;  // bytes
-    __half* f16 = nullptr;
-    size_t pitch16 = 0;  // bytes
-    cudaArray_t arr32 = nullptr, arr16 = nullptr;
-    cudaTextureObject_t tex32 = 0, tex16 = 0;
-};
-
-// Grow-only device buffer.
-struct DevBuf {
-    void* p = nullptr;
-    size_t cap = 0;
-    cudaError_t ensure(size_t bytes) {
-        if (bytes <= cap) return cudaSuccess;
-        if (p) cudaFree(p);
-        p = nullptr;
-        cap = 0;
-        cudaError_t e = cudaMalloc(&p, bytes);
-        if (e == cudaSuccess) cap = bytes;
-        return e;
-    }
-    void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        cap = 0;
-    }
-};
-
-}  // namespace
-
-struct hp_ctx {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    std::string err;
-    std::map<int, Image> images;
-    int next_id = 1;
-    DevBuf state;   // hypotheses + costs of all jobs of a solve
-    DevBuf descs;   // ViewDesc array
-    DevBuf lists;   // active-view lists and tile prefixes
-    DevBuf staging; // host-memory results pass through here
-    // Profiler: launch counts always; with profiling on, CUDA events bracket
-    // each launch and are read back at the next synchronisation point.
-    bool profiling = false;
-    hp_profile prof{};
-    std::vector<cudaEvent_t> events;
-    std::vector<std::pair<int, size_t>> pending;  // (kind, index of the start event)
-    size_t events_used = 0;
-};
+using namespace hpx;
 
 namespace {
-
-// Run one launch, counted under `kind` and, when profiling, bracketed by events.
-template <class F>
-cudaError_t counted(hp_ctx* ctx, int kind, F&& launch) {
-    ctx->prof.launches[kind]++;
-    if (!ctx->profiling) return launch();
-    while (ctx->events.size() < ctx->events_used + 2) {
-        cudaEvent_t e;
-        cudaError_t err = cudaEventCreate(&e);
-        if (err != cudaSuccess) return err;
-        ctx->events.push_back(e);
-    }
-    const size_t i = ctx->events_used;
-    ctx->events_used += 2;
-    cudaEventRecord(ctx->events[i], ctx->stream);
-    cudaError_t err = launch();
-    cudaEventRecord(ctx->events[i + 1], ctx->stream);
-    ctx->pending.emplace_back(kind, i);
-    return err;
-}
-
-// Fold completed event pairs into the profile (call after a stream sync).
-void flush_profile(hp_ctx* ctx) {
-    for (auto& pk : ctx->pending) {
-        float ms = 0.f;
-        if (cudaEventElapsedTime(&ms, ctx->events[pk.second], ctx->events[pk.second + 1]) == cudaSuccess) {
-            ctx->prof.device_ms[pk.first] += ms;
-            ctx->prof.timed[pk.first]++;
-        }
-    }
-    ctx->pending.clear();
-    ctx->events_used = 0;
-}
-
-hp_status fail(hp_ctx* c, hp_status s, const char* fmt, ...) {
-    if (c) {
-        char buf[512];
-        va_list ap;
-        va_start(ap, fmt);
-        vsnprintf(buf, sizeof buf, fmt, ap);
-        va_end(ap);
-        c->err = buf;
-    }
-    return s;
-}
-
-#define HP_CUDA(call)                                                                              \
-    do {                                                                                           \
-        cudaError_t e_ = (call);                                                                   \
-        if (e_ != cudaSuccess)                                                                     \
-            return fail(ctx, e_ == cudaErrorMemoryAllocation ? HP_ERR_OUT_OF_MEMORY : HP_ERR_CUDA, \
-                        "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__);       \
-    } while (0)
-
-struct DeviceGuard {
-    int prev = -1;
-    explicit DeviceGuard(int dev) {
-        cudaGetDevice(&prev);
-        if (prev != dev) cudaSetDevice(dev);
-    }
-    ~DeviceGuard() {
-        int cur = -1;
-        cudaGetDevice(&cur);
-        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
-    }
-};
 
 void mat3_mul(const double* a, const double* b, double* c) {
     for (int r = 0; r < 3; ++r)
@@ -166,6 +48,10 @@ bool mat3_inv(const double* m, double* inv) {
     inv[8] = (m[0] * m[4] - m[1] * m[3]) * id;
     return true;
 }
+
+}  // namespace
+
+namespace hpx {
 
 hp_status check_params(hp_ctx* ctx, const hp_params* p) {
     if (!p) return fail(ctx, HP_ERR_INVALID_ARG, "params is null");
@@ -246,6 +132,10 @@ hp_status fill_desc(hp_ctx* ctx, const hp_job* j, int jobno, hp::ViewDesc* d) {
     d->iterations = j->iterations;
     return HP_OK;
 }
+
+}  // namespace hpx
+
+namespace {
 
 // Everything one solve needs on the device: descriptors, state, launch lists.
 struct Prepared {
@@ -393,6 +283,10 @@ hp_status launch_pass(hp_ctx* ctx, const hp::BatchList& bl, const hp_params* p, 
     return HP_OK;
 }
 
+}  // namespace
+
+namespace hpx {
+
 void free_image(Image& im) {
     if (im.tex32) cudaDestroyTextureObject(im.tex32);
     if (im.tex16) cudaDestroyTextureObject(im.tex16);
@@ -418,7 +312,7 @@ cudaError_t make_linear_texture(cudaArray_t arr, cudaTextureObject_t* tex) {
     return cudaCreateTextureObject(tex, &rd, &td, nullptr);
 }
 
-}  // namespace
+}  // namespace hpx
 
 extern "C" {
 

@@ -35,6 +35,13 @@ struct ViewDesc {
     float dmin, dmax;
     uint32_t seed_lo, seed_hi, view_id;
     int iterations;
+    // Persistent schedule only: per-tile completed-stage flags (tiles_x *
+    // tiles_y, -1 before stage 0) and, when set, the device maps the final
+    // stage unpacks into (depth H*W, normal H*W*3 camera frame, cost H*W).
+    int* done;
+    float* out_depth;
+    float* out_normal;
+    float* out_cost;
 };
 
 // Solver constants for one launch.
@@ -51,6 +58,40 @@ struct BatchList {
     const int* tile_prefix;     // n_active + 1 entries
     int n_active;
     int total_tiles;
+};
+
+// Persistent launch.  A view's work is a sequence of stages, each covering
+// all its tiles: stage 0 initialises the hypotheses and scores them, stage
+// 1 + 2*it + color is red-black half-pass (it, color), and stage
+// 2*iterations + 1, present when the view has output maps, unpacks its state
+// into them.  Tickets number (view, stage, tile) stage-major - every tile of
+// every view's stage k precedes any of stage k + 1 - and entry e of the
+// schedule is the run of tickets [entry_ticket[e], entry_ticket[e + 1]) of
+// view entry_info[e].x at stage entry_info[e].y.  A CTA takes tickets from an
+// atomic counter and, before running a stage k >= 1 tile, waits until that
+// tile and its four neighbour tiles have finished stage k - 1 (the half-pass
+// reads one pixel of halo).  Every ticket waited on is smaller than the
+// waiter's, so it is held by a CTA that is already running: progress needs no
+// co-residency guarantee.  The waiting thread's acquire load followed by the
+// CTA barrier orders the neighbours' earlier stores before every thread's
+// later plain loads (PTX memory model: release/acquire at gpu scope, then
+// bar.sync), so the stage bodies read state with ordinary loads.  Waits are
+// bounded by wait_limit_ns; a wait that
+// runs out records SCHED_TIMEOUT in status[0] and raises status[1], and every
+// CTA then stops taking tickets.
+constexpr int SCHED_OK = 0;
+constexpr int SCHED_TIMEOUT = 1;
+struct Schedule {
+    const ViewDesc* views;
+    const int* entry_ticket;      // n_entries + 1 (the last is the ticket total)
+    const int2* entry_info;       // (view, stage)
+    int n_entries;
+    int total;
+    unsigned* counter;            // next ticket
+    int* status;                  // [0] SCHED_* code, [1] abort flag
+    unsigned long long wait_limit_ns;
+    int stall_view, stall_tile;   // this tile never reports completion (bounded-wait test); -1 = none
+    SolveConsts sc;
 };
 
 // Geometric-filter launch arguments: FP32 cameras (cast from FP64 like the
@@ -77,6 +118,11 @@ cudaError_t launch_cost_f32(const BatchList& bl, const SolveConsts& sc, cudaStre
 cudaError_t launch_propagate_f32(const BatchList& bl, const SolveConsts& sc, int iteration, int color,
                                  cudaStream_t st);
 cudaError_t launch_cost_f16(const BatchList& bl, const SolveConsts& sc, cudaStream_t st);
+cudaError_t launch_persistent_f32(const Schedule& s, int grid, cudaStream_t st);
+cudaError_t launch_persistent_f16(const Schedule& s, int grid, cudaStream_t st);
+// Resident CTAs per SM of the persistent kernel for (radius, stride).
+cudaError_t persistent_occupancy_f32(int radius, int stride, int* blocks_per_sm);
+cudaError_t persistent_occupancy_f16(int radius, int stride, int* blocks_per_sm);
 cudaError_t launch_propagate_f16(const BatchList& bl, const SolveConsts& sc, int iteration, int color,
                                  cudaStream_t st);
 cudaError_t launch_unpack(const ViewDesc* views_host_copy, int view, float* depth, float* normal, float* cost,

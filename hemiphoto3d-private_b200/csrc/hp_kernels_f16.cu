@@ -25,6 +25,7 @@
 
 #include "hp_internal.h"
 #include "hp_rng.cuh"
+#include "hp_tile.cuh"
 
 #ifndef HP_F16_MIN_BLOCKS
 #define HP_F16_MIN_BLOCKS 3
@@ -297,11 +298,8 @@ __device__ __forceinline__ bool same_plane16(float4 a, float4 b) {
 }
 
 template <int R, int ST>
-__global__ void __launch_bounds__(CTA_THREADS, HP_F16_MIN_BLOCKS) cost16_kernel(BatchList bl, SolveConsts sc) {
-    __shared__ float s_ref[MAX_TW * MAX_TH];
-    __shared__ __half2 s_win[Win<R, ST>::IN_SMEM ? WIN_PAIRS_MAX * CTA_THREADS : 1];
-    int tile_x, tile_y;
-    const ViewDesc* v = locate_tile16(bl, blockIdx.x, &tile_x, &tile_y);
+__device__ __forceinline__ void tile_cost16(const ViewDesc* v, int tile_x, int tile_y, const SolveConsts& sc,
+                                            float* s_ref, __half2* s_win) {
     constexpr int tw = TILE_W + 2 * R, th = TILE_H + 2 * R;
     const int x0 = tile_x * TILE_W, y0 = tile_y * TILE_H;
     load_ref_tile16(s_ref, tw, th, v, x0, y0, R);
@@ -320,21 +318,26 @@ __global__ void __launch_bounds__(CTA_THREADS, HP_F16_MIN_BLOCKS) cost16_kernel(
     }
 }
 
+template <int R, int ST>
+__global__ void __launch_bounds__(CTA_THREADS, HP_F16_MIN_BLOCKS) cost16_kernel(BatchList bl, SolveConsts sc) {
+    __shared__ float s_ref[MAX_TW * MAX_TH];
+    __shared__ __half2 s_win[Win<R, ST>::IN_SMEM ? WIN_PAIRS_MAX * CTA_THREADS : 1];
+    int tile_x, tile_y;
+    const ViewDesc* v = locate_tile16(bl, blockIdx.x, &tile_x, &tile_y);
+    tile_cost16<R, ST>(v, tile_x, tile_y, sc, s_ref, s_win);
+}
+
 // One red-black half-pass.  The neighbour phase is compacted per warp exactly
 // as in the FP32 kernel (see propagate_kernel there): lanes list the
 // neighbour planes they must score, the warp scores the union 32 items at a
 // time (an item borrows its owner's window statistics by shuffle and the
 // owner's column of s_win), and owners fold the costs in L, R, U, D order.
+constexpr int WARPS = CTA_THREADS / 32;
+
 template <int R, int ST>
-__global__ void __launch_bounds__(CTA_THREADS, HP_F16_MIN_BLOCKS) propagate16_kernel(BatchList bl, SolveConsts sc,
-                                                                                     int iteration, int color) {
-    constexpr int WARPS = CTA_THREADS / 32;
-    __shared__ float s_ref[MAX_TW * MAX_TH];
-    __shared__ __half2 s_win[Win<R, ST>::IN_SMEM ? WIN_PAIRS_MAX * CTA_THREADS : 1];
-    __shared__ float s_cost[WARPS][32 * 4];
-    __shared__ unsigned char s_items[WARPS][32 * 4];
-    int tile_x, tile_y;
-    const ViewDesc* v = locate_tile16(bl, blockIdx.x, &tile_x, &tile_y);
+__device__ __forceinline__ void tile_propagate16(const ViewDesc* v, int tile_x, int tile_y, const SolveConsts& sc,
+                                                 int iteration, int color, float* s_ref, __half2* s_win,
+                                                 float (*s_cost)[32 * 4], unsigned char (*s_items)[32 * 4]) {
     constexpr int tw = TILE_W + 2 * R, th = TILE_H + 2 * R;
     const int x0 = tile_x * TILE_W, y0 = tile_y * TILE_H;
     load_ref_tile16(s_ref, tw, th, v, x0, y0, R);
@@ -451,6 +454,74 @@ __global__ void __launch_bounds__(CTA_THREADS, HP_F16_MIN_BLOCKS) propagate16_ke
 }
 
 template <int R, int ST>
+__global__ void __launch_bounds__(CTA_THREADS, HP_F16_MIN_BLOCKS) propagate16_kernel(BatchList bl, SolveConsts sc,
+                                                                                     int iteration, int color) {
+    __shared__ float s_ref[MAX_TW * MAX_TH];
+    __shared__ __half2 s_win[Win<R, ST>::IN_SMEM ? WIN_PAIRS_MAX * CTA_THREADS : 1];
+    __shared__ float s_cost[WARPS][32 * 4];
+    __shared__ unsigned char s_items[WARPS][32 * 4];
+    int tile_x, tile_y;
+    const ViewDesc* v = locate_tile16(bl, blockIdx.x, &tile_x, &tile_y);
+    tile_propagate16<R, ST>(v, tile_x, tile_y, sc, iteration, color, s_ref, s_win, s_cost, s_items);
+}
+
+// Persistent form (see Schedule and the FP32 persistent kernel): the stage
+// bodies are those of the per-stage kernels, so the results are bit-identical.
+template <int R, int ST>
+__global__ void __launch_bounds__(CTA_THREADS, HP_F16_MIN_BLOCKS) persistent16_kernel(Schedule s) {
+    __shared__ float s_ref[MAX_TW * MAX_TH];
+    __shared__ __half2 s_win[Win<R, ST>::IN_SMEM ? WIN_PAIRS_MAX * CTA_THREADS : 1];
+    __shared__ float s_cost[WARPS][32 * 4];
+    __shared__ unsigned char s_items[WARPS][32 * 4];
+    __shared__ int s_ticket;
+    for (;;) {
+        if (threadIdx.x == 0) s_ticket = sched_next(s);
+        __syncthreads();
+        const int ticket = s_ticket;
+        if (ticket < 0) break;
+        const SchedTile t = decode_ticket(s, ticket);
+        const ViewDesc* v = t.v;
+        if (t.stage == 0) {
+            tile_init(v, t.tx, t.ty);
+            __syncthreads();
+            tile_cost16<R, ST>(v, t.tx, t.ty, s.sc, s_ref, s_win);
+        } else if (t.stage <= 2 * v->iterations) {
+            const int k = t.stage - 1;
+            tile_propagate16<R, ST>(v, t.tx, t.ty, s.sc, k >> 1, k & 1, s_ref, s_win, s_cost, s_items);
+        } else {
+            tile_unpack(v, t.tx, t.ty);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) sched_publish(s, t);
+    }
+}
+
+template <int R, int ST>
+cudaError_t persistent_r(const Schedule& s, int grid, cudaStream_t st, int* occ) {
+    if (occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, persistent16_kernel<R, ST>, CTA_THREADS, 0);
+    persistent16_kernel<R, ST><<<grid, CTA_THREADS, 0, st>>>(s);
+    return cudaGetLastError();
+}
+
+cudaError_t persistent_dispatch16(int radius, int stride, const Schedule* s, int grid, cudaStream_t st, int* occ) {
+    if (stride != 1 && stride != 2) return cudaErrorInvalidValue;
+#define HP_CASE(RR)                                                                            \
+    case RR:                                                                                   \
+        return stride == 1 ? persistent_r<RR, 1>(*s, grid, st, occ) : persistent_r<RR, 2>(*s, grid, st, occ);
+    switch (radius) {
+        HP_CASE(1)
+        HP_CASE(2)
+        HP_CASE(3)
+        HP_CASE(4)
+        HP_CASE(5)
+        HP_CASE(6)
+        HP_CASE(7)
+        default: return cudaErrorInvalidValue;
+    }
+#undef HP_CASE
+}
+
+template <int R, int ST>
 cudaError_t launch_r(const BatchList& bl, const SolveConsts& sc, int iteration, int color, bool full, cudaStream_t st) {
     if (full)
         cost16_kernel<R, ST><<<bl.total_tiles, CTA_THREADS, 0, st>>>(bl, sc);
@@ -489,6 +560,16 @@ cudaError_t launch_cost_f16(const BatchList& bl, const SolveConsts& sc, cudaStre
 cudaError_t launch_propagate_f16(const BatchList& bl, const SolveConsts& sc, int iteration, int color,
                                  cudaStream_t st) {
     return dispatch(bl, sc, iteration, color, false, st);
+}
+
+cudaError_t launch_persistent_f16(const Schedule& s, int grid, cudaStream_t st) {
+    if (s.total <= 0 || grid <= 0) return cudaSuccess;
+    return persistent_dispatch16(s.sc.radius, s.sc.stride, &s, grid, st, nullptr);
+}
+
+cudaError_t persistent_occupancy_f16(int radius, int stride, int* blocks_per_sm) {
+    Schedule dummy{};
+    return persistent_dispatch16(radius, stride, &dummy, 0, nullptr, blocks_per_sm);
 }
 
 }  // namespace hp

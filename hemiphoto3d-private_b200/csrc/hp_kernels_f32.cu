@@ -20,6 +20,7 @@
 // intrinsics so the CPU restatement reproduces it bit for bit.
 #include "hp_internal.h"
 #include "hp_rng.cuh"
+#include "hp_tile.cuh"
 
 // Resident CTAs per SM the cost kernels are register-budgeted for.
 #ifndef HP_F32_MIN_BLOCKS
@@ -196,42 +197,17 @@ __device__ __forceinline__ bool same_plane(float4 a, float4 b) {
            __float_as_uint(a.z) == __float_as_uint(b.z) && __float_as_uint(a.w) == __float_as_uint(b.w);
 }
 
-// --------------------------------------------------------------------------
-// Initial hypotheses: depth uniform in [dmin, dmax]; normal from theta in
-// [0, 2pi) and cos(phi) in (0, 1), flipped to face the camera, normalised
-// (init_depth_normal_kernel, patchmatch_mvs.cu:164-216).
-// --------------------------------------------------------------------------
 __global__ void __launch_bounds__(CTA_THREADS) init_kernel(BatchList bl) {
     int tile_x, tile_y;
     const ViewDesc* v = locate_tile(bl, blockIdx.x, &tile_x, &tile_y);
-    const int ly = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int y = tile_y * TILE_H + ly;
-    if (y >= v->H) return;
-    for (int j = 0; j < 2; ++j) {
-        const int x = tile_x * TILE_W + j * 32 + lane;
-        if (x >= v->W) continue;
-        const uint32_t idx = static_cast<uint32_t>(y * v->W + x);
-        const uint4 r = philox4x32_10(make_uint4(idx, v->view_id, 0u, 0u), v->seed_lo, v->seed_hi);
-        const float depth = __fmaf_rn(u01(r.x), __fsub_rn(v->dmax, v->dmin), v->dmin);
-        const float3 ray = view_ray(v->kinv, x, y);
-        float st, ct;
-        sincos_2pi(u01(r.y), &st, &ct);
-        const float cp = u01(r.z);
-        const float sp = __fsqrt_rn(fmaxf(0.0f, __fmaf_rn(-cp, cp, 1.0f)));
-        float3 n = make_float3(__fmul_rn(sp, ct), __fmul_rn(sp, st), cp);
-        if (dot3_rn(n, ray) > 0.0f) n = make_float3(-n.x, -n.y, -n.z);
-        n = normalize3_rn(n.x, n.y, n.z);
-        v->hyp[idx] = make_float4(depth, n.x, n.y, n.z);
-    }
+    tile_init(v, tile_x, tile_y);
 }
 
-// Full-map cost of the current hypotheses (compute_ncc_cost_kernel,
+// Full-map cost of the current hypotheses of one tile (compute_ncc_cost_kernel,
 // patchmatch_mvs.cu:349-513).  Each thread owns a horizontal pixel pair.
 template <int R, int ST>
-__global__ void __launch_bounds__(CTA_THREADS, HP_F32_MIN_BLOCKS) cost_kernel(BatchList bl, SolveConsts sc) {
-    __shared__ float s_ref[MAX_TW * MAX_TH];
-    int tile_x, tile_y;
-    const ViewDesc* v = locate_tile(bl, blockIdx.x, &tile_x, &tile_y);
+__device__ __forceinline__ void tile_cost(const ViewDesc* v, int tile_x, int tile_y, const SolveConsts& sc,
+                                          float* s_ref) {
     constexpr int tw = TILE_W + 2 * R, th = TILE_H + 2 * R;
     const int x0 = tile_x * TILE_W, y0 = tile_y * TILE_H;
     load_ref_tile(s_ref, tw, th, v, x0, y0, R);
@@ -246,6 +222,14 @@ __global__ void __launch_bounds__(CTA_THREADS, HP_F32_MIN_BLOCKS) cost_kernel(Ba
         const float4 h = v->hyp[idx];
         v->cost[idx] = cost_f32<R, ST>(s_ref, tw, lx, ly, x, y, h.x, h.y, h.z, h.w, v, sc.top_k);
     }
+}
+
+template <int R, int ST>
+__global__ void __launch_bounds__(CTA_THREADS, HP_F32_MIN_BLOCKS) cost_kernel(BatchList bl, SolveConsts sc) {
+    __shared__ float s_ref[MAX_TW * MAX_TH];
+    int tile_x, tile_y;
+    const ViewDesc* v = locate_tile(bl, blockIdx.x, &tile_x, &tile_y);
+    tile_cost<R, ST>(v, tile_x, tile_y, sc, s_ref);
 }
 
 // One red-black half-pass (propagate_and_refine_kernel, patchmatch_mvs.cu:519-655).
@@ -263,15 +247,12 @@ __global__ void __launch_bounds__(CTA_THREADS, HP_F32_MIN_BLOCKS) cost_kernel(Ba
 // folds its costs in L, R, U, D order with the same strict-less rule - the
 // result is that of the sequential loop.  The refinement perturbations
 // (:583-648) follow per lane: every lane has exactly refine_steps of them.
+constexpr int WARPS = CTA_THREADS / 32;
+
 template <int R, int ST>
-__global__ void __launch_bounds__(CTA_THREADS, HP_F32_MIN_BLOCKS) propagate_kernel(BatchList bl, SolveConsts sc,
-                                                                                   int iteration, int color) {
-    constexpr int WARPS = CTA_THREADS / 32;
-    __shared__ float s_ref[MAX_TW * MAX_TH];
-    __shared__ float s_cost[WARPS][32 * 4];
-    __shared__ unsigned char s_items[WARPS][32 * 4];
-    int tile_x, tile_y;
-    const ViewDesc* v = locate_tile(bl, blockIdx.x, &tile_x, &tile_y);
+__device__ __forceinline__ void tile_propagate(const ViewDesc* v, int tile_x, int tile_y, const SolveConsts& sc,
+                                               int iteration, int color, float* s_ref, float (*s_cost)[32 * 4],
+                                               unsigned char (*s_items)[32 * 4]) {
     constexpr int tw = TILE_W + 2 * R, th = TILE_H + 2 * R;
     const int x0 = tile_x * TILE_W, y0 = tile_y * TILE_H;
     load_ref_tile(s_ref, tw, th, v, x0, y0, R);
@@ -385,6 +366,49 @@ __global__ void __launch_bounds__(CTA_THREADS, HP_F32_MIN_BLOCKS) propagate_kern
 }
 
 template <int R, int ST>
+__global__ void __launch_bounds__(CTA_THREADS, HP_F32_MIN_BLOCKS) propagate_kernel(BatchList bl, SolveConsts sc,
+                                                                                   int iteration, int color) {
+    __shared__ float s_ref[MAX_TW * MAX_TH];
+    __shared__ float s_cost[WARPS][32 * 4];
+    __shared__ unsigned char s_items[WARPS][32 * 4];
+    int tile_x, tile_y;
+    const ViewDesc* v = locate_tile(bl, blockIdx.x, &tile_x, &tile_y);
+    tile_propagate<R, ST>(v, tile_x, tile_y, sc, iteration, color, s_ref, s_cost, s_items);
+}
+
+// Persistent form: one launch runs every stage of every view of a solve
+// (see Schedule), each CTA taking tiles until the tickets run out.  The stage
+// bodies are the functions the per-stage kernels above run, so the results
+// are bit-identical to the per-stage launch sequence.
+template <int R, int ST>
+__global__ void __launch_bounds__(CTA_THREADS, HP_F32_MIN_BLOCKS) persistent_kernel(Schedule s) {
+    __shared__ float s_ref[MAX_TW * MAX_TH];
+    __shared__ float s_cost[WARPS][32 * 4];
+    __shared__ unsigned char s_items[WARPS][32 * 4];
+    __shared__ int s_ticket;
+    for (;;) {
+        if (threadIdx.x == 0) s_ticket = sched_next(s);
+        __syncthreads();
+        const int ticket = s_ticket;
+        if (ticket < 0) break;
+        const SchedTile t = decode_ticket(s, ticket);
+        const ViewDesc* v = t.v;
+        if (t.stage == 0) {
+            tile_init(v, t.tx, t.ty);
+            __syncthreads();
+            tile_cost<R, ST>(v, t.tx, t.ty, s.sc, s_ref);
+        } else if (t.stage <= 2 * v->iterations) {
+            const int k = t.stage - 1;
+            tile_propagate<R, ST>(v, t.tx, t.ty, s.sc, k >> 1, k & 1, s_ref, s_cost, s_items);
+        } else {
+            tile_unpack(v, t.tx, t.ty);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) sched_publish(s, t);
+    }
+}
+
+template <int R, int ST>
 cudaError_t launch_rs(const BatchList& bl, const SolveConsts& sc, int iteration, int color, bool full,
                       cudaStream_t st) {
     if (full)
@@ -415,7 +439,42 @@ cudaError_t dispatch_f32(const BatchList& bl, const SolveConsts& sc, int iterati
 #undef HP_CASE
 }
 
+template <int R, int ST>
+cudaError_t persistent_rs(const Schedule& s, int grid, cudaStream_t st, int* occ) {
+    if (occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, persistent_kernel<R, ST>, CTA_THREADS, 0);
+    persistent_kernel<R, ST><<<grid, CTA_THREADS, 0, st>>>(s);
+    return cudaGetLastError();
+}
+
+cudaError_t persistent_dispatch(int radius, int stride, const Schedule* s, int grid, cudaStream_t st, int* occ) {
+    if (stride != 1 && stride != 2) return cudaErrorInvalidValue;
+#define HP_CASE(RR)                                                                              \
+    case RR:                                                                                     \
+        return stride == 1 ? persistent_rs<RR, 1>(*s, grid, st, occ) : persistent_rs<RR, 2>(*s, grid, st, occ);
+    switch (radius) {
+        HP_CASE(1)
+        HP_CASE(2)
+        HP_CASE(3)
+        HP_CASE(4)
+        HP_CASE(5)
+        HP_CASE(6)
+        HP_CASE(7)
+        default: return cudaErrorInvalidValue;
+    }
+#undef HP_CASE
+}
+
 }  // namespace
+
+cudaError_t launch_persistent_f32(const Schedule& s, int grid, cudaStream_t st) {
+    if (s.total <= 0 || grid <= 0) return cudaSuccess;
+    return persistent_dispatch(s.sc.radius, s.sc.stride, &s, grid, st, nullptr);
+}
+
+cudaError_t persistent_occupancy_f32(int radius, int stride, int* blocks_per_sm) {
+    Schedule dummy{};
+    return persistent_dispatch(radius, stride, &dummy, 0, nullptr, blocks_per_sm);
+}
 
 cudaError_t launch_init(const BatchList& bl, cudaStream_t st) {
     if (bl.total_tiles <= 0) return cudaSuccess;

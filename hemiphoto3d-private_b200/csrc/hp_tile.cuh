@@ -1,0 +1,161 @@
+// Tile-level stages shared by the FP32 and FP16 kernels (hypothesis
+// initialisation, output unpacking) and the device side of the persistent
+// schedule (ticket decoding, bounded dependency waits, completion flags).
+#pragma once
+
+#include "hp_internal.h"
+#include "hp_rng.cuh"
+
+namespace hp {
+
+// Initial hypotheses of one tile: depth uniform in [dmin, dmax]; normal from
+// theta in [0, 2pi) and cos(phi) in (0, 1), flipped to face the camera,
+// normalised (init_depth_normal_kernel, src/dense_recon/patchmatch_mvs.cu:164-216).
+// Every operation is explicitly rounded, so the result does not depend on the
+// including translation unit's flags (no intermediate is ever subnormal:
+// depths lie in [dmin, dmax] and normal components are at least ~1e-10).
+__device__ __forceinline__ void tile_init(const ViewDesc* v, int tile_x, int tile_y) {
+    const int ly = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int y = tile_y * TILE_H + ly;
+    if (y >= v->H) return;
+    for (int j = 0; j < 2; ++j) {
+        const int x = tile_x * TILE_W + j * 32 + lane;
+        if (x >= v->W) continue;
+        const uint32_t idx = static_cast<uint32_t>(y * v->W + x);
+        const uint4 r = philox4x32_10(make_uint4(idx, v->view_id, 0u, 0u), v->seed_lo, v->seed_hi);
+        const float depth = __fmaf_rn(u01(r.x), __fsub_rn(v->dmax, v->dmin), v->dmin);
+        const float3 ray = view_ray(v->kinv, x, y);
+        float st, ct;
+        sincos_2pi(u01(r.y), &st, &ct);
+        const float cp = u01(r.z);
+        const float sp = __fsqrt_rn(fmaxf(0.0f, __fmaf_rn(-cp, cp, 1.0f)));
+        float3 n = make_float3(__fmul_rn(sp, ct), __fmul_rn(sp, st), cp);
+        if (dot3_rn(n, ray) > 0.0f) n = make_float3(-n.x, -n.y, -n.z);
+        n = normalize3_rn(n.x, n.y, n.z);
+        v->hyp[idx] = make_float4(depth, n.x, n.y, n.z);
+    }
+}
+
+// Final stage of a view in a persistent launch: its tile's packed state into
+// the output maps (depth, camera-frame AoS normal, cost).
+__device__ __forceinline__ void tile_unpack(const ViewDesc* v, int tile_x, int tile_y) {
+    const int ly = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int y = tile_y * TILE_H + ly;
+    if (y >= v->H) return;
+    for (int j = 0; j < 2; ++j) {
+        const int x = tile_x * TILE_W + j * 32 + lane;
+        if (x >= v->W) continue;
+        const size_t i = static_cast<size_t>(y) * v->W + x;
+        const float4 h = __ldcg(v->hyp + i);
+        v->out_depth[i] = h.x;
+        v->out_normal[3 * i] = h.y;
+        v->out_normal[3 * i + 1] = h.z;
+        v->out_normal[3 * i + 2] = h.w;
+        v->out_cost[i] = __ldcg(v->cost + i);
+    }
+}
+
+__device__ __forceinline__ int ld_acquire_gpu(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release_gpu(int* p, int v) {
+    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ int ld_relaxed_gpu(const int* p) {
+    int v;
+    asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+struct SchedTile {
+    const ViewDesc* v;
+    int view, stage;
+    int tile, tx, ty;
+};
+
+__device__ __forceinline__ SchedTile decode_ticket(const Schedule& s, int t) {
+    int lo = 0, hi = s.n_entries - 1;
+    while (lo < hi) {  // last entry starting at or before t
+        const int mid = (lo + hi + 1) >> 1;
+        if (s.entry_ticket[mid] <= t) lo = mid; else hi = mid - 1;
+    }
+    const int2 info = s.entry_info[lo];
+    SchedTile r;
+    r.v = &s.views[info.x];
+    r.view = info.x;
+    r.stage = info.y;
+    r.tile = t - s.entry_ticket[lo];
+    r.tx = r.tile % r.v->tiles_x;
+    r.ty = r.tile / r.v->tiles_x;
+    return r;
+}
+
+// Raise the abort flag with `code` (the first code recorded wins).
+__device__ __forceinline__ void sched_abort(const Schedule& s, int code) {
+    atomicCAS(s.status, SCHED_OK, code);
+    atomicExch(s.status + 1, 1);
+}
+
+// Thread 0 of a CTA: wait until the tile and its 4-neighbour tiles have
+// finished stage - 1.  Bounded by the schedule's time limit and by a poll
+// count (in case the global timer stands still); false when this or another
+// CTA gave up.
+__device__ __forceinline__ bool sched_wait(const Schedule& s, const SchedTile& t) {
+    if (t.stage == 0) return true;
+    const int need = t.stage - 1;
+    const int* done = t.v->done;
+    const int tx = t.v->tiles_x;
+    int deps[5];
+    int n = 0;
+    deps[n++] = t.tile;
+    if (t.tx > 0) deps[n++] = t.tile - 1;
+    if (t.tx + 1 < tx) deps[n++] = t.tile + 1;
+    if (t.ty > 0) deps[n++] = t.tile - tx;
+    if (t.ty + 1 < t.v->tiles_y) deps[n++] = t.tile + tx;
+    unsigned long long start = 0;
+    unsigned polls = 0;
+    constexpr unsigned kMaxPolls = 1u << 26;
+    for (int i = 0; i < n; ++i) {
+        while (ld_acquire_gpu(done + deps[i]) < need) {
+            if (ld_relaxed_gpu(s.status + 1)) return false;
+            if (++polls > 16) {
+                const unsigned long long now = global_ns();
+                if (start == 0) start = now;
+                if (now - start > s.wait_limit_ns || polls > kMaxPolls) {
+                    sched_abort(s, SCHED_TIMEOUT);
+                    return false;
+                }
+                __nanosleep(256);
+            }
+        }
+    }
+    return true;
+}
+
+// Thread 0, after the CTA's barrier at the end of a stage: publish it.
+__device__ __forceinline__ void sched_publish(const Schedule& s, const SchedTile& t) {
+    if (t.view == s.stall_view && t.tile == s.stall_tile) return;
+    __threadfence();
+    st_release_gpu(t.v->done + t.tile, t.stage);
+}
+
+// Thread 0: the CTA's next ticket, or -1 when the schedule is exhausted or
+// aborted (including a dependency wait of this ticket that ran out).
+__device__ __forceinline__ int sched_next(const Schedule& s) {
+    if (ld_relaxed_gpu(s.status + 1)) return -1;
+    const int t = static_cast<int>(atomicAdd(s.counter, 1u));
+    if (t >= s.total) return -1;
+    return sched_wait(s, decode_ticket(s, t)) ? t : -1;
+}
+
+}  // namespace hp

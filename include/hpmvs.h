@@ -143,7 +143,8 @@ typedef enum hp_kernel_kind {
     HP_KERNEL_COST = 1,      /* full-map cost */
     HP_KERNEL_PROPAGATE = 2, /* red-black propagate + refine half-pass */
     HP_KERNEL_OTHER = 3,     /* layout, conversion and filter kernels */
-    HP_KERNEL_KINDS = 4
+    HP_KERNEL_PERSISTENT = 4, /* whole-solve persistent launches (plans, server) */
+    HP_KERNEL_KINDS = 5
 } hp_kernel_kind;
 
 typedef struct hp_profile {
@@ -238,6 +239,78 @@ hp_status hp_geometric_filter(hp_ctx* ctx, const hp_camera* ref_cam, int width, 
 hp_status hp_solve_static(int device, void* stream, const hp_job* job, const float* ref_image, int ref_pitch,
                           int width, int height, const unsigned long long* src_textures, const hp_params* params,
                           hp_maps* out);
+
+/* ---------------------------------------------------------------------------
+ * Plans: a batched solve prepared once and run many times.  No counterpart in
+ * the reference, which solves one view at a time with a device
+ * synchronisation after every launch (runPatchMatchMVS,
+ * patchmatch_mvs.cu:1199-1232).  A plan owns the device state of its jobs
+ * (views of any size and source count, each with its own iteration count) and
+ * the output binding, and replays its launch sequence as one CUDA graph.
+ * Every schedule gives bit-identical results (the per-pixel arithmetic does
+ * not depend on how tiles are scheduled); they differ only in speed.
+ * ------------------------------------------------------------------------- */
+typedef enum hp_schedule_kind {
+    HP_SCHEDULE_AUTO = 0,       /* persistent until hp_plan_tune has chosen */
+    HP_SCHEDULE_PER_PASS = 1,   /* init, cost, one launch per red-black half-pass over all views, unpack */
+    HP_SCHEDULE_PERSISTENT = 2  /* one launch for the whole solve: CTAs take (view, stage, tile) tickets */
+} hp_schedule_kind;
+
+typedef struct hp_plan_options {
+    int schedule;         /* hp_schedule_kind */
+    int ctas_per_sm;      /* persistent: resident CTAs per SM, 0 = the occupancy maximum */
+    int use_graph;        /* 1: capture the launch sequence once and replay it as a CUDA graph */
+    int wait_limit_ms;    /* persistent: bound on one inter-tile dependency wait (0 = 2000 ms) */
+    int debug_stall_view; /* tests only: tile (view, tile) never reports completion, so its */
+    int debug_stall_tile; /*   dependants' bounded waits run out (-1 = off) */
+} hp_plan_options;
+
+typedef struct hp_plan_info {
+    int schedule;            /* the schedule a run uses (never AUTO) */
+    int ctas_per_sm;         /* persistent: resident CTAs per SM in use */
+    int grid;                /* persistent: CTAs launched */
+    int max_ctas_per_sm;     /* persistent: occupancy maximum of the kernel */
+    int tickets;             /* persistent: (view, stage, tile) work items */
+    int launches_per_run;    /* kernel launches one run issues */
+    int views;
+    int use_graph;
+    uint64_t state_bytes;    /* device memory the plan holds */
+    double pixel_iterations; /* sum over views of W * H * iterations */
+    float tuned_ms;          /* hp_plan_tune: the chosen candidate's median solve time (0 before) */
+} hp_plan_info;
+
+typedef struct hp_plan hp_plan;
+
+void hp_plan_options_default(hp_plan_options* o);
+/* Validates the jobs, allocates their state and binds `out` (one hp_maps per
+ * job, host or device memory; host maps are filled when a run finishes). */
+hp_status hp_plan_create(hp_ctx* ctx, const hp_job* jobs, int num_jobs, const hp_params* params,
+                         const hp_plan_options* options, const hp_maps* out, hp_plan** plan);
+/* One full solve into the bound maps; returns when they are written.
+ * HP_ERR_TIMEOUT when a persistent dependency wait ran out (the kernel then
+ * stops taking work and the context stays usable). */
+hp_status hp_plan_run(hp_plan* plan);
+/* Enqueue one solve on the context stream without waiting (device maps
+ * only); hp_plan_wait completes it and reports its status. */
+hp_status hp_plan_launch(hp_plan* plan);
+hp_status hp_plan_wait(hp_plan* plan);
+/* Autotuner: times every schedule candidate (per-pass graph; persistent at
+ * each resident-CTA count up to the occupancy maximum) `repeats` times on the
+ * plan's own jobs, keeps the fastest by median, and reports it in `best`.
+ * The bound maps hold a valid solve afterwards. */
+hp_status hp_plan_tune(hp_plan* plan, int repeats, hp_plan_info* best);
+hp_status hp_plan_get_info(const hp_plan* plan, hp_plan_info* info);
+hp_status hp_plan_destroy(hp_plan* plan);
+
+/* The persistent ticket order, computed on the host (no device needed): view
+ * v runs stages [stage_begin[v], stage_end[v]) of its stage sequence (0 init +
+ * cost, 1 + 2*it + color the half-passes, 2*iterations + 1 the unpack) and
+ * entry e covers tickets [entry_ticket[e], entry_ticket[e + 1]) of view
+ * entry_view[e] at stage entry_stage[e].  Entries are ordered by the stage's
+ * offset from its view's stage_begin, then by view.  `capacity` bounds the
+ * entries; entry_ticket needs capacity + 1 slots. */
+hp_status hp_schedule_build(int num_views, const int* tiles, const int* stage_begin, const int* stage_end,
+                            int capacity, int* entry_ticket, int* entry_view, int* entry_stage, int* num_entries);
 
 /* Replaces saveDepthMapPFM / loadDepthMapPFM (patchmatch_mvs.cu:990-1022):
  * 'Pf' (channels 1) or 'PF' (channels 3) little-endian PFM, rows bottom-up. */
