@@ -48,7 +48,7 @@ class Params(C.Structure):
     _fields_ = [
         ("radius", C.c_int), ("stride", C.c_int), ("top_k", C.c_int), ("precision", C.c_int),
         ("refine_steps", C.c_int), ("iter_decay", C.c_float), ("step_decay", C.c_float),
-        ("tile_w", C.c_int), ("tile_h", C.c_int),
+        ("tile_w", C.c_int), ("tile_h", C.c_int), ("soft_sources", C.c_int),
     ]
 
 

@@ -77,6 +77,10 @@ hp::SolveConsts consts_of(const hp_params* p) {
     sc.refine_steps = p->refine_steps;
     sc.iter_decay = p->iter_decay;
     sc.step_decay = p->step_decay;
+    // Default: every source through the software sampler (measured fastest).
+    sc.soft_mask = p->precision == HP_PRECISION_F16ACC
+                       ? (p->soft_sources < 0 ? 0xFFu : static_cast<unsigned>(p->soft_sources) & 0xFFu)
+                       : 0u;
     return sc;
 }
 
@@ -110,7 +114,9 @@ hp_status fill_desc(hp_ctx* ctx, const hp_job* j, int jobno, hp::ViewDesc* d) {
                         si->second.W, si->second.H, ref.W, ref.H);
         d->src_tex[s] = si->second.tex32;
         d->src_tex16[s] = si->second.tex16;
+        d->src_quad[s] = si->second.quad16;
     }
+    d->quad_pitch = static_cast<int>(ref.quad_pitch / sizeof(uint2));
     if (j->use_coeffs) {
         std::memcpy(d->kinv, j->kinv, sizeof d->kinv);
         for (int s = 0; s < j->num_sources; ++s) std::memcpy(d->ab[s], j->ab[s], sizeof d->ab[s]);
@@ -294,6 +300,7 @@ void free_image(Image& im) {
     if (im.arr16) cudaFreeArray(im.arr16);
     if (im.f32) cudaFree(im.f32);
     if (im.f16) cudaFree(im.f16);
+    if (im.quad16) cudaFree(im.quad16);
     im = Image();
 }
 
@@ -345,6 +352,7 @@ void hp_params_default(hp_params* p) {
     p->step_decay = 0.5f;
     p->tile_w = 0;
     p->tile_h = 0;
+    p->soft_sources = -1;
 }
 
 hp_status hp_ctx_create(int device, hp_ctx** out) {
@@ -435,8 +443,9 @@ hp_status hp_image_upload(hp_ctx* ctx, const void* data, int memory, int width, 
                           int* image_id) {
     if (!ctx) return HP_ERR_INVALID_ARG;
     if (!data || !image_id) return fail(ctx, HP_ERR_INVALID_ARG, "image_upload: null pointer");
-    if (width < 2 || height < 2 || width > 32768 || height > 32768)
-        return fail(ctx, HP_ERR_INVALID_ARG, "image_upload: size %dx%d outside 2..32768", width, height);
+    // 16384: the software sampler's fixed-point coordinate range (hp_kernels_f16.cu, SOFT_MAGIC).
+    if (width < 2 || height < 2 || width > 16384 || height > 16384)
+        return fail(ctx, HP_ERR_INVALID_ARG, "image_upload: size %dx%d outside 2..16384", width, height);
     if (dtype != HP_DTYPE_U8 && dtype != HP_DTYPE_F16 && dtype != HP_DTYPE_F32)
         return fail(ctx, HP_ERR_INVALID_ARG, "image_upload: unknown dtype %d", dtype);
     if (memory != HP_MEMORY_HOST && memory != HP_MEMORY_DEVICE)
@@ -482,6 +491,11 @@ hp_status hp_image_upload(hp_ctx* ctx, const void* data, int memory, int width, 
                                    cudaMemcpyDeviceToDevice, ctx->stream));
     HP_UP(cudaMemcpy2DToArrayAsync(im.arr16, 0, 0, im.f16, im.pitch16, width * sizeof(__half), height,
                                    cudaMemcpyDeviceToDevice, ctx->stream));
+    HP_UP(cudaMallocPitch(reinterpret_cast<void**>(&im.quad16), &im.quad_pitch, width * sizeof(uint2), height));
+    HP_UP(counted(ctx, HP_KERNEL_OTHER, [&] {
+        return hp::launch_quads(im.f16, static_cast<int>(im.pitch16 / sizeof(__half)), width, height, im.quad16,
+                                static_cast<int>(im.quad_pitch / sizeof(uint2)), ctx->stream);
+    }));
     HP_UP(make_linear_texture(im.arr32, &im.tex32));
     HP_UP(make_linear_texture(im.arr16, &im.tex16));
     HP_UP(cudaStreamSynchronize(ctx->stream));

@@ -25,6 +25,10 @@ struct Image {
     size_t pitch16 = 0;  // bytes
     cudaArray_t arr32 = nullptr, arr16 = nullptr;
     cudaTextureObject_t tex32 = 0, tex16 = 0;
+    // Software-sampler plane: texel (x, y) holds the 2x2 FP16 block
+    // {t(x,y), t(x+1,y)}, {t(x,y+1), t(x+1,y+1)} shifted by -0.5 (edges clamped).
+    uint2* quad16 = nullptr;
+    size_t quad_pitch = 0;  // bytes
 };
 
 // Grow-only device buffer.

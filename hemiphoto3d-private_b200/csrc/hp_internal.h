@@ -25,6 +25,8 @@ struct ViewDesc {
     const __half* ref16;              // FP16 reference image, row pitch ref16_pitch halves
     cudaTextureObject_t src_tex[HP_MAX_SOURCES];    // FP32 sources, linear filter
     cudaTextureObject_t src_tex16[HP_MAX_SOURCES];  // FP16 sources, linear filter
+    const uint2* src_quad[HP_MAX_SOURCES];          // FP16 sources, software-sampler quads
+    int quad_pitch;                                 // uint2 per quad row
     float kinv[9];
     float ab[HP_MAX_SOURCES][12];     // A (9), b (3) per source
     float4* hyp;                      // H*W
@@ -48,6 +50,7 @@ struct ViewDesc {
 struct SolveConsts {
     int radius, stride, top_k, refine_steps;
     float iter_decay, step_decay;
+    unsigned soft_mask;  // FP16 path: sources sampled in software (bit per source)
 };
 
 // A batch launch covers the tiles of several views: view k owns flattened
@@ -125,6 +128,9 @@ cudaError_t persistent_occupancy_f32(int radius, int stride, int* blocks_per_sm)
 cudaError_t persistent_occupancy_f16(int radius, int stride, int* blocks_per_sm);
 cudaError_t launch_propagate_f16(const BatchList& bl, const SolveConsts& sc, int iteration, int color,
                                  cudaStream_t st);
+// FP16 plane -> software-sampler quad plane (see hpx::Image::quad16).
+cudaError_t launch_quads(const __half* src16, int pitch16, int W, int H, uint2* quads, int quad_pitch,
+                         cudaStream_t st);
 cudaError_t launch_unpack(const ViewDesc* views_host_copy, int view, float* depth, float* normal, float* cost,
                           cudaStream_t st);
 cudaError_t launch_pack(const ViewDesc* views_host_copy, int view, const float* depth, const float* normal,

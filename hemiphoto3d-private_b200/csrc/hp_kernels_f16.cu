@@ -121,55 +121,85 @@ struct Plane {
     float h[9];  // homography with the +0.5 texel offset folded into rows 0, 1
 };
 
+// Software bilinear sampler (sources whose bit is set in soft_mask).  The
+// texture unit filters about four taps per SM clock; these taps go through the
+// load/store pipe and the FP16 units instead, which run alongside it.
+//
+// A warped coordinate c (texel centres at integers) becomes fixed point with
+// 8 fractional bits by one FMA: the bits of RN(c + 49152) are
+// 0x47400000 + RN(256 c) for 0 <= c < 16384.  Two byte permutes then give
+//  - the quad index: bits 8..23 are 0x4000 + floor(c), folded into the base
+//    pointer of the quad plane, and
+//  - the weight as an FP16 number: 0x47 above the fraction byte is the FP16
+//    encoding of 7 + frac/256, exact, so one FP16 subtraction of 7 leaves the
+//    8-bit fraction (the texture unit's weight resolution).
+// The quad plane stores each 2x2 texel block in difference form, shifted by
+// -0.5 (see quads_kernel), so a sample is two FP16 FMAs on values of
+// magnitude <= 0.5 (half-ulp <= 2^-13).
+constexpr float SOFT_MAGIC = 49152.0f;
+constexpr unsigned SOFT_ORIGIN = 0x47400000u;  // bits of SOFT_MAGIC: coordinate 0
+
+__device__ __forceinline__ const uint2* soft_base(const uint2* quad, int pitch) {
+    // quad - (0x4000 * pitch + 0x4000), formed on the integer address.
+    return reinterpret_cast<const uint2*>(reinterpret_cast<uintptr_t>(quad) -
+                                          static_cast<uintptr_t>(0x4000u) * (static_cast<uintptr_t>(pitch) + 1u) *
+                                              sizeof(uint2));
+}
+
+__device__ __forceinline__ unsigned soft_offset(unsigned bu, unsigned bv, int pitch) {
+    return __byte_perm(bv, 0u, 0x4421) * static_cast<unsigned>(pitch) + __byte_perm(bu, 0u, 0x4421);
+}
+
+__device__ __forceinline__ __half soft_lerp(uint2 q, unsigned wbits) {
+    __half2 w;
+    memcpy(&w, &wbits, sizeof w);
+    w = __hsub2(w, __float2half2_rn(7.0f));  // (fx, fy), exact
+    __half2 a, b;
+    memcpy(&a, &q.x, sizeof a);  // (t00 - 0.5, t01 - t00)
+    memcpy(&b, &q.y, sizeof b);  // (t10 - t00, dxy)
+    const __half2 c = __hfma2(__low2half2(w), b, a);  // (row y0 at fx, column difference at fx)
+    return __hfma(__high2half(w), __high2half(c), __low2half(c));
+}
+
 // Cost (1 - NCC, or 2 when invalid) of one source.  Sums of e = s - mean and
 // products (r - mean) e are formed in FP16 per window row and flushed to FP32.
 // CHECK = false assumes every tap is valid (the caller's corner test proved
 // it); CHECK = true applies the reference's validity rules per tap
 // (|w_z| >= 1e-8, u in [0, W-1), v in [0, H-1), count >= taps/2) by masking
-// the tap's terms.  Each lane picks its form from its own corner test, so a
-// pixel's cost never depends on which other pixels share its warp.
-template <int R, int ST, bool CHECK>
-__device__ __forceinline__ float source_cost(const Plane& P, cudaTextureObject_t tex, RefStats st,
-                                             const __half2* s_win, const float* s_ref, int tw, int lx, int ly, int x,
-                                             int y, float fW, float fH) {
+// the tap's terms.  With every tap valid both forms execute the same
+// arithmetic on the same values, so the choice (made per warp) never changes
+// a result.  SOFT selects the software sampler; P then holds the homography
+// without the texture's +0.5 texel-centre offset.
+template <int R, int ST, bool CHECK, bool SOFT>
+__device__ __forceinline__ float source_cost(const Plane& P, cudaTextureObject_t tex, const uint2* qbase, int qpitch,
+                                             RefStats st, const __half2* s_win, const float* s_ref, int tw, int lx,
+                                             int ly, int x, int y, float fW, float fH) {
     constexpr int SIDE = Win<R, ST>::SIDE;
     constexpr int PAIRS = Win<R, ST>::PAIRS;
     constexpr int N = Win<R, ST>::N;
     const float c0 = st.mean;
+    // Software taps are interpolated on texels shifted by -0.5, so their
+    // residual is s' - (mean - 0.5).  The FP16 rounding of that shift is a
+    // constant offset over the window, which the compensated sums cancel.
+    const __half2 c0s = __float2half2_rn(__fsub_rn(c0, 0.5f));
     float s1 = 0.f, s2 = 0.f, s3 = 0.f, r1 = 0.f, r2 = 0.f;
     int count = 0;
     const float sx0 = static_cast<float>(x - R), sy0 = static_cast<float>(y - R);
     const float hx0 = __fmul_rn(P.h[0], ST), hx1 = __fmul_rn(P.h[3], ST), hx2 = __fmul_rn(P.h[6], ST);
     const float rx0 = __fmaf_rn(P.h[0], sx0, P.h[2]), rx1 = __fmaf_rn(P.h[3], sx0, P.h[5]);
     const float rx2 = __fmaf_rn(P.h[6], sx0, P.h[8]);
+    // Validity bounds of the (offset) coordinate: [lo, W - 1 + lo) with lo = 0.5 for texture taps.
+    constexpr float LO = SOFT ? 0.0f : 0.5f;
 #pragma unroll 1
     for (int i = 0; i < SIDE; ++i) {
         const float py = __fadd_rn(sy0, static_cast<float>(i * ST));
         float wx = __fmaf_rn(P.h[1], py, rx0);
         float wy = __fmaf_rn(P.h[4], py, rx1);
         float wz = __fmaf_rn(P.h[7], py, rx2);
-        float smp[2 * PAIRS];
         unsigned ok = (1u << SIDE) - 1u;
-#pragma unroll
-        for (int j = 0; j < SIDE; ++j) {
-            const float iz = rcp_approx(wz);
-            const float u = __fmul_rn(wx, iz), v = __fmul_rn(wy, iz);  // texel-centre offset already folded in
-            if constexpr (CHECK) {
-                const bool skip = fabsf(wz) < 1e-8f || u < 0.5f || u >= fW - 0.5f || v < 0.5f || v >= fH - 0.5f;
-                ok &= ~(static_cast<unsigned>(skip) << j);
-            }
-            smp[j] = tex2D<float>(tex, u, v);
-            wx = __fadd_rn(wx, hx0);
-            wy = __fadd_rn(wy, hx1);
-            wz = __fadd_rn(wz, hx2);
-        }
-        if constexpr (SIDE & 1) smp[SIDE] = c0;  // pads the last pair: e = 0
         __half2 a1 = __float2half2_rn(0.f), a2 = a1, a3 = a1, a4 = a1, a5 = a1;
-#pragma unroll
-        for (int p = 0; p < PAIRS; ++p) {
-            // The shift is subtracted in FP32 and only the small residual is
-            // rounded to FP16 (rounding the sample first would cost ~2.4e-4).
-            float ea = __fsub_rn(smp[2 * p], c0), eb = __fsub_rn(smp[2 * p + 1], c0);
+        // Folds the residual pair of taps (2p, 2p + 1) into the row sums.
+        auto accumulate = [&](int p, __half2 e) {
             __half2 rq;
             if constexpr (Win<R, ST>::IN_SMEM) {
                 rq = s_win[(i * PAIRS + p) * CTA_THREADS];  // s_win points at the pixel's column
@@ -182,21 +212,83 @@ __device__ __forceinline__ float source_cost(const Plane& P, cudaTextureObject_t
             if constexpr (CHECK) {
                 const bool va = (ok >> (2 * p)) & 1u;
                 const bool vb = (2 * p + 1 < SIDE) && ((ok >> (2 * p + 1)) & 1u);
-                ea = va ? ea : 0.f;
-                eb = vb ? eb : 0.f;
-                // Bitwise mask (exact; a multiply by 1 would not preserve FP16 subnormals).
+                // Bitwise masks (exact; a multiply by 1 would not preserve FP16 subnormals).
+                const unsigned m = (va ? 0x0000ffffu : 0u) | (vb ? 0xffff0000u : 0u);
                 unsigned bits;
                 memcpy(&bits, &rq, sizeof bits);
-                bits &= (va ? 0x0000ffffu : 0u) | (vb ? 0xffff0000u : 0u);
+                bits &= m;
                 memcpy(&rq, &bits, sizeof bits);
+                memcpy(&bits, &e, sizeof bits);
+                bits &= m;
+                memcpy(&e, &bits, sizeof bits);
             }
-            const __half2 e = __floats2half2_rn(ea, eb);
             a1 = __hadd2(a1, e);
             a2 = __hfma2(e, e, a2);
             a3 = __hfma2(rq, e, a3);
             if constexpr (CHECK) {
                 a4 = __hadd2(a4, rq);
                 a5 = __hfma2(rq, rq, a5);
+            }
+        };
+        if constexpr (SOFT) {
+            // Chunks of four taps: four quad loads in flight, then two pairs folded.
+            constexpr int CHUNKS = (SIDE + 3) / 4;
+#pragma unroll
+            for (int ch = 0; ch < CHUNKS; ++ch) {
+                uint2 q[4];
+                unsigned wb[4];
+#pragma unroll
+                for (int jj = 0; jj < 4; ++jj) {
+                    const int j = 4 * ch + jj;
+                    if (j >= SIDE) break;
+                    const float iz = rcp_approx(wz);
+                    unsigned bu = __float_as_uint(__fmaf_rn(wx, iz, SOFT_MAGIC));
+                    unsigned bv = __float_as_uint(__fmaf_rn(wy, iz, SOFT_MAGIC));
+                    if constexpr (CHECK) {
+                        const float u = __fmul_rn(wx, iz), v = __fmul_rn(wy, iz);
+                        const bool skip = fabsf(wz) < 1e-8f || !(u >= LO) || !(u < fW - 1.0f + LO) || !(v >= LO) ||
+                                          !(v < fH - 1.0f + LO);
+                        ok &= ~(static_cast<unsigned>(skip) << j);
+                        bu = skip ? SOFT_ORIGIN : bu;  // an in-bounds quad; the tap is masked
+                        bv = skip ? SOFT_ORIGIN : bv;
+                    }
+                    wb[jj] = __byte_perm(bu, bv, 0x7430);
+                    q[jj] = __ldg(qbase + soft_offset(bu, bv, qpitch));
+                    wx = __fadd_rn(wx, hx0);
+                    wy = __fadd_rn(wy, hx1);
+                    wz = __fadd_rn(wz, hx2);
+                }
+#pragma unroll
+                for (int pp = 0; pp < 2; ++pp) {
+                    const int p = 2 * ch + pp;
+                    if (p >= PAIRS) break;
+                    const __half sa = soft_lerp(q[2 * pp], wb[2 * pp]);
+                    const __half sb = (2 * p + 1 < SIDE) ? soft_lerp(q[2 * pp + 1], wb[2 * pp + 1]) : __low2half(c0s);
+                    accumulate(p, __hsub2(__halves2half2(sa, sb), c0s));
+                }
+            }
+        } else {
+            float smp[2 * PAIRS];
+#pragma unroll
+            for (int j = 0; j < SIDE; ++j) {
+                const float iz = rcp_approx(wz);
+                const float u = __fmul_rn(wx, iz), v = __fmul_rn(wy, iz);  // texel-centre offset already folded in
+                if constexpr (CHECK) {
+                    const bool skip = fabsf(wz) < 1e-8f || !(u >= LO) || !(u < fW - 1.0f + LO) || !(v >= LO) ||
+                                      !(v < fH - 1.0f + LO);
+                    ok &= ~(static_cast<unsigned>(skip) << j);
+                }
+                smp[j] = tex2D<float>(tex, u, v);
+                wx = __fadd_rn(wx, hx0);
+                wy = __fadd_rn(wy, hx1);
+                wz = __fadd_rn(wz, hx2);
+            }
+            if constexpr (SIDE & 1) smp[SIDE] = c0;  // pads the last pair: e = 0
+#pragma unroll
+            for (int p = 0; p < PAIRS; ++p) {
+                // The shift is subtracted in FP32 and only the small residual is
+                // rounded to FP16 (rounding the sample first would cost ~2.4e-4).
+                accumulate(p, __floats2half2_rn(__fsub_rn(smp[2 * p], c0), __fsub_rn(smp[2 * p + 1], c0)));
             }
         }
         const float2 f1 = __half22float2(a1), f2 = __half22float2(a2), f3 = __half22float2(a3);
@@ -230,7 +322,7 @@ __device__ __forceinline__ float source_cost(const Plane& P, cudaTextureObject_t
 template <int R, int ST>
 __device__ __forceinline__ float cost_f16(RefStats st, const __half2* s_win, const float* s_ref, int tw, int lx,
                                           int ly, int x, int y, float d, float cnx, float cny, float cnz,
-                                          const ViewDesc* __restrict__ v, int topk) {
+                                          const ViewDesc* __restrict__ v, int topk, unsigned soft_mask) {
     const float* k = v->kinv;
     const float fx = static_cast<float>(x), fy = static_cast<float>(y);
     const float Px = __fmul_rn(d, __fmaf_rn(k[0], fx, __fmaf_rn(k[1], fy, k[2])));
@@ -249,34 +341,54 @@ __device__ __forceinline__ float cost_f16(RefStats st, const __half2* s_win, con
     const int S = v->S;
     for (int s = 0; s < S; ++s) {
         const float* A = v->ab[s];
+        // Uniform over the launch: every lane of a warp takes the same sampler.
+        const bool soft = (soft_mask >> s) & 1u;
+        const float lo = soft ? 0.0f : 0.5f;  // texel-centre offset of the sampler's coordinate
         Plane P;
         P.h[6] = __fmaf_rn(A[11], m0, A[6]);
         P.h[7] = __fmaf_rn(A[11], m1, A[7]);
         P.h[8] = __fmaf_rn(A[11], m2, A[8]);
-        P.h[0] = __fmaf_rn(0.5f, P.h[6], __fmaf_rn(A[9], m0, A[0]));
-        P.h[1] = __fmaf_rn(0.5f, P.h[7], __fmaf_rn(A[9], m1, A[1]));
-        P.h[2] = __fmaf_rn(0.5f, P.h[8], __fmaf_rn(A[9], m2, A[2]));
-        P.h[3] = __fmaf_rn(0.5f, P.h[6], __fmaf_rn(A[10], m0, A[3]));
-        P.h[4] = __fmaf_rn(0.5f, P.h[7], __fmaf_rn(A[10], m1, A[4]));
-        P.h[5] = __fmaf_rn(0.5f, P.h[8], __fmaf_rn(A[10], m2, A[5]));
-        // Corner test (margin 1e-3 px): one-signed depth and all four corners inside.
+        P.h[0] = __fmaf_rn(lo, P.h[6], __fmaf_rn(A[9], m0, A[0]));
+        P.h[1] = __fmaf_rn(lo, P.h[7], __fmaf_rn(A[9], m1, A[1]));
+        P.h[2] = __fmaf_rn(lo, P.h[8], __fmaf_rn(A[9], m2, A[2]));
+        P.h[3] = __fmaf_rn(lo, P.h[6], __fmaf_rn(A[10], m0, A[3]));
+        P.h[4] = __fmaf_rn(lo, P.h[7], __fmaf_rn(A[10], m1, A[4]));
+        P.h[5] = __fmaf_rn(lo, P.h[8], __fmaf_rn(A[10], m2, A[5]));
+        // Corner test: in front of the source (w_z > 1e-6) with all four
+        // corners inside [lo, W - 1 + lo) x [lo, H - 1 + lo) by a 0.05 px
+        // margin (which covers the rounding of the row-stepped taps), tested
+        // as w_x >= ulo w_z etc. without a division.  The warp of the window
+        // rectangle is then the convex quad of its corners, so every tap is
+        // valid by the per-tap rules too.
+        const float ulo = __fadd_rn(lo, 0.05f), uhi = __fsub_rn(__fadd_rn(fW, lo), 1.05f);
+        const float vhi = __fsub_rn(__fadd_rn(fH, lo), 1.05f);
         bool inside = true;
-        float zsign = 0.f;
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             const float px = (c & 1) ? xb : xa, py = (c & 2) ? yb : ya;
             const float wz = __fmaf_rn(P.h[6], px, __fmaf_rn(P.h[7], py, P.h[8]));
-            const float u = __fdiv_rn(__fmaf_rn(P.h[0], px, __fmaf_rn(P.h[1], py, P.h[2])), wz);
-            const float vv = __fdiv_rn(__fmaf_rn(P.h[3], px, __fmaf_rn(P.h[4], py, P.h[5])), wz);
-            if (c == 0) zsign = wz;
-            inside = inside && (fabsf(wz) > 1e-6f) && (__fmul_rn(wz, zsign) > 0.f) && u >= 0.501f && u < fW - 0.501f &&
-                     vv >= 0.501f && vv < fH - 0.501f;
+            const float wxc = __fmaf_rn(P.h[0], px, __fmaf_rn(P.h[1], py, P.h[2]));
+            const float wyc = __fmaf_rn(P.h[3], px, __fmaf_rn(P.h[4], py, P.h[5]));
+            inside = inside && wz > 1e-6f && wxc >= __fmul_rn(ulo, wz) && wxc < __fmul_rn(uhi, wz) &&
+                     wyc >= __fmul_rn(ulo, wz) && wyc < __fmul_rn(vhi, wz);
         }
-        const cudaTextureObject_t tex = v->src_tex16[s];
-        // Per-lane choice: a pixel's cost depends only on its own window and plane.
-        const float c = inside
-                            ? source_cost<R, ST, false>(P, tex, st, s_win, s_ref, tw, lx, ly, x, y, fW, fH)
-                            : source_cost<R, ST, true>(P, tex, st, s_win, s_ref, tw, lx, ly, x, y, fW, fH);
+        // One form per warp: the checked form gives the unchecked form's bits
+        // whenever every tap is valid, so lanes that are inside lose nothing.
+        const bool all_inside = __all_sync(__activemask(), inside);
+        float c;
+        if (soft) {
+            const uint2* qb = soft_base(v->src_quad[s], v->quad_pitch);
+            c = all_inside ? source_cost<R, ST, false, true>(P, 0, qb, v->quad_pitch, st, s_win, s_ref, tw, lx, ly, x,
+                                                             y, fW, fH)
+                           : source_cost<R, ST, true, true>(P, 0, qb, v->quad_pitch, st, s_win, s_ref, tw, lx, ly, x,
+                                                            y, fW, fH);
+        } else {
+            const cudaTextureObject_t tex = v->src_tex16[s];
+            c = all_inside ? source_cost<R, ST, false, false>(P, tex, nullptr, 0, st, s_win, s_ref, tw, lx, ly, x, y,
+                                                              fW, fH)
+                           : source_cost<R, ST, true, false>(P, tex, nullptr, 0, st, s_win, s_ref, tw, lx, ly, x, y,
+                                                             fW, fH);
+        }
         if (c < top2) {
             top2 = c;
             if (top2 < top1) {
@@ -314,7 +426,7 @@ __device__ __forceinline__ void tile_cost16(const ViewDesc* v, int tile_x, int t
         const size_t idx = static_cast<size_t>(y) * v->W + x;
         const float4 h = v->hyp[idx];
         v->cost[idx] = cost_f16<R, ST>(st, s_win + threadIdx.x, s_ref, tw, lx, ly, x, y, h.x, h.y, h.z, h.w, v,
-                                       sc.top_k);
+                                       sc.top_k, sc.soft_mask);
     }
 }
 
@@ -405,7 +517,7 @@ __device__ __forceinline__ void tile_propagate16(const ViewDesc* v, int tile_x, 
             const int nyp = y + (cand == 2 ? -1 : (cand == 3 ? 1 : 0));
             const float4 h = v->hyp[static_cast<size_t>(nyp) * W + nxp];
             s_cost[ly][item] = cost_f16<R, ST>(ost, s_win + ly * 32 + owner, s_ref, tw, olx, ly, ox, y, h.x, h.y,
-                                               h.z, h.w, v, sc.top_k);
+                                               h.z, h.w, v, sc.top_k, sc.soft_mask);
         }
     }
     __syncwarp();
@@ -441,7 +553,7 @@ __device__ __forceinline__ void tile_propagate16(const ViewDesc* v, int tile_x, 
         float3 cn = normalize3_rn(cx, cy, cz);
         if (dot3_rn(cn, ray) > 0.0f) cn = make_float3(-cn.x, -cn.y, -cn.z);
         const float c = cost_f16<R, ST>(st, s_win + threadIdx.x, s_ref, tw, lx, ly, x, y, cd, cn.x, cn.y, cn.z, v,
-                                        sc.top_k);
+                                        sc.top_k, sc.soft_mask);
         if (c < best_cost) {
             best_cost = c;
             best = make_float4(cd, cn.x, cn.y, cn.z);

@@ -43,6 +43,33 @@ __global__ void to_planes_kernel(const void* __restrict__ src, int dtype, int W,
     }
 }
 
+// Quad plane of the FP16 software sampler.  Quad (x, y) holds the bilinear
+// patch of texels t00 = t(x,y), t10 = t(x+1,y), t01 = t(x,y+1), t11 =
+// t(x+1,y+1) (right and bottom neighbours clamped) in difference form:
+//   .x = (t00 - 0.5, t01 - t00), .y = (t10 - t00, t11 - t10 - t01 + t00),
+// each formed exactly in FP32 from the FP16 texels and rounded once to FP16,
+// so a sample is t00 + fx (t10 - t00) + fy ((t01 - t00) + fx dxy): two FP16
+// FMAs.  The -0.5 shift keeps the interpolated values within [-0.5, 0.5].
+__global__ void quads_kernel(const __half* __restrict__ src, int pitch16, int W, int H, uint2* __restrict__ quads,
+                             int quad_pitch) {
+    const size_t n = static_cast<size_t>(W) * H;
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const int y = static_cast<int>(i / W), x = static_cast<int>(i - static_cast<size_t>(y) * W);
+        const int x1 = min(x + 1, W - 1), y1 = min(y + 1, H - 1);
+        const __half* r0 = src + static_cast<size_t>(y) * pitch16;
+        const __half* r1 = src + static_cast<size_t>(y1) * pitch16;
+        const float t00 = __half2float(r0[x]), t10 = __half2float(r0[x1]);
+        const float t01 = __half2float(r1[x]), t11 = __half2float(r1[x1]);
+        const __half2 a = __floats2half2_rn(__fsub_rn(t00, 0.5f), __fsub_rn(t01, t00));
+        const __half2 b = __floats2half2_rn(__fsub_rn(t10, t00), __fadd_rn(__fsub_rn(t11, t10), __fsub_rn(t00, t01)));
+        uint2 q;
+        memcpy(&q.x, &a, sizeof q.x);
+        memcpy(&q.y, &b, sizeof q.y);
+        quads[static_cast<size_t>(y) * quad_pitch + x] = q;
+    }
+}
+
 __global__ void unpack_kernel(const float4* __restrict__ hyp, const float* __restrict__ cost_in, size_t n,
                               float* __restrict__ depth, float* __restrict__ normal, float* __restrict__ cost) {
     for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
@@ -73,6 +100,12 @@ __global__ void pack_kernel(const float* __restrict__ depth, const float* __rest
 cudaError_t launch_to_f32(const void* src, int dtype, int W, int H, float* dst, int dst_pitch, __half* dst16,
                           int dst16_pitch, cudaStream_t st) {
     to_planes_kernel<<<stream_grid(), 256, 0, st>>>(src, dtype, W, H, dst, dst_pitch, dst16, dst16_pitch);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_quads(const __half* src16, int pitch16, int W, int H, uint2* quads, int quad_pitch,
+                         cudaStream_t st) {
+    quads_kernel<<<stream_grid(), 256, 0, st>>>(src16, pitch16, W, H, quads, quad_pitch);
     return cudaGetLastError();
 }
 

@@ -89,6 +89,14 @@ typedef struct hp_params {
     float step_decay;    /* perturbation range factor per refinement step */
     int tile_w;          /* pixels per CTA row, 0 = engine choice (autotuned) */
     int tile_h;          /* rows per CTA, 0 = engine choice */
+    /* FP16-acc path only: bit s set = source s is sampled by the software
+     * bilinear sampler (quad-packed FP16 texels, fixed-point weights, FP16
+     * interpolation) instead of the texture unit.  The software sampler
+     * runs on the load/store and FP16 pipes, which sustain more taps per SM
+     * clock than the texture filter (B200: ~500 vs ~400 Mpix*iter/s at
+     * 20 x 1920x1080, r 7, s 2, 6 sources).
+     * -1 = engine default (every source), 0 = texture unit only. */
+    int soft_sources;
 } hp_params;
 
 /* One reference view to solve. */

@@ -214,6 +214,23 @@ static inline double bilinear_exact(const float* img, int W, int H, double u, do
     return (1 - a) * (1 - b) * t00 + a * (1 - b) * t10 + (1 - a) * b * t01 + a * b * t11;
 }
 
+/* The FP16 path's software sampler: the coordinate rounded to 8 fractional
+ * bits (round to nearest even, the rounding of its fused multiply-add) and
+ * separable weights a/256, b/256 (no joint quantisation of the 2-D weights). */
+static inline double bilinear_sep8(const float* img, int W, int H, double u, double v) {
+    const double X = nearbyint(u * 256.0), Y = nearbyint(v * 256.0);
+    const double fi = floor(X / 256.0), fj = floor(Y / 256.0);
+    const long i = (long)fi, j = (long)fj;
+    const double a = (X - fi * 256.0) / 256.0, b = (Y - fj * 256.0) / 256.0;
+    double t00 = texel(img, W, H, i, j), t10 = texel(img, W, H, i + 1, j);
+    double t01 = texel(img, W, H, i, j + 1), t11 = texel(img, W, H, i + 1, j + 1);
+    return (1 - a) * (1 - b) * t00 + a * (1 - b) * t10 + (1 - a) * b * t01 + a * b * t11;
+}
+
+static unsigned g_soft_sources = 0;
+void orc_set_soft_sources(unsigned mask) { g_soft_sources = mask; }
+unsigned orc_get_soft_sources(void) { return g_soft_sources; }
+
 static inline double bilinear_q8(const float* img, int W, int H, double u, double v) {
     /* The texture unit's fixed-point weights from an exact coordinate (FP64 oracle with texture weights). */
     long X = g_tex_rounding == 0 ? (long)floor(u * 256.0 + 0.5) : (long)floor(u * 256.0);
@@ -348,8 +365,9 @@ int orc_source_ncc_f64(const orc_view* v, int x, int y, double d, double nx, dou
                 if (fabs(wz) < 1e-8) continue;
                 const double u = wx / wz, vv = wy / wz;
                 if (u < 0.0 || u >= v->W - 1.0 || vv < 0.0 || vv >= v->H - 1.0) continue;
-                const double sv = qw ? bilinear_q8(v->src[s], v->W, v->H, u, vv)
-                                     : bilinear_exact(v->src[s], v->W, v->H, u, vv);
+                const double sv = !qw ? bilinear_exact(v->src[s], v->W, v->H, u, vv)
+                                  : ((g_soft_sources >> s) & 1u) ? bilinear_sep8(v->src[s], v->W, v->H, u, vv)
+                                                                 : bilinear_q8(v->src[s], v->W, v->H, u, vv);
                 sr += rv;
                 ss += sv;
                 srr += rv * rv;

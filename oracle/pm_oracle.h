@@ -50,6 +50,12 @@ typedef struct orc_view {
 void orc_set_tex_rounding(int mode);
 int orc_get_tex_rounding(void);
 
+/* FP64 cost with quantized weights: sources whose bit is set use the FP16
+ * path's software-sampler model (separable 8-bit weights, coordinates rounded
+ * to nearest) instead of the texture unit's.  Default 0. */
+void orc_set_soft_sources(unsigned mask);
+unsigned orc_get_soft_sources(void);
+
 void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 float orc_u01(uint32_t x);
 

@@ -55,6 +55,8 @@ def lib():
         fp, dp = P(C.c_float), P(C.c_double)
         sig = {
             "orc_set_tex_rounding": (None, [C.c_int]),
+            "orc_set_soft_sources": (None, [C.c_uint]),
+            "orc_get_soft_sources": (C.c_uint, []),
             "orc_philox4x32_10": (None, [P(C.c_uint32), P(C.c_uint32), P(C.c_uint32)]),
             "orc_u01": (C.c_float, [C.c_uint32]),
             "orc_setup_f64": (C.c_int, [P(OrcCamera), P(OrcCamera), C.c_int, dp, dp]),
@@ -205,6 +207,16 @@ def geometric_filter(ref_cam, depth, normal, conf, src_cams, src_depths, src_nor
 
 def set_tex_rounding(mode: int):
     lib().orc_set_tex_rounding(mode)
+
+
+def set_soft_sources(mask: int):
+    """Sources (bit per source) whose quantized-weight FP64 cost uses the FP16 path's
+    software-sampler model (separable 8-bit weights, round-to-nearest coordinates)."""
+    lib().orc_set_soft_sources(mask & 0xFF)
+
+
+def soft_sources() -> int:
+    return int(lib().orc_get_soft_sources())
 
 
 def num_threads() -> int:

@@ -87,34 +87,41 @@ def test_fp32_cost_vs_cpu_oracle(hp, ctx, ids_full, full_scene, po):
             assert st["p90"] <= p90 and st["p99"] <= p99 and st["max"] <= 5e-2, (stride, tag, st)
 
 
-@pytest.mark.parametrize("radius,stride", [(5, 1), (5, 2), (7, 2), (3, 1)])
-def test_fp16acc_cost_vs_fp64_oracle(hp, ctx, ids_full, full_scene, po, radius, stride):
+@pytest.mark.parametrize("radius,stride,soft", [(5, 1, -1), (5, 2, -1), (7, 2, -1), (3, 1, -1), (7, 2, 0),
+                                                (5, 1, 0), (5, 2, 0x3), (3, 1, 0xAA)])
+def test_fp16acc_cost_vs_fp64_oracle(hp, ctx, ids_full, full_scene, po, radius, stride, soft):
     """FP16-storage / FP32-accumulate cost vs the FP64 oracle.
 
-    Gate: against FP64 evaluation of the same sampling model (the texture unit's fixed-point
-    bilinear weights, which the reference's algorithm and both engine paths use), |err| <= 1e-3
-    on ground-truth planes everywhere and on >= 99.9% of random hypotheses (the rest are validity
-    flips at the count / contrast thresholds, where FP32 flips too).
-    Also bounded: against exact-bilinear FP64 math, p99 <= 1e-3 - the texture weights' own
+    `soft` picks which sources the software bilinear sampler reads (-1: the engine default,
+    every source; 0: texture unit only; 0x3, 0xAA: mixed, some sources in software, the rest textured).
+    Gate: against FP64 evaluation of the same sampling model (per source, the texture unit's
+    fixed-point bilinear weights or the software sampler's separable 8-bit weights),
+    |err| <= 1e-3 on ground-truth planes everywhere and on >= 99.9% of random hypotheses (the
+    rest are validity flips at the count / contrast thresholds, where FP32 flips too).
+    Also bounded: against exact-bilinear FP64 math, p99 <= 1e-3 - the 8-bit weights' own
     quantisation (shared with the FP32 path and the reference) dominates that difference.
     The oracle reads the images as the FP16 path stores them (FP16-rounded), so the comparison
     measures arithmetic error, not the storage format's input rounding."""
     s, r = full_scene, 2
     job = job_for(hp, s, ids_full, r)
-    p = hp.default_params(radius=radius, stride=stride, precision=hp.PRECISION_F16ACC)
+    p = hp.default_params(radius=radius, stride=stride, precision=hp.PRECISION_F16ACC, soft_sources=soft)
     as16 = lambda a: a.astype(np.float16).astype(np.float32)
     srcs = s.sources[r]
     v = po.View(as16(s.views[r].image_f32), [as16(s.views[i].image_f32) for i in srcs], radius=radius,
                 stride=stride, ref_cam=cam_of(s, r), src_cams=[cam_of(s, i) for i in srcs])
-    for tag, (d, n) in hypotheses(hp, ctx, s, ids_full, r).items():
-        c16 = engine_cost(hp, ctx, job, p, d, n)
-        c64q = v.cost_map_f64(d, n, quantized=True)
-        e = np.abs(c16 - c64q)
-        if tag == "gt":
-            assert e.max() <= 1e-3, err_stats(c16, c64q)
-        assert (e <= 1e-3).mean() >= 0.999, (tag, err_stats(c16, c64q))
-        c64 = v.cost_map_f64(d, n, quantized=False)
-        assert err_stats(c16, c64)["p99"] <= 1e-3, (tag, err_stats(c16, c64))
+    po.set_soft_sources(0xFF if soft < 0 else soft)
+    try:
+        for tag, (d, n) in hypotheses(hp, ctx, s, ids_full, r).items():
+            c16 = engine_cost(hp, ctx, job, p, d, n)
+            c64q = v.cost_map_f64(d, n, quantized=True)
+            e = np.abs(c16 - c64q)
+            if tag == "gt":
+                assert e.max() <= 1e-3, err_stats(c16, c64q)
+            assert (e <= 1e-3).mean() >= 0.999, (tag, err_stats(c16, c64q))
+            c64 = v.cost_map_f64(d, n, quantized=False)
+            assert err_stats(c16, c64)["p99"] <= 1e-3, (tag, err_stats(c16, c64))
+    finally:
+        po.set_soft_sources(0)
 
 
 def test_init_bit_exact_vs_oracle(hp, ctx, ids_full, full_scene, po):
