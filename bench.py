@@ -42,6 +42,10 @@ PKG = "hemiphoto3d-private_b200"
 WORKLOAD = dict(name="multi_object_20x1920x1080", views=20, width=1920, height=1080, sources=6, radius=7, stride=2,
                 iterations=12, depth_range=[1.0, 6.0], image_dtype="u8")
 METRIC = "depth-map Mpix*iter/s on 1 B200 (FP16-acc vs plain FP32)"
+# Serving form: Poisson arrivals, each request one depth-map solve on the FP16-acc path.
+SERVING = dict(name="serving_poisson", sizes=[[640, 480], [1920, 1080], [4000, 3000]], sources=[2, 8],
+               iterations=[4, 12], radius=7, stride=2, requests=240, rate_per_s=10.0, views_per_size=9,
+               mem_fraction=0.8)
 
 
 def parse():
@@ -57,6 +61,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--views", type=int, default=WORKLOAD["views"], help="reduce for profiling captures only")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving leg (N = 1 only)")
+    ap.add_argument("--serve-requests", type=int, default=SERVING["requests"])
+    ap.add_argument("--serve-rate", type=float, default=SERVING["rate_per_s"], help="Poisson arrivals per second")
     return ap.parse_args()
 
 
@@ -355,6 +362,8 @@ def run_engine(args, rank, world, local_rank):
         "clocks": clocks,
         "variants": variants,
     }
+    if world == 1 and not args.no_serving:
+        line["serving"] = run_serving(args, hp, local_rank)
     # CPU baseline (rank 0, N = 1)
     if world == 1 and not args.no_cpu_baseline:
         rate, secs, thr, desc = cpu_sample(s, args.cpu_rows)
@@ -362,6 +371,98 @@ def run_engine(args, rank, world, local_rank):
                                 "sample": desc, "seconds": round(secs, 2)}
     ctx.close()
     return line
+
+
+def run_serving(args, hp, device: int):
+    """Serving form: requests of sizes drawn from SERVING["sizes"] (2-8 sources, 4-12 iterations, FP16-acc,
+    r 7, s 2) arrive as a Poisson stream; images stay resident on the device (uploaded once per view pool), the
+    server admits requests by free HBM (<= 80% of the device) and batches all admitted ones into its persistent
+    launches.  Latency is submit -> completion; throughput is completed Mpix*iter over the span from the first
+    submission to the last completion."""
+    import torch
+    scene = importlib.import_module(PKG + ".scene")
+    rng = np.random.default_rng(2024)
+    ctx = hp.Context(device)
+    pools = []
+    for k, (w, h) in enumerate(SERVING["sizes"]):
+        sc = scene.multi_object(seed=31 + k, w=w, h=h, n_views=SERVING["views_per_size"], n_src=8,
+                                f=1500.0 * w / 1920.0, n_refs=1)
+        ids = [ctx.upload(v.image) for v in sc.views]
+        cams = [hp.make_camera(v.cam.K, v.cam.R, v.cam.t) for v in sc.views]
+        pools.append((sc, ids, cams, w, h))
+    reqs = []
+    t = 0.0
+    for i in range(args.serve_requests):
+        t += rng.exponential(1.0 / args.serve_rate)
+        sc, ids, cams, w, h = pools[int(rng.integers(0, len(pools)))]
+        r = int(rng.integers(0, len(sc.views)))
+        S = int(rng.integers(SERVING["sources"][0], SERVING["sources"][1] + 1))
+        srcs = scene.nearest_sources([v.cam for v in sc.views], r, S)
+        it = int(rng.integers(SERVING["iterations"][0], SERVING["iterations"][1] + 1))
+        job = hp.make_job(ids[r], [ids[j] for j in srcs], cams[r], [cams[j] for j in srcs], *sc.depth_range,
+                          seed=7 + i, view_id=r, iterations=it)
+        reqs.append((t, job, w, h, w * h * it))
+    params = hp.default_params(radius=SERVING["radius"], stride=SERVING["stride"], precision=hp.PRECISION_F16ACC)
+    srv = hp.Server(ctx, params, mem_fraction=SERVING["mem_fraction"])
+    # Warm-up: one request of each size, not counted.
+    for sc, ids, cams, w, h in pools:
+        m = hp.maps_of(torch.empty(h, w, device="cuda"), torch.empty(h, w, 3, device="cuda"),
+                       torch.empty(h, w, device="cuda"))
+        srv.submit(hp.make_job(ids[0], [ids[1], ids[2]], cams[0], [cams[1], cams[2]], *sc.depth_range,
+                               iterations=2), m)
+    srv.drain(timeout_ms=120000)
+    srv.poll(capacity=16)
+    srv.reset_stats()
+    done, outs = [], {}
+    lock = threading.Lock()
+
+    def producer():
+        t0 = time.perf_counter()
+        for t_arr, job, w, h, _ in reqs:
+            dt = t_arr - (time.perf_counter() - t0)
+            if dt > 0:
+                time.sleep(dt)
+            m = hp.maps_of(torch.empty(h, w, device="cuda"), torch.empty(h, w, 3, device="cuda"),
+                           torch.empty(h, w, device="cuda"))
+            rid = srv.submit(job, m)
+            with lock:
+                outs[rid] = m
+
+    t_start = time.perf_counter()
+    th = threading.Thread(target=producer)
+    th.start()
+    deadline = t_start + reqs[-1][0] + 600
+    while len(done) < len(reqs) and time.perf_counter() < deadline:
+        for c in srv.poll(timeout_ms=100):
+            done.append(c)
+            with lock:
+                outs.pop(c["request_id"], None)
+    wall = time.perf_counter() - t_start
+    th.join()
+    st = srv.stats()
+    srv.close()
+    ctx.close()
+    ok = [c for c in done if c["status"] == 0]
+    lat = np.array([c["latency_ms"] for c in ok]) if ok else np.zeros(1)
+    pix_iter = sum(r[4] for r in reqs) / 1e6
+    offered = pix_iter / reqs[-1][0]
+    return {
+        "workload": SERVING["name"], "requests": len(reqs), "completed": len(ok), "failed": len(done) - len(ok),
+        "rate_per_s": args.serve_rate, "offered_mpix_iter_per_s": round(offered, 1),
+        "p50_ms": round(float(np.percentile(lat, 50)), 1), "p99_ms": round(float(np.percentile(lat, 99)), 1),
+        "mean_ms": round(float(lat.mean()), 1), "max_ms": round(float(lat.max()), 1),
+        "queue_p50_ms": round(float(np.percentile([c["queue_ms"] for c in ok], 50)), 1) if ok else None,
+        "mpix_iter_per_s": round(st["pixel_iterations"] / 1e6 / wall, 1),
+        "device_mpix_iter_per_s": round(st["pixel_iterations"] / 1e6 / (st["device_ms"] / 1e3), 1)
+        if st["device_ms"] else None,
+        "device_busy_frac": round(st["device_ms"] / 1e3 / wall, 3), "wall_s": round(wall, 1),
+        "peak_active": st["peak_active"], "steps": st["steps"], "launches": st["launches"],
+        "peak_state_gb": round(st["peak_state_bytes"] / 1e9, 2),
+        "config": {"sizes": SERVING["sizes"], "sources": SERVING["sources"], "iterations": SERVING["iterations"],
+                   "window": "15x15", "stride": SERVING["stride"], "precision": "f16acc",
+                   "admission": "state <= 80% of device memory", "images": "resident, u8 uploads, 9 views per size",
+                   "arrivals": f"Poisson, {args.serve_rate}/s, {len(reqs)} requests"},
+    }
 
 
 def run_reference(args, rank, world):

@@ -11,6 +11,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import threading
 from dataclasses import dataclass, field
 from typing import List, Optional, Sequence
 
@@ -94,6 +95,29 @@ class PlanInfo(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class ServerOptions(C.Structure):
+    _fields_ = [("max_active", C.c_int), ("mem_fraction", C.c_float), ("mem_limit", C.c_uint64),
+                ("passes_per_step", C.c_int), ("split_launches", C.c_int), ("ctas_per_sm", C.c_int),
+                ("inflight_steps", C.c_int), ("wait_limit_ms", C.c_int)]
+
+
+class Completion(C.Structure):
+    _fields_ = [("request_id", C.c_uint64), ("status", C.c_int), ("latency_ms", C.c_double),
+                ("queue_ms", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("admitted", C.c_uint64), ("completed", C.c_uint64),
+                ("failed", C.c_uint64), ("steps", C.c_uint64), ("launches", C.c_uint64), ("queued", C.c_int),
+                ("active", C.c_int), ("peak_active", C.c_int), ("p50_ms", C.c_double), ("p99_ms", C.c_double),
+                ("mean_ms", C.c_double), ("max_ms", C.c_double), ("pixel_iterations", C.c_double),
+                ("device_ms", C.c_double), ("state_bytes", C.c_uint64), ("peak_state_bytes", C.c_uint64),
+                ("budget_bytes", C.c_uint64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 def _load() -> C.CDLL:
     if not os.path.exists(LIB_PATH):
         raise ImportError(
@@ -137,6 +161,17 @@ def _load() -> C.CDLL:
         "hp_plan_destroy": (C.c_int, [C.c_void_p]),
         "hp_schedule_build": (C.c_int, [C.c_int, P(C.c_int), P(C.c_int), P(C.c_int), C.c_int, P(C.c_int),
                                         P(C.c_int), P(C.c_int), P(C.c_int)]),
+        "hp_server_options_default": (None, [P(ServerOptions)]),
+        "hp_server_create": (C.c_int, [C.c_void_p, P(Params), P(ServerOptions), P(C.c_void_p)]),
+        "hp_submit": (C.c_int, [C.c_void_p, P(Job), P(Maps), P(C.c_uint64)]),
+        "hp_poll": (C.c_int, [C.c_void_p, P(Completion), C.c_int, P(C.c_int), C.c_int]),
+        "hp_server_drain": (C.c_int, [C.c_void_p, C.c_int]),
+        "hp_server_stats_get": (C.c_int, [C.c_void_p, P(ServerStats)]),
+        "hp_server_stats_reset": (C.c_int, [C.c_void_p]),
+        "hp_server_last_error": (C.c_char_p, [C.c_void_p]),
+        "hp_server_destroy": (C.c_int, [C.c_void_p]),
+        "hp_server_simulate": (C.c_int, [C.c_int, P(C.c_int), P(C.c_uint64), P(C.c_int), C.c_int, C.c_uint64,
+                                         C.c_int, P(C.c_int), P(C.c_int), P(C.c_int)]),
         "hp_pfm_write": (C.c_int, [C.c_char_p, C.c_void_p, C.c_int, C.c_int, C.c_int]),
         "hp_pfm_read": (C.c_int, [C.c_char_p, C.c_void_p, C.c_size_t, P(C.c_int), P(C.c_int), P(C.c_int)]),
     }
@@ -157,7 +192,9 @@ EXPORTS = (
     "hp_image_size", "hp_setup_homographies", "hp_solve", "hp_init_hypotheses", "hp_ncc_cost",
     "hp_propagate_pass", "hp_geometric_filter", "hp_pfm_write", "hp_pfm_read", "hp_solve_static",
     "hp_plan_options_default", "hp_plan_create", "hp_plan_run", "hp_plan_launch", "hp_plan_wait", "hp_plan_tune",
-    "hp_plan_get_info", "hp_plan_destroy", "hp_schedule_build",
+    "hp_plan_get_info", "hp_plan_destroy", "hp_schedule_build", "hp_server_options_default", "hp_server_create",
+    "hp_submit", "hp_poll", "hp_server_drain", "hp_server_stats_get", "hp_server_stats_reset",
+    "hp_server_last_error", "hp_server_destroy", "hp_server_simulate",
 )
 STATIC_MAX_PIXELS = 1280 * 1024  # HP_STATIC_MAX_PIXELS
 
@@ -403,6 +440,105 @@ def schedule_build(tiles: Sequence[int], stage_begin: Sequence[int], stage_end: 
         raise HpError(st, "hp_schedule_build")
     k = ne.value
     return np.array(et[:k + 1]), np.array(ev[:k]), np.array(es[:k])
+
+
+def server_options(**kw) -> ServerOptions:
+    o = ServerOptions()
+    lib.hp_server_options_default(C.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+class Server:
+    """Continuous-batching solve server (hp_server): submit jobs from any thread, poll completions.
+
+    The output maps of a request are kept alive here until its completion has been polled."""
+
+    def __init__(self, ctx: "Context", params: Params, options: ServerOptions | None = None, **kw):
+        self.ctx = ctx
+        opts = options if options is not None else server_options(**kw)
+        h = C.c_void_p()
+        ctx._check(lib.hp_server_create(ctx.handle, C.byref(params), C.byref(opts), C.byref(h)), "hp_server_create")
+        self._h = h
+        self._maps = {}
+        self._lock = threading.Lock()
+
+    def _fail(self, st: int, what: str):
+        raise HpError(st, f"{what}: {lib.hp_server_last_error(self._h).decode()}")
+
+    def submit(self, job: Job, maps: Maps) -> int:
+        rid = C.c_uint64()
+        st = lib.hp_submit(self._h, C.byref(job), C.byref(maps), C.byref(rid))
+        if st != OK:
+            self._fail(st, "hp_submit")
+        with self._lock:
+            self._maps[rid.value] = maps
+        return rid.value
+
+    def poll(self, timeout_ms: int = 0, capacity: int = 256) -> List[dict]:
+        """Completed requests as dicts (request_id, status, latency_ms, queue_ms)."""
+        buf = (Completion * capacity)()
+        n = C.c_int()
+        st = lib.hp_poll(self._h, buf, capacity, C.byref(n), int(timeout_ms))
+        if st != OK:
+            self._fail(st, "hp_poll")
+        out = []
+        for c in buf[:n.value]:
+            out.append({"request_id": c.request_id, "status": c.status, "latency_ms": c.latency_ms,
+                        "queue_ms": c.queue_ms})
+            with self._lock:
+                self._maps.pop(c.request_id, None)
+        return out
+
+    def drain(self, timeout_ms: int = -1):
+        st = lib.hp_server_drain(self._h, int(timeout_ms))
+        if st != OK:
+            self._fail(st, "hp_server_drain")
+
+    def stats(self) -> dict:
+        s = ServerStats()
+        st = lib.hp_server_stats_get(self._h, C.byref(s))
+        if st != OK:
+            self._fail(st, "hp_server_stats_get")
+        return s.as_dict()
+
+    def reset_stats(self):
+        lib.hp_server_stats_reset(self._h)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.hp_server_destroy(self._h)
+            self._h = None
+            self._maps.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def server_simulate(arrive_step: Sequence[int], state_bytes: Sequence[int], stages: Sequence[int], max_active: int,
+                    budget: int, passes_per_step: int):
+    """The server's admission and step policy without a device (hp_server_simulate):
+    (admit_step[n], finish_step[n], steps)."""
+    n = len(arrive_step)
+    m = max(1, n)
+    a = (C.c_int * m)(*arrive_step)
+    b = (C.c_uint64 * m)(*state_bytes)
+    k = (C.c_int * m)(*stages)
+    adm, fin, steps = (C.c_int * m)(), (C.c_int * m)(), C.c_int()
+    st = lib.hp_server_simulate(n, a, b, k, max_active, budget, passes_per_step, adm, fin, C.byref(steps))
+    if st != OK:
+        raise HpError(st, "hp_server_simulate")
+    return np.array(adm[:n]), np.array(fin[:n]), steps.value
 
 
 def make_job(ref_image: int, src_images: Sequence[int], ref_cam: Camera, src_cams: Sequence[Camera],

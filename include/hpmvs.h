@@ -320,6 +320,87 @@ hp_status hp_plan_destroy(hp_plan* plan);
 hp_status hp_schedule_build(int num_views, const int* tiles, const int* stage_begin, const int* stage_end,
                             int capacity, int* entry_ticket, int* entry_view, int* entry_stage, int* num_entries);
 
+/* ---------------------------------------------------------------------------
+ * Server: continuous batching of depth-map solves.  No counterpart in the
+ * reference, which solves one view at a time, synchronously
+ * (runPatchMatchMVS, patchmatch_mvs.cu:1076-1260).  Requests - one hp_job
+ * each, with its own size, sources and iteration count, over images already
+ * uploaded to the context - are submitted from any host thread.  A worker
+ * thread admits queued requests in arrival order while request slots and
+ * device memory allow, and runs steps: each step advances every admitted
+ * request by `passes_per_step` stages (initialisation + cost, red-black
+ * half-passes, unpacking into its maps) in the persistent kernel, all
+ * requests together.  A request that arrives while others are on the GPU
+ * joins at the next step.  Its result does not depend on what it was
+ * batched with: it equals hp_solve of the same job bit for bit.
+ * While a server runs, the context's images must stay uploaded until the
+ * requests that read them have completed; other work on the context may
+ * proceed from the caller's thread (the server uses its own stream).
+ * ------------------------------------------------------------------------- */
+typedef struct hp_server hp_server;
+
+typedef struct hp_server_options {
+    int max_active;         /* request slots (admitted, not yet completed); 0 = 64 */
+    float mem_fraction;     /* admit while device memory in use stays <= this fraction
+                             * of the device total (0 = 0.8) */
+    uint64_t mem_limit;     /* if nonzero: byte budget for request state instead */
+    int passes_per_step;    /* stages per request per step, 1..64 (0 = 4) */
+    int split_launches;     /* 1: one launch per stage offset of a step (no waits between
+                             * tiles); 0: one persistent launch per step */
+    int ctas_per_sm;        /* resident CTAs per SM (0 = the occupancy maximum) */
+    int inflight_steps;     /* steps enqueued ahead of the oldest unfinished one, 1..4 (0 = 2) */
+    int wait_limit_ms;      /* bound on one inter-tile dependency wait (0 = 2000) */
+} hp_server_options;
+
+/* One finished request. */
+typedef struct hp_completion {
+    uint64_t request_id;
+    int status;             /* hp_status: HP_OK, or why the request failed */
+    double latency_ms;      /* hp_submit to completion, host clock */
+    double queue_ms;        /* hp_submit to admission */
+} hp_completion;
+
+typedef struct hp_server_stats {
+    uint64_t submitted, admitted, completed, failed;
+    uint64_t steps, launches;
+    int queued, active, peak_active;
+    double p50_ms, p99_ms, mean_ms, max_ms;   /* latency of the completed requests */
+    double pixel_iterations;                  /* sum of W * H * iterations, completed */
+    double device_ms;                         /* device time of all finished steps */
+    uint64_t state_bytes, peak_state_bytes;   /* request state held now / at most */
+    uint64_t budget_bytes;                    /* admission budget at the last admission */
+} hp_server_stats;
+
+void hp_server_options_default(hp_server_options* o);
+/* params apply to every request (radius, stride, precision, ...). */
+hp_status hp_server_create(hp_ctx* ctx, const hp_params* params, const hp_server_options* options,
+                           hp_server** server);
+/* Queue one solve.  `out` (depth, normal, cost; host or device memory) must
+ * stay valid until the request completes.  HP_ERR_OUT_OF_MEMORY when the
+ * request alone exceeds the admission budget. */
+hp_status hp_submit(hp_server* s, const hp_job* job, const hp_maps* out, uint64_t* request_id);
+/* Completed requests, oldest first: up to `capacity` into `done`, waiting up
+ * to timeout_ms (0: no wait, < 0: until one completes) for the first. */
+hp_status hp_poll(hp_server* s, hp_completion* done, int capacity, int* num_done, int timeout_ms);
+/* Waits until no request is queued or running (HP_ERR_TIMEOUT after timeout_ms, < 0 = no limit). */
+hp_status hp_server_drain(hp_server* s, int timeout_ms);
+hp_status hp_server_stats_get(hp_server* s, hp_server_stats* stats);
+hp_status hp_server_stats_reset(hp_server* s);
+const char* hp_server_last_error(hp_server* s);
+/* Stops the worker after the requests already admitted finish; queued
+ * requests complete with HP_ERR_CANCELLED (their completions are dropped). */
+hp_status hp_server_destroy(hp_server* s);
+
+/* The server's admission and step-composition policy run without a device,
+ * for tests: requests k = 0..n-1 arrive before steps arrive_step[k], need
+ * state_bytes[k] and have stages[k] stages (2 * iterations + 2).  With the
+ * given slots, byte budget and stages per step, admit_step[k] and
+ * finish_step[k] receive the step in which request k is admitted and the one
+ * in which its last stage runs; *steps the number of steps run. */
+hp_status hp_server_simulate(int n, const int* arrive_step, const uint64_t* state_bytes, const int* stages,
+                             int max_active, uint64_t budget, int passes_per_step, int* admit_step,
+                             int* finish_step, int* steps);
+
 /* Replaces saveDepthMapPFM / loadDepthMapPFM (patchmatch_mvs.cu:990-1022):
  * 'Pf' (channels 1) or 'PF' (channels 3) little-endian PFM, rows bottom-up. */
 hp_status hp_pfm_write(const char* path, const float* data, int width, int height, int channels);
