@@ -43,6 +43,9 @@ WORKLOAD = dict(name="multi_object_20x1920x1080", views=20, width=1920, height=1
                 iterations=12, depth_range=[1.0, 6.0], image_dtype="u8")
 METRIC = "depth-map Mpix*iter/s on 1 B200 (FP16-acc vs plain FP32)"
 # Serving form: Poisson arrivals, each request one depth-map solve on the FP16-acc path.
+# Batched form: one plan over views of uneven sizes, autotuned schedule, replayed as a CUDA graph.
+BATCHED = dict(name="batched_uneven_64", views=64, sizes=[[640, 480], [1280, 720], [1920, 1080], [4000, 3000]],
+               sources=[2, 8], iterations=[6, 12], radius=7, stride=2, views_per_size=9, runs=3, tune_repeats=2)
 SERVING = dict(name="serving_poisson", sizes=[[640, 480], [1920, 1080], [4000, 3000]], sources=[2, 8],
                iterations=[4, 12], radius=7, stride=2, requests=240, rate_per_s=10.0, views_per_size=9,
                mem_fraction=0.8)
@@ -62,6 +65,7 @@ def parse():
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--views", type=int, default=WORKLOAD["views"], help="reduce for profiling captures only")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving leg (N = 1 only)")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-plan leg (N = 1 only)")
     ap.add_argument("--serve-requests", type=int, default=SERVING["requests"])
     ap.add_argument("--serve-rate", type=float, default=SERVING["rate_per_s"], help="Poisson arrivals per second")
     return ap.parse_args()
@@ -114,7 +118,8 @@ class ClockSampler:
 # ------------------------------------------------------------------------------------------------
 def build_scene(views: int):
     scene = importlib.import_module(PKG + ".scene")
-    return scene.multi_object(n_views=max(views, WORKLOAD["sources"] + 1), n_refs=views)
+    # The full 20-view arc is always rendered, so a reduced --views case keeps the workload's geometry.
+    return scene.multi_object(n_views=max(views, WORKLOAD["views"]), n_refs=views)
 
 
 def cpu_sample(s, rows: int, reps: int = 1):
@@ -348,11 +353,22 @@ def run_engine(args, rank, world, local_rank):
                      "kernel": "propagate half-pass", "ms_per_launch": round(prop_ms, 4),
                      "algorithmic_bytes_per_launch": int(visits * hbm_bytes_per_visit),
                      "note": "compulsory DRAM bytes; HBM does not bind this kernel - see roofline_tex"},
-        "roofline_tex": {"bound": "texture-filter fetches", "achieved": round(fetch_rate / 1e9, 2),
+        "roofline_tex": {"bound": "texture-filter fetches" if head == "f32" else
+                         "bilinear taps (software sampler; the texture rate is the reference ceiling)", "achieved": round(fetch_rate / 1e9, 2),
                          "peak": None if tex_peak is None else round(tex_peak / 1e9, 2), "unit": "Gfetch/s",
                          "frac": None if not tex_peak else round(fetch_rate / tex_peak, 4),
                          "peak_source": "measured live (L1-resident bilinear fetch microbenchmark)",
                          "algorithmic_fetches_per_launch": int(visits * taps_per_visit)},
+        # On-chip gather bytes (4 bilinear texels of the source + 1 reference value per tap, at the stored
+        # element width) against the measured shared-memory/L1 read bandwidth.
+        "roofline_l1": {"bound": "L1/shared gather bytes",
+                        "achieved": round(fetch_rate * (4 * b_img + b_img) / 1e9, 1),
+                        "peak": None if not onchip.get("smem_bytes_per_s") else round(onchip["smem_bytes_per_s"] / 1e9, 1),
+                        "unit": "GB/s",
+                        "frac": None if not onchip.get("smem_bytes_per_s")
+                        else round(fetch_rate * 5 * b_img / onchip["smem_bytes_per_s"], 4),
+                        "bytes_per_tap": 5 * b_img,
+                        "peak_source": "measured live (shared-memory streaming microbenchmark)"},
         "roofline_fp32": {"achieved_fma_equiv": None if fma_peak is None else round(fetch_rate * 14 / 1e12, 3),
                           "peak_fma": None if fma_peak is None else round(fma_peak / 1e12, 3), "unit": "TFMA/s",
                           "note": "~14 FMA-equivalent issue slots per tap on the FP32 path (28 ops)"},
@@ -362,6 +378,19 @@ def run_engine(args, rank, world, local_rank):
         "clocks": clocks,
         "variants": variants,
     }
+    for name, var in variants.items():
+        b_v = 2 if name == "f16acc" else 4
+        rate_v = visits * taps_per_visit / (var["propagate_ms_per_launch"] * 1e-3)
+        var["taps_per_s"] = rate_v
+        if onchip.get("smem_bytes_per_s"):
+            var["roofline_l1"] = {"achieved": round(rate_v * 5 * b_v / 1e9, 1), "unit": "GB/s",
+                                  "frac": round(rate_v * 5 * b_v / onchip["smem_bytes_per_s"], 4)}
+    if world == 1 and not args.no_batched:
+        bctx = hp.Context(local_rank)
+        try:
+            line["batched"] = run_batched(args, hp, bctx)
+        finally:
+            bctx.close()
     if world == 1 and not args.no_serving:
         line["serving"] = run_serving(args, hp, local_rank)
     # CPU baseline (rank 0, N = 1)
@@ -371,6 +400,70 @@ def run_engine(args, rank, world, local_rank):
                                 "sample": desc, "seconds": round(secs, 2)}
     ctx.close()
     return line
+
+
+def view_pools(hp, ctx, sizes, seed0):
+    """Per size, a 9-view arc of the multi-object generator (its own seeded layout), uploaded once."""
+    scene = importlib.import_module(PKG + ".scene")
+    pools = {}
+    for k, (w, h) in enumerate(sizes):
+        if (w, h) in pools:
+            continue
+        sc = scene.multi_object(seed=seed0 + k, w=w, h=h, n_views=9, n_src=8, f=1500.0 * w / 1920.0, n_refs=1)
+        ids = [ctx.upload(v.image) for v in sc.views]
+        cams = [hp.make_camera(v.cam.K, v.cam.R, v.cam.t) for v in sc.views]
+        pools[(w, h)] = (sc, ids, cams, w, h)
+    return pools
+
+
+def run_batched(args, hp, ctx):
+    """Batched form: BATCHED["views"] reference views of sizes drawn from BATCHED["sizes"], 2-8 sources and
+    6-12 iterations each, in one plan.  The autotuner times the per-pass graph and the persistent kernel at
+    every resident-CTA count and keeps the fastest; the plan then replays as one CUDA graph.  Reported:
+    Mpix*iter/s of the tuned plan (device-resident, median of the timed runs) for both precisions."""
+    import torch
+    scene = importlib.import_module(PKG + ".scene")
+    rng = np.random.default_rng(4096)
+    pools = view_pools(hp, ctx, BATCHED["sizes"], 51)
+    jobs, shapes = [], []
+    for i in range(BATCHED["views"]):
+        w, h = BATCHED["sizes"][int(rng.integers(0, len(BATCHED["sizes"])))]
+        sc, ids, cams, _, _ = pools[(w, h)]
+        r = int(rng.integers(0, len(sc.views)))
+        S = int(rng.integers(BATCHED["sources"][0], BATCHED["sources"][1] + 1))
+        srcs = scene.nearest_sources([v.cam for v in sc.views], r, S)
+        it = int(rng.integers(BATCHED["iterations"][0], BATCHED["iterations"][1] + 1))
+        jobs.append(hp.make_job(ids[r], [ids[j] for j in srcs], cams[r], [cams[j] for j in srcs], *sc.depth_range,
+                                seed=1000 + i, view_id=i, iterations=it))
+        shapes.append((h, w))
+    outs = [hp.maps_of(torch.empty(h, w, device="cuda"), torch.empty(h, w, 3, device="cuda"),
+                       torch.empty(h, w, device="cuda")) for h, w in shapes]
+    stream = torch.cuda.ExternalStream(ctx.stream_handle)
+    res = {"workload": BATCHED["name"], "views": len(jobs),
+           "sizes_drawn": {f"{w}x{h}": sum(1 for s in shapes if s == (h, w)) for w, h in BATCHED["sizes"]}}
+    for prec in ("f32", "f16acc"):
+        params = hp.default_params(radius=BATCHED["radius"], stride=BATCHED["stride"],
+                                   precision=hp.PRECISION_F16ACC if prec == "f16acc" else hp.PRECISION_F32)
+        with hp.Plan(ctx, jobs, params, outs) as plan:
+            info = plan.tune(BATCHED["tune_repeats"])
+            times = []
+            for _ in range(BATCHED["runs"]):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                plan.launch()
+                e1.record(stream)
+                plan.wait()
+                e1.synchronize()
+                times.append(e0.elapsed_time(e1))
+            ms = float(np.median(times))
+            res[prec] = {"mpix_iter_per_s": round(info["pixel_iterations"] / 1e6 / (ms / 1e3), 1),
+                         "ms_per_run": round(ms, 2), "mpix_iter_per_run": round(info["pixel_iterations"] / 1e6, 1),
+                         "schedule": {1: "per_pass", 2: "persistent"}[info["schedule"]],
+                         "ctas_per_sm": info["ctas_per_sm"], "launches_per_run": info["launches_per_run"],
+                         "tuned_ms": round(info["tuned_ms"], 2), "graph": bool(info["use_graph"]),
+                         "state_gb": round(info["state_bytes"] / 1e9, 2)}
+    res["f16acc_over_f32"] = round(res["f16acc"]["mpix_iter_per_s"] / res["f32"]["mpix_iter_per_s"], 3)
+    return res
 
 
 def run_serving(args, hp, device: int):

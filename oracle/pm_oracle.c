@@ -436,9 +436,15 @@ void orc_cost_rows_f32(const orc_view* v, const float* depth, const float* norma
 }
 
 void orc_cost_map_f64(const orc_view* v, const float* depth, const float* normal, int qw, double* cost) {
-    const int W = v->W, H = v->H;
+    orc_cost_rows_f64(v, depth, normal, qw, cost, 0, v->H);
+}
+
+/* Rows [y0, y1) of the FP64 cost map (the rest of `cost` is left as is). */
+void orc_cost_rows_f64(const orc_view* v, const float* depth, const float* normal, int qw, double* cost, int y0,
+                       int y1) {
+    const int W = v->W;
 #pragma omp parallel for schedule(dynamic, 4)
-    for (int y = 0; y < H; ++y)
+    for (int y = y0; y < y1; ++y)
         for (int x = 0; x < W; ++x) {
             size_t i = (size_t)y * W + x;
             cost[i] = orc_pixel_cost_f64(v, x, y, depth[i], normal[3 * i], normal[3 * i + 1], normal[3 * i + 2], qw);

@@ -79,6 +79,8 @@ void orc_cost_map_f32(const orc_view* v, const float* depth, const float* normal
 void orc_cost_rows_f32(const orc_view* v, const float* depth, const float* normal, float* cost, int y0, int y1);
 void orc_cost_map_f64(const orc_view* v, const float* depth, const float* normal, int quantized_weights,
                       double* cost);
+void orc_cost_rows_f64(const orc_view* v, const float* depth, const float* normal, int quantized_weights,
+                       double* cost, int y0, int y1);
 
 void orc_init(const orc_view* v, float dmin, float dmax, uint64_t seed, uint32_t view_id,
               float* depth, float* normal);

@@ -68,6 +68,7 @@ def lib():
                                                 C.c_double, C.c_int]),
             "orc_cost_map_f32": (None, [P(OrcView), fp, fp, fp]),
             "orc_cost_map_f64": (None, [P(OrcView), fp, fp, C.c_int, dp]),
+            "orc_cost_rows_f64": (None, [P(OrcView), fp, fp, C.c_int, dp, C.c_int, C.c_int]),
             "orc_cost_rows_f32": (None, [P(OrcView), fp, fp, fp, C.c_int, C.c_int]),
             "orc_propagate_rows": (None, [P(OrcView), fp, fp, fp, C.c_float, C.c_float, C.c_int, C.c_int, C.c_uint64,
                                           C.c_uint32, P(OrcRefine), C.c_int, C.c_int]),
@@ -147,6 +148,13 @@ class View:
         lib().orc_cost_map_f64(C.byref(self.c), _fp(depth), _fp(normal), int(quantized),
                                cost.ctypes.data_as(C.POINTER(C.c_double)))
         return cost
+
+    def cost_rows_f64(self, depth, normal, y0, y1, quantized=False):
+        """Rows [y0, y1) of the FP64 cost map, as a (y1 - y0, W) array."""
+        cost = np.zeros(depth.shape, np.float64)
+        lib().orc_cost_rows_f64(C.byref(self.c), _fp(depth), _fp(normal), int(quantized),
+                                cost.ctypes.data_as(C.POINTER(C.c_double)), y0, y1)
+        return cost[y0:y1]
 
     def cost_rows_f32(self, depth, normal, cost, y0, y1):
         lib().orc_cost_rows_f32(C.byref(self.c), _fp(depth), _fp(normal), _fp(cost), y0, y1)
