@@ -60,6 +60,7 @@ class Job(C.Structure):
         ("depth_min", C.c_float), ("depth_max", C.c_float),
         ("seed", C.c_uint64), ("view_id", C.c_uint32), ("iterations", C.c_int),
         ("use_coeffs", C.c_int), ("kinv", C.c_float * 9), ("ab", (C.c_float * 12) * MAX_SOURCES),
+        ("seeds", C.c_void_p), ("num_seeds", C.c_int), ("seed_radius", C.c_int),
     ]
 
 
@@ -93,6 +94,21 @@ class PlanInfo(C.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Seed(C.Structure):
+    _fields_ = [("x", C.c_int), ("y", C.c_int), ("depth", C.c_float), ("normal", C.c_float * 3)]
+
+
+class SparsePoints(C.Structure):
+    _fields_ = [("num_points", C.c_int), ("position", C.c_void_p), ("track_offset", C.c_void_p),
+                ("track_images", C.c_void_p)]
+
+
+class ViewSelection(C.Structure):
+    _fields_ = [("ref_image", C.c_int), ("num_sources", C.c_int), ("sources", C.c_int * MAX_SOURCES),
+                ("scores", C.c_float * MAX_SOURCES), ("baseline_deg", C.c_float * MAX_SOURCES),
+                ("depth_min", C.c_float), ("depth_max", C.c_float)]
 
 
 class ServerOptions(C.Structure):
@@ -161,6 +177,10 @@ def _load() -> C.CDLL:
         "hp_plan_destroy": (C.c_int, [C.c_void_p]),
         "hp_schedule_build": (C.c_int, [C.c_int, P(C.c_int), P(C.c_int), P(C.c_int), C.c_int, P(C.c_int),
                                         P(C.c_int), P(C.c_int), P(C.c_int)]),
+        "hp_select_sources": (C.c_int, [P(Camera), P(C.c_int), C.c_int, P(SparsePoints), C.c_int,
+                                        P(ViewSelection), P(C.c_int)]),
+        "hp_project_seeds": (C.c_int, [P(Camera), C.c_int, C.c_float, C.c_float, P(SparsePoints), P(Seed),
+                                       C.c_int, P(C.c_int)]),
         "hp_server_options_default": (None, [P(ServerOptions)]),
         "hp_server_create": (C.c_int, [C.c_void_p, P(Params), P(ServerOptions), P(C.c_void_p)]),
         "hp_submit": (C.c_int, [C.c_void_p, P(Job), P(Maps), P(C.c_uint64)]),
@@ -194,7 +214,7 @@ EXPORTS = (
     "hp_plan_options_default", "hp_plan_create", "hp_plan_run", "hp_plan_launch", "hp_plan_wait", "hp_plan_tune",
     "hp_plan_get_info", "hp_plan_destroy", "hp_schedule_build", "hp_server_options_default", "hp_server_create",
     "hp_submit", "hp_poll", "hp_server_drain", "hp_server_stats_get", "hp_server_stats_reset",
-    "hp_server_last_error", "hp_server_destroy", "hp_server_simulate",
+    "hp_server_last_error", "hp_server_destroy", "hp_server_simulate", "hp_select_sources", "hp_project_seeds",
 )
 STATIC_MAX_PIXELS = 1280 * 1024  # HP_STATIC_MAX_PIXELS
 
@@ -541,6 +561,64 @@ def server_simulate(arrive_step: Sequence[int], state_bytes: Sequence[int], stag
     return np.array(adm[:n]), np.array(fin[:n]), steps.value
 
 
+class SfmPoints:
+    """Sparse points and their tracks (hp_sparse_points) over numpy arrays kept alive here.
+    ``positions``: (P, 3) float64 world points; ``tracks``: one sequence of camera indices per point."""
+
+    def __init__(self, positions, tracks):
+        self.positions = np.ascontiguousarray(np.asarray(positions, np.float64).reshape(-1, 3))
+        self.offsets = np.zeros(len(tracks) + 1, np.int32)
+        self.offsets[1:] = np.cumsum([len(t) for t in tracks]) if len(tracks) else []
+        flat = [int(c) for t in tracks for c in t]
+        self.images = np.ascontiguousarray(np.asarray(flat if flat else [0], np.int32))
+        self.c = SparsePoints(len(tracks), self.positions.ctypes.data, self.offsets.ctypes.data,
+                              self.images.ctypes.data)
+
+
+def select_sources(cameras: Sequence[Camera], points: SfmPoints, num_sources: int, registered=None) -> List[dict]:
+    """hp_select_sources (selectSourceViews, patchmatch_mvs.cu:74-157): per registered camera its sources
+    (best first), their scores and baseline angles, and the depth range."""
+    n = len(cameras)
+    cams = (Camera * n)(*cameras)
+    reg = (C.c_int * n)(*([1] * n if registered is None else [int(bool(r)) for r in registered]))
+    out = (ViewSelection * n)()
+    cnt = C.c_int()
+    st = lib.hp_select_sources(cams, reg, n, C.byref(points.c), int(num_sources), out, C.byref(cnt))
+    if st != OK:
+        raise HpError(st, "hp_select_sources")
+    res = []
+    for v in out[:cnt.value]:
+        k = v.num_sources
+        res.append({"ref": v.ref_image, "sources": list(v.sources[:k]), "scores": list(v.scores[:k]),
+                    "baseline_deg": list(v.baseline_deg[:k]), "depth_min": v.depth_min, "depth_max": v.depth_max})
+    return res
+
+
+def project_seeds(camera: Camera, ref: int, depth_min: float, depth_max: float, points: SfmPoints):
+    """hp_project_seeds: the SfM seeds of reference camera ``ref`` as a ctypes Seed array (point order)."""
+    n = C.c_int()
+    st = lib.hp_project_seeds(C.byref(camera), int(ref), float(depth_min), float(depth_max), C.byref(points.c),
+                              None, 0, C.byref(n))
+    if st != OK:
+        raise HpError(st, "hp_project_seeds")
+    arr = (Seed * max(1, n.value))()
+    st = lib.hp_project_seeds(C.byref(camera), int(ref), float(depth_min), float(depth_max), C.byref(points.c),
+                              arr, n.value, C.byref(n))
+    if st != OK:
+        raise HpError(st, "hp_project_seeds")
+    arr.count = n.value
+    return arr
+
+
+def with_seeds(job: Job, seeds, radius: int = 50) -> Job:
+    """Attach seeds (from project_seeds) to a job; the job keeps the array alive."""
+    job.seeds = C.cast(seeds, C.c_void_p).value if seeds is not None and seeds.count else None
+    job.num_seeds = seeds.count if seeds is not None else 0
+    job.seed_radius = int(radius)
+    job._seeds = seeds
+    return job
+
+
 def make_job(ref_image: int, src_images: Sequence[int], ref_cam: Camera, src_cams: Sequence[Camera],
              depth_min: float, depth_max: float, seed: int = 42, view_id: int = 0, iterations: int = 12,
              coeffs=None) -> Job:
@@ -647,12 +725,20 @@ class MVSConfig:
     save_intermediate: bool = False
     output_dir: Optional[str] = None
     device: int = 0
+    sfm_seeding: bool = True   # paint the SfM points' depths over the random init (:1111-1177)
+    seed_radius: int = 50      # SEED_RADIUS (:1123)
 
 
-def run_patchmatch_mvs(images: Sequence[np.ndarray], cameras: Sequence[Camera], views: Sequence[ViewParams],
-                       config: MVSConfig = MVSConfig(), ctx: Optional[Context] = None) -> List[DepthMap]:
-    """runPatchMatchMVS (patchmatch_mvs.cu:1028-1388) with explicit view parameters.
+def run_patchmatch_mvs(images: Sequence[np.ndarray], cameras: Sequence[Camera],
+                       views: Optional[Sequence[ViewParams]] = None, config: MVSConfig = MVSConfig(),
+                       ctx: Optional[Context] = None, sfm: Optional[SfmPoints] = None,
+                       registered: Optional[Sequence[bool]] = None) -> List[DepthMap]:
+    """runPatchMatchMVS (patchmatch_mvs.cu:1028-1388).
 
+    With ``sfm`` (the sparse points and their tracks) and no ``views``, the views come from
+    :func:`select_sources` with min(8, max(3, registered - 1)) sources (:1037-1039), and with
+    ``config.sfm_seeding`` every view's hypotheses are seeded from the points it sees
+    (:1111-1177).  Explicit ``views`` override the selection.
     Views without sources are skipped (:1089-1092); the per-view seed is
     42 + 1e6 * ref_id (:1106); radius = (patch_size - 1) / 2 clamped to 1..7;
     confidence = 1 - cost / 2 (:1246-1252); with iterations > 0 and >= 2 maps the
@@ -664,6 +750,13 @@ def run_patchmatch_mvs(images: Sequence[np.ndarray], cameras: Sequence[Camera], 
     try:
         radius = min(MAX_RADIUS, max(1, (config.mvs_patch_size - 1) // 2))
         params = default_params(radius=radius, stride=config.window_stride, precision=config.precision)
+        if views is None:
+            if sfm is None:
+                raise ValueError("run_patchmatch_mvs needs views or sfm points")
+            reg = [True] * len(cameras) if registered is None else list(registered)
+            ns = min(MAX_SOURCES, max(3, sum(bool(r) for r in reg) - 1))
+            views = [ViewParams(v["ref"], v["sources"], v["depth_min"], v["depth_max"])
+                     for v in select_sources(cameras, sfm, ns, reg)]
         ids = {}
         views = [v for v in views if v.source_ids]
         for v in views:
@@ -674,10 +767,14 @@ def run_patchmatch_mvs(images: Sequence[np.ndarray], cameras: Sequence[Camera], 
         for v in views:
             h, w = images[v.ref_image_id].shape[:2]
             m, d, n, c = host_maps(h, w)
-            jobs.append(make_job(ids[v.ref_image_id], [ids[s] for s in v.source_ids], cameras[v.ref_image_id],
-                                 [cameras[s] for s in v.source_ids], v.depth_min, v.depth_max,
-                                 seed=42 + 1_000_000 * v.ref_image_id, view_id=v.ref_image_id,
-                                 iterations=config.mvs_iterations))
+            job = make_job(ids[v.ref_image_id], [ids[s] for s in v.source_ids], cameras[v.ref_image_id],
+                           [cameras[s] for s in v.source_ids], v.depth_min, v.depth_max,
+                           seed=42 + 1_000_000 * v.ref_image_id, view_id=v.ref_image_id,
+                           iterations=config.mvs_iterations)
+            if sfm is not None and config.sfm_seeding:
+                with_seeds(job, project_seeds(cameras[v.ref_image_id], v.ref_image_id, v.depth_min, v.depth_max,
+                                              sfm), config.seed_radius)
+            jobs.append(job)
             outs.append(m)
             maps.append((d, n, c))
         if jobs:

@@ -206,6 +206,36 @@ hp_status prepare(hp_ctx* ctx, const hp_job* jobs, int n, Prepared* P) {
     return HP_OK;
 }
 
+// Seed fields of a job: none, or a host list with a sane radius.
+hp_status check_seeds(hp_ctx* ctx, const hp_job* j, int jobno) {
+    if (j->num_seeds == 0) return HP_OK;
+    if (j->num_seeds < 0 || j->num_seeds > (1 << 26) || !j->seeds || j->seed_radius < 0 || j->seed_radius > 4096)
+        return fail(ctx, HP_ERR_INVALID_ARG, "job %d: seeds (%d, radius %d) invalid", jobno, j->num_seeds,
+                    j->seed_radius);
+    return HP_OK;
+}
+
+// Paint every job's SfM seeds over its freshly initialised hypotheses
+// (runPatchMatchMVS, patchmatch_mvs.cu:1111-1177), one job at a time.
+hp_status apply_seeds(hp_ctx* ctx, const hp_job* jobs, int n, const Prepared& P) {
+    for (int k = 0; k < n; ++k) {
+        const hp_job& j = jobs[k];
+        if (j.num_seeds <= 0) continue;
+        const hp::ViewDesc& v = P.host[k];
+        const size_t seed_bytes = (static_cast<size_t>(j.num_seeds) * sizeof(hp_seed) + 255) & ~size_t(255);
+        HP_CUDA(ctx->seedbuf.ensure(seed_bytes + static_cast<size_t>(v.W) * v.H * sizeof(int)));
+        hp_seed* d_seeds = static_cast<hp_seed*>(ctx->seedbuf.p);
+        int* d_map = reinterpret_cast<int*>(static_cast<char*>(ctx->seedbuf.p) + seed_bytes);
+        // Pageable source: the copy is complete when the call returns, before the next job reuses the buffer.
+        HP_CUDA(cudaMemcpyAsync(d_seeds, j.seeds, static_cast<size_t>(j.num_seeds) * sizeof(hp_seed),
+                                cudaMemcpyHostToDevice, ctx->stream));
+        HP_CUDA(counted(ctx, HP_KERNEL_OTHER,
+                        [&] { return hp::launch_seed(v, d_seeds, j.num_seeds, j.seed_radius, d_map, ctx->stream); }));
+        HP_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+    return HP_OK;
+}
+
 hp::BatchList batch_of(const Prepared& P, int list) {
     hp::BatchList bl;
     bl.views = P.dev;
@@ -382,6 +412,7 @@ hp_status hp_ctx_destroy(hp_ctx* ctx) {
         ctx->descs.release();
         ctx->lists.release();
         ctx->staging.release();
+        ctx->seedbuf.release();
         for (cudaEvent_t e : ctx->events) cudaEventDestroy(e);
         cudaStreamDestroy(ctx->stream);
     }
@@ -555,14 +586,17 @@ hp_status hp_solve(hp_ctx* ctx, const hp_job* jobs, int num_jobs, const hp_param
     if (!jobs || !out || num_jobs < 1) return fail(ctx, HP_ERR_INVALID_ARG, "solve: no jobs or outputs");
     hp_status st = check_params(ctx, params);
     if (st != HP_OK) return st;
-    for (int k = 0; k < num_jobs; ++k)
+    for (int k = 0; k < num_jobs; ++k) {
         if (!out[k].depth || !out[k].normal || !out[k].cost)
             return fail(ctx, HP_ERR_INVALID_ARG, "solve: output maps of job %d incomplete", k);
+        if ((st = check_seeds(ctx, &jobs[k], k)) != HP_OK) return st;
+    }
     DeviceGuard g(ctx->device);
     Prepared P;
     if ((st = prepare(ctx, jobs, num_jobs, &P)) != HP_OK) return st;
     hp::BatchList all = batch_of(P, 0);
     HP_CUDA(counted(ctx, HP_KERNEL_INIT, [&] { return hp::launch_init(all, ctx->stream); }));
+    if ((st = apply_seeds(ctx, jobs, num_jobs, P)) != HP_OK) return st;
     if ((st = launch_cost(ctx, all, params)) != HP_OK) return st;
     for (int it = 0; it < P.max_iter; ++it) {
         hp::BatchList bl = batch_of(P, 1 + it);
@@ -581,10 +615,12 @@ hp_status hp_init_hypotheses(hp_ctx* ctx, const hp_job* job, const hp_params* pa
     if (!job || !out || !out->depth || !out->normal) return fail(ctx, HP_ERR_INVALID_ARG, "init: null argument");
     hp_status st = check_params(ctx, params);
     if (st != HP_OK) return st;
+    if ((st = check_seeds(ctx, job, 0)) != HP_OK) return st;
     DeviceGuard g(ctx->device);
     Prepared P;
     if ((st = prepare(ctx, job, 1, &P)) != HP_OK) return st;
     HP_CUDA(counted(ctx, HP_KERNEL_INIT, [&] { return hp::launch_init(batch_of(P, 0), ctx->stream); }));
+    if ((st = apply_seeds(ctx, job, 1, P)) != HP_OK) return st;
     if ((st = export_maps(ctx, P, 0, out, true, false)) != HP_OK) return st;
     HP_CUDA(cudaStreamSynchronize(ctx->stream));
     flush_profile(ctx);

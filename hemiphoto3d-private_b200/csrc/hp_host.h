@@ -63,6 +63,7 @@ struct hp_ctx {
     hpx::DevBuf descs;   // ViewDesc array
     hpx::DevBuf lists;   // active-view lists and tile prefixes
     hpx::DevBuf staging; // host-memory results pass through here
+    hpx::DevBuf seedbuf; // SfM seeds of one job and their W*H index map
     // Profiler: launch counts always; with profiling on, CUDA events bracket
     // each launch and are read back at the next synchronisation point.
     bool profiling = false;

@@ -131,6 +131,10 @@ cudaError_t launch_propagate_f16(const BatchList& bl, const SolveConsts& sc, int
 // FP16 plane -> software-sampler quad plane (see hpx::Image::quad16).
 cudaError_t launch_quads(const __half* src16, int pitch16, int W, int H, uint2* quads, int quad_pitch,
                          cudaStream_t st);
+// SfM seeds (host list uploaded to `seeds`) painted over the view's hypotheses; `map` is
+// W*H ints of scratch.
+cudaError_t launch_seed(const ViewDesc& v, const hp_seed* seeds, int num_seeds, int radius, int* map,
+                        cudaStream_t st);
 cudaError_t launch_unpack(const ViewDesc* views_host_copy, int view, float* depth, float* normal, float* cost,
                           cudaStream_t st);
 cudaError_t launch_pack(const ViewDesc* views_host_copy, int view, const float* depth, const float* normal,

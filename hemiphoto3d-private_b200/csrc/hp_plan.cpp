@@ -321,6 +321,8 @@ hp_status hp_plan_create(hp_ctx* ctx, const hp_job* jobs, int num_jobs, const hp
     p->host.resize(num_jobs);
     p->out.assign(out, out + num_jobs);
     for (int k = 0; k < num_jobs; ++k) {
+        if (jobs[k].num_seeds != 0)
+            return fail(ctx, HP_ERR_UNSUPPORTED, "plan_create: job %d carries SfM seeds (use hp_solve)", k);
         if ((st = fill_desc(ctx, &jobs[k], k, &p->host[k])) != HP_OK) return st;
         p->iters.push_back(jobs[k].iterations);
         p->max_iter = std::max(p->max_iter, jobs[k].iterations);

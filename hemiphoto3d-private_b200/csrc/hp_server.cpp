@@ -625,6 +625,7 @@ hp_status hp_submit(hp_server* s, const hp_job* job, const hp_maps* out, uint64_
     };
     if (!job || !out || !request_id) return bad(HP_ERR_INVALID_ARG, "submit: null argument");
     if (!out->depth || !out->normal || !out->cost) return bad(HP_ERR_INVALID_ARG, "submit: output maps incomplete");
+    if (job->num_seeds != 0) return bad(HP_ERR_UNSUPPORTED, "submit: jobs with SfM seeds go through hp_solve");
     if (out->memory != HP_MEMORY_HOST && out->memory != HP_MEMORY_DEVICE)
         return bad(HP_ERR_INVALID_ARG, "submit: unknown memory kind");
     std::unique_ptr<SrvReq> r(new SrvReq);

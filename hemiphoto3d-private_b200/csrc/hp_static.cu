@@ -74,6 +74,7 @@ extern "C" hp_status hp_solve_static(int device, void* stream, const hp_job* job
     if (params->radius < 1 || params->radius > HP_MAX_RADIUS || (params->stride != 1 && params->stride != 2) ||
         params->top_k < 1 || params->top_k > HP_MAX_TOP_K || params->refine_steps < 0 || params->refine_steps > 4)
         return HP_ERR_INVALID_ARG;
+    if (job->num_seeds != 0) return HP_ERR_UNSUPPORTED;  // the seed index map would need scratch
     if (job->num_sources < 1 || job->num_sources > HP_MAX_SOURCES || !(job->depth_min > 0.f) ||
         !(job->depth_max > job->depth_min) || job->iterations < 0 || job->iterations > 1000)
         return HP_ERR_INVALID_ARG;

@@ -298,3 +298,37 @@ def depth_metrics(depth: np.ndarray, gt: np.ndarray, rel_tol: float = 0.01, mask
     comp = good.sum() / max(1, valid.sum())
     mean_err = float(rel[kept].mean()) if kept.any() else float("nan")
     return float(comp), float(kept.sum() / max(1, valid.sum())), mean_err
+
+
+def sparse_points(scene: Scene, n: int = 2000, seed: int = 0, rel_tol: float = 0.02):
+    """A stand-in for an SfM sparse reconstruction of a rendered scene: `n` surface points back-projected
+    from random ground-truth pixels of random views, each with the track of views that see it (projection
+    inside the image and ground-truth depth within rel_tol of the point's depth).  Points seen by fewer than
+    two views are dropped.  Returns (positions (P, 3) float64, tracks list of camera-index lists)."""
+    rng = np.random.default_rng(seed)
+    H, W = scene.height, scene.width
+    pts, tracks = [], []
+    for _ in range(n):
+        v = scene.views[int(rng.integers(0, len(scene.views)))]
+        y, x = int(rng.integers(0, H)), int(rng.integers(0, W))
+        d = float(v.depth_gt[y, x])
+        if d <= 0:
+            continue
+        pc = np.linalg.solve(v.cam.K, np.array([x + 0.5, y + 0.5, 1.0])) * d
+        pw = v.cam.R.T @ (pc - v.cam.t)
+        tr = []
+        for j, w in enumerate(scene.views):
+            q = w.cam.R @ pw + w.cam.t
+            if q[2] <= 0:
+                continue
+            u = w.cam.K @ q
+            ux, uy = u[0] / u[2], u[1] / u[2]
+            if not (0 <= ux < W and 0 <= uy < H):
+                continue
+            g = float(w.depth_gt[int(uy), int(ux)])
+            if g > 0 and abs(g - q[2]) <= rel_tol * q[2]:
+                tr.append(j)
+        if len(tr) >= 2:
+            pts.append(pw)
+            tracks.append(tr)
+    return np.array(pts, np.float64).reshape(-1, 3), tracks

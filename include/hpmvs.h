@@ -99,6 +99,13 @@ typedef struct hp_params {
     int soft_sources;
 } hp_params;
 
+/* One SfM seed in a reference view: pixel, depth and camera-frame normal. */
+typedef struct hp_seed {
+    int x, y;
+    float depth;
+    float normal[3];
+} hp_seed;
+
 /* One reference view to solve. */
 typedef struct hp_job {
     int ref_image;                     /* id from hp_image_upload */
@@ -118,6 +125,16 @@ typedef struct hp_job {
     int use_coeffs;
     float kinv[9];
     float ab[HP_MAX_SOURCES][12];
+    /* SfM-seeded initialisation (runPatchMatchMVS, patchmatch_mvs.cu:1111-1177):
+     * after the random initialisation every pixel within seed_radius (per axis)
+     * of a seed's pixel takes that seed's depth and normal; where squares
+     * overlap, the seed listed last wins.  Host memory, num_seeds records, as
+     * hp_project_seeds makes them; NULL / 0 for none.  The reference's radius
+     * is 50.  hp_solve and hp_init_hypotheses apply seeds; plans and the
+     * server refuse jobs that carry them (HP_ERR_UNSUPPORTED). */
+    const hp_seed* seeds;
+    int num_seeds;
+    int seed_radius;
 } hp_job;
 
 /* Per-view maps, caller-owned. */
@@ -400,6 +417,53 @@ hp_status hp_server_destroy(hp_server* s);
 hp_status hp_server_simulate(int n, const int* arrive_step, const uint64_t* state_bytes, const int* stages,
                              int max_active, uint64_t budget, int passes_per_step, int* admit_step,
                              int* finish_step, int* steps);
+
+/* ---------------------------------------------------------------------------
+ * SfM front of the stage: what runPatchMatchMVS derives from the sparse
+ * reconstruction before solving.
+ * ------------------------------------------------------------------------- */
+/* Sparse points with their tracks: point p is seen by cameras
+ * track_images[track_offset[p] .. track_offset[p + 1]) (SparsePoint,
+ * include/types.h:76-83). */
+typedef struct hp_sparse_points {
+    int num_points;
+    const double* position;      /* 3 per point, world frame */
+    const int* track_offset;     /* num_points + 1 */
+    const int* track_images;     /* camera indices */
+} hp_sparse_points;
+
+/* Sources and depth range of one reference view (MVSViewParams, patchmatch_mvs.h:16-28). */
+typedef struct hp_view_selection {
+    int ref_image;                       /* camera index */
+    int num_sources;
+    int sources[HP_MAX_SOURCES];         /* camera indices, best first */
+    float scores[HP_MAX_SOURCES];        /* shared points * baseline score */
+    float baseline_deg[HP_MAX_SOURCES];
+    float depth_min, depth_max;
+} hp_view_selection;
+
+/* Replaces selectSourceViews (patchmatch_mvs.cu:74-157).  For every
+ * registered camera, in index order: the other registered cameras whose
+ * baseline angle at the points' centroid lies in [5, 90] degrees and that
+ * share points with it, scored shared * sin(clamp(angle, 5, 30)) and sorted
+ * best first (equal scores: lower camera index first; the reference's sort
+ * leaves their order unspecified), at most num_sources (1..HP_MAX_SOURCES).
+ * Depth range: the 5th and 95th percentile of the camera-frame depths of the
+ * points it sees, x0.5 and x1.5 (fewer than two: the centroid depth x0.3 and
+ * x3).  Shared counts come from one pass over the tracks.  out needs one entry
+ * per registered camera; *num_out receives the count. */
+hp_status hp_select_sources(const hp_camera* cams, const int* registered, int num_cams,
+                            const hp_sparse_points* points, int num_sources, hp_view_selection* out,
+                            int* num_out);
+
+/* The seeds of reference camera `ref` (patchmatch_mvs.cu:1122-1160): every
+ * point whose track contains `ref` and whose camera-frame depth is positive
+ * and inside [depth_min, depth_max], at the rounded pixel of its projection,
+ * with the unit normal towards the camera centre in the camera frame, in
+ * point order.  FP64 throughout, as the reference.  Returns up to capacity
+ * seeds; *num_seeds receives how many there are. */
+hp_status hp_project_seeds(const hp_camera* cam, int ref, float depth_min, float depth_max,
+                           const hp_sparse_points* points, hp_seed* out, int capacity, int* num_seeds);
 
 /* Replaces saveDepthMapPFM / loadDepthMapPFM (patchmatch_mvs.cu:990-1022):
  * 'Pf' (channels 1) or 'PF' (channels 3) little-endian PFM, rows bottom-up. */

@@ -11,9 +11,10 @@
 // 1..7 instead of the reference's 1..5), per-view seed 42 + 1e6 * ref_id,
 // confidence 1 - cost / 2, then the in-place geometric filter (tolerance 0.12,
 // normal check off, 2 agreeing views) when iterations > 0 and >= 2 maps, PFM
-// depth per view when save_intermediate.  Not done: the SfM-point seeding of
-// the initial hypotheses (:1111-1177).  Errors are reported by return value
-// (an empty vector and `*status`), never by exit().
+// depth per view when save_intermediate.  The initial hypotheses are seeded
+// from the SfM points each view sees (:1111-1177, radius 50) through
+// hp_project_seeds.  Errors are reported by return value (an empty vector and
+// `*status`), never by exit().
 #pragma once
 
 #include <algorithm>
@@ -61,6 +62,22 @@ inline std::vector<DepthMap> runPatchMatchMVS(const std::vector<ImageData>& imag
     hp_params_default(&params);
     params.radius = std::min(HP_MAX_RADIUS, std::max(1, (config.mvs_patch_size - 1) / 2));
 
+    // The sparse points and their tracks, flattened once for hp_project_seeds.
+    std::vector<double> pos;
+    std::vector<int> toff(1, 0), timg;
+    for (const SparsePoint& p : sfm.points) {
+        for (int i = 0; i < 3; ++i) pos.push_back(p.position(i));
+        for (int id : p.image_ids) timg.push_back(id);
+        toff.push_back(static_cast<int>(timg.size()));
+    }
+    hp_sparse_points pts;
+    pts.num_points = static_cast<int>(sfm.points.size());
+    pts.position = pos.data();
+    pts.track_offset = toff.data();
+    pts.track_images = timg.data();
+    std::vector<std::vector<hp_seed>> seeds;
+    seeds.reserve(views.size());
+
     std::vector<hp_job> jobs;
     std::vector<const MVSViewParams*> solved;
     for (const MVSViewParams& vp : views) {
@@ -83,6 +100,19 @@ inline std::vector<DepthMap> runPatchMatchMVS(const std::vector<ImageData>& imag
         j.seed = 42ull + static_cast<uint64_t>(vp.ref_image_id) * 1000000ull;  // :1106
         j.view_id = static_cast<uint32_t>(vp.ref_image_id);
         j.iterations = config.mvs_iterations;
+        // SfM seeding (:1111-1177): the points this view sees, painted over the random init.
+        const hp_camera seed_cam = to_hp_camera(cameras[vp.ref_image_id]);
+        int n_seeds = 0;
+        st = hp_project_seeds(&seed_cam, vp.ref_image_id, vp.depth_min, vp.depth_max, &pts, nullptr, 0, &n_seeds);
+        if (st != HP_OK) break;
+        seeds.emplace_back(static_cast<size_t>(n_seeds));
+        if (n_seeds > 0 &&
+            (st = hp_project_seeds(&seed_cam, vp.ref_image_id, vp.depth_min, vp.depth_max, &pts,
+                                   seeds.back().data(), n_seeds, &n_seeds)) != HP_OK)
+            break;
+        j.seeds = seeds.back().data();
+        j.num_seeds = n_seeds;
+        j.seed_radius = 50;  // SEED_RADIUS, :1123
         jobs.push_back(j);
         solved.push_back(&vp);
     }

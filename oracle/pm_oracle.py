@@ -8,6 +8,7 @@ it, always as the checker or the timed CPU baseline, never as the engine.
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 import subprocess
 from typing import Sequence
@@ -233,3 +234,131 @@ def num_threads() -> int:
 
 def set_num_threads(n: int):
     lib().orc_set_num_threads(n)
+
+
+# ---------------------------------------------------------------------------------------------
+# SfM front of the stage (patchmatch_mvs.cu:40-157, :1111-1177), restated in FP64 numpy scalars.
+# Small cases only (pure Python loops).  Cameras are (K, R, t) tuples; tracks hold camera indices.
+# ---------------------------------------------------------------------------------------------
+
+_LIBM = None
+
+
+def _sinf(x):
+    """The C library's single-precision sine (the reference calls std::sin on a float)."""
+    global _LIBM
+    if _LIBM is None:
+        _LIBM = C.CDLL("libm.so.6")
+        _LIBM.sinf.restype, _LIBM.sinf.argtypes = C.c_float, [C.c_float]
+    return np.float32(_LIBM.sinf(float(x)))
+
+
+def _cam_centre(R, t):
+    """-R^T t, summed left to right (CameraPose::cam_center, include/types.h:71-73)."""
+    return np.array([(-R[0, i] * t[0] + -R[1, i] * t[1]) + -R[2, i] * t[2] for i in range(3)])
+
+
+def _mv(M, v):
+    return np.array([(M[i, 0] * v[0] + M[i, 1] * v[1]) + M[i, 2] * v[2] for i in range(3)])
+
+
+def _unit(v):
+    n = math.sqrt((v[0] * v[0] + v[1] * v[1]) + v[2] * v[2])
+    return v / n if n > 0 else v
+
+
+def sfm_select_sources(cams, registered, positions, tracks, num_sources):
+    """selectSourceViews (patchmatch_mvs.cu:74-157): per registered camera, sources scored by shared points x
+    sin(clamped baseline angle at the centroid), best first (ties: lower index), and the 5/95-percentile depth
+    range x0.5 / x1.5 (centroid depth x0.3 / x3 with fewer than two points)."""
+    pos = [np.asarray(p, np.float64) for p in positions]
+    cen = np.zeros(3)
+    for p in pos:
+        cen = cen + p
+    if pos:
+        cen = cen / float(len(pos))
+    sets = [set(t) for t in tracks]
+    out = []
+    for ref, (K, R, t) in enumerate(cams):
+        if not registered[ref]:
+            continue
+        R, t = np.asarray(R, np.float64), np.asarray(t, np.float64)
+        cand = []
+        for src, (Ks, Rs, ts) in enumerate(cams):
+            if src == ref or not registered[src]:
+                continue
+            vi = _unit(cen - _cam_centre(R, t))
+            vj = _unit(cen - _cam_centre(np.asarray(Rs, np.float64), np.asarray(ts, np.float64)))
+            c = min(1.0, max(-1.0, (vi[0] * vj[0] + vi[1] * vj[1]) + vi[2] * vj[2]))
+            ang = np.float32(math.acos(c) * 180.0 / math.pi)
+            if ang < np.float32(5.0) or ang > np.float32(90.0):
+                continue
+            cl = min(max(ang, np.float32(5.0)), np.float32(30.0))
+            b = _sinf(np.float32(cl * np.float32(math.pi) / np.float32(180.0)))
+            shared = sum(1 for s in sets if ref in s and src in s)
+            if shared == 0:
+                continue
+            cand.append((-(np.float32(shared) * b), src, np.float32(shared) * b, ang))
+        cand.sort(key=lambda c: (c[0], c[1]))
+        cand = cand[:num_sources]
+        depths = []
+        for p, s in zip(pos, sets):
+            if ref in s:
+                z = _mv(R, p)[2] + t[2]
+                if z > 0:
+                    depths.append(np.float32(z))
+        if len(depths) >= 2:
+            depths.sort()
+            i5 = int(len(depths) * 0.05)
+            i95 = min(int(len(depths) * 0.95), len(depths) - 1)
+            dmin, dmax = depths[i5] * np.float32(0.5), depths[i95] * np.float32(1.5)
+        else:
+            d = np.float32(_mv(R, cen)[2] + t[2])
+            dmin, dmax = d * np.float32(0.3), d * np.float32(3.0)
+        out.append({"ref": ref, "sources": [c[1] for c in cand], "scores": [float(c[2]) for c in cand],
+                    "baseline_deg": [float(c[3]) for c in cand], "depth_min": float(dmin), "depth_max": float(dmax)})
+    return out
+
+
+def sfm_project_seeds(cam, ref, depth_min, depth_max, positions, tracks):
+    """The seeds of camera `ref` (patchmatch_mvs.cu:1122-1160): (x, y, depth, nx, ny, nz) per point it sees
+    with positive depth inside [depth_min, depth_max], in point order."""
+    K, R, t = (np.asarray(a, np.float64) for a in cam)
+    c = _cam_centre(R, t)
+    seeds = []
+    for p, tr in zip(positions, tracks):
+        if ref not in tr:
+            continue
+        p = np.asarray(p, np.float64)
+        pc = _mv(R, p) + t
+        if pc[2] <= 0:
+            continue
+        px = _mv(K, pc)
+        x, y = _round_half_away(px[0] / px[2]), _round_half_away(px[1] / px[2])
+        d = np.float32(pc[2])
+        if d < np.float32(depth_min) or d > np.float32(depth_max):
+            continue
+        n = _mv(R, _unit(c - p))
+        seeds.append((int(x), int(y), float(d), float(np.float32(n[0])), float(np.float32(n[1])),
+                      float(np.float32(n[2]))))
+    return seeds
+
+
+def _round_half_away(v):
+    """std::round: nearest integer, halves away from zero (v - floor(v) is exact here)."""
+    a = abs(v)
+    r = math.floor(a)
+    r = r + 1 if a - r >= 0.5 else r
+    return r if v >= 0 else -r
+
+
+def paint_seeds(depth, normal, seeds, radius):
+    """Overwrite the (2r+1)^2 square around each seed's pixel with its depth and normal, in list order."""
+    H, W = depth.shape
+    for x, y, d, nx, ny, nz in seeds:
+        x0, x1 = max(0, x - radius), min(W - 1, x + radius)
+        y0, y1 = max(0, y - radius), min(H - 1, y + radius)
+        if x0 > x1 or y0 > y1:
+            continue
+        depth[y0:y1 + 1, x0:x1 + 1] = d
+        normal[y0:y1 + 1, x0:x1 + 1] = (nx, ny, nz)

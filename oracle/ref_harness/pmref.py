@@ -37,8 +37,10 @@ def lib():
         L.pmref_solve_view.argtypes = [fp, C.c_void_p, ip, ip, ip, fp, fp, C.c_float, C.c_float, ip, ip, ip, fp, fp,
                                        fp, C.POINTER(C.c_float)]
         L.pmref_geometric_filter.argtypes = [fp, fp, fp, dp, fp, fp, dp, ip, ip, ip, C.c_float, C.c_float, ip]
+        L.pmref_select_sources.argtypes = [dp, fp, ip, dp, fp, fp, ip, ip] + [fp] * 8
+        L.pmref_run_stage.argtypes = [C.c_void_p, ip, ip, dp, fp, ip, dp, fp, fp, ip, ip, fp, fp, fp, fp]
         for f in ("pmref_setup_views", "pmref_ncc_cost", "pmref_pixel_cost", "pmref_init", "pmref_propagate",
-                  "pmref_solve_view", "pmref_geometric_filter"):
+                  "pmref_solve_view", "pmref_geometric_filter", "pmref_select_sources", "pmref_run_stage"):
             getattr(L, f).restype = C.c_int
         _lib = L
     return _lib
@@ -115,3 +117,51 @@ def geometric_filter(ref_cam, depth, normal, conf, src_cams, src_depths, src_nor
     assert lib().pmref_geometric_filter(_p(depth), _p(np.ascontiguousarray(normal, np.float32)), _p(conf), _p(r),
                                         _p(sd), _p(sn), _p(s), S, w, h, depth_tol, normal_tol_cos,
                                         min_consistent) == 0
+
+
+def _sfm_arrays(cams, registered, positions, tracks):
+    krt = np.ascontiguousarray(np.concatenate([_krt(c) for c in cams]))
+    reg = np.ascontiguousarray(np.asarray(registered, np.int32))
+    pos = np.ascontiguousarray(np.asarray(positions, np.float64).reshape(-1, 3))
+    toff = np.zeros(len(tracks) + 1, np.int32)
+    toff[1:] = np.cumsum([len(t) for t in tracks]) if len(tracks) else []
+    timg = np.ascontiguousarray(np.asarray([c for t in tracks for c in t] or [0], np.int32))
+    return krt, reg, pos, toff, timg
+
+
+def select_sources(cams, registered, positions, tracks, num_sources):
+    """The reference's selectSourceViews (host code; no GPU needed).  cams: (K, R, t) per camera."""
+    krt, reg, pos, toff, timg = _sfm_arrays(cams, registered, positions, tracks)
+    n = len(cams)
+    ref, cnt = np.zeros(n, np.int32), np.zeros(n, np.int32)
+    src = np.zeros(8 * n, np.int32)
+    score, ang = np.zeros(8 * n, np.float32), np.zeros(8 * n, np.float32)
+    dmin, dmax = np.zeros(n, np.float32), np.zeros(n, np.float32)
+    n_out = np.zeros(1, np.int32)
+    rc = lib().pmref_select_sources(_p(krt), _p(reg), n, _p(pos), _p(toff), _p(timg), len(tracks), num_sources,
+                                    _p(ref), _p(cnt), _p(src), _p(score), _p(ang), _p(dmin), _p(dmax), _p(n_out))
+    assert rc == 0
+    out = []
+    for i in range(int(n_out[0])):
+        k = int(cnt[i])
+        out.append({"ref": int(ref[i]), "sources": src[8 * i:8 * i + k].tolist(), "scores": score[8 * i:8 * i + k].tolist(),
+                    "baseline_deg": ang[8 * i:8 * i + k].tolist(), "depth_min": float(dmin[i]),
+                    "depth_max": float(dmax[i])})
+    return out
+
+
+def run_stage(grays: Sequence[np.ndarray], cams, positions, tracks, patch_size=11):
+    """The reference's runPatchMatchMVS with 0 iterations (init + SfM seeding): {image id: (depth, normal)}."""
+    H, W = grays[0].shape
+    g = [np.ascontiguousarray(x, np.float32) for x in grays]
+    ptrs = (C.c_void_p * len(g))(*[x.ctypes.data for x in g])
+    krt, reg, pos, toff, timg = _sfm_arrays(cams, [1] * len(cams), positions, tracks)
+    n = len(cams)
+    ids = np.zeros(n, np.int32)
+    depth = np.zeros((n, H, W), np.float32)
+    normal = np.zeros((n, H, W, 3), np.float32)
+    n_out = np.zeros(1, np.int32)
+    rc = lib().pmref_run_stage(ptrs, W, H, _p(krt), _p(reg), n, _p(pos), _p(toff), _p(timg), len(tracks), patch_size,
+                               _p(ids), _p(depth), _p(normal), _p(n_out))
+    assert rc == 0
+    return {int(ids[i]): (depth[i], normal[i]) for i in range(int(n_out[0]))}

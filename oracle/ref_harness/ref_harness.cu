@@ -16,6 +16,9 @@
 //   pmref_solve_view    the per-view body of runPatchMatchMVS without SfM seeding
 //                       (:1094-1107, :1189-1232)
 //   pmref_geometric_filter launchGeometricFilterKernel            (:963-988, :668-781)
+//   pmref_select_sources selectSourceViews (host only)            (:74-157)
+//   pmref_run_stage     runPatchMatchMVS itself with mvs_iterations = 0: random
+//                       init, SfM seeding, initial cost, download (:1028-1260)
 
 #ifndef PMREF_SOURCE
 #error "PMREF_SOURCE must name the reference patchmatch_mvs.cu"
@@ -66,6 +69,11 @@ __global__ void pixel_cost_wrapper_kernel(cudaTextureObject_t ref, const cudaTex
                                  normal[3 * idx + 2], kinv, views, x, y, radius, W, H, S);
 }
 
+// A flat SfM description: camera c is K R t (21 doubles) at cams_krt + 21 c; point p
+// at pos + 3 p, seen by cameras timg[toff[p] .. toff[p + 1]).
+SfMResult make_sfm(const double* cams_krt, const int* registered, int n_cams, const double* pos, const int* toff,
+                   const int* timg, int n_pts);
+
 CameraPose to_pose(const double* krt) {
     CameraPose c;
     for (int i = 0; i < 9; ++i) c.K(i / 3, i % 3) = krt[i];
@@ -75,9 +83,87 @@ CameraPose to_pose(const double* krt) {
     return c;
 }
 
+SfMResult make_sfm(const double* cams_krt, const int* registered, int n_cams, const double* pos, const int* toff,
+                   const int* timg, int n_pts) {
+    SfMResult sfm;
+    sfm.num_registered = 0;
+    for (int c = 0; c < n_cams; ++c) {
+        CameraPose cp = to_pose(cams_krt + 21 * c);
+        cp.image_id = c;
+        cp.is_registered = registered[c] != 0;
+        sfm.num_registered += cp.is_registered ? 1 : 0;
+        sfm.cameras.push_back(cp);
+    }
+    for (int p = 0; p < n_pts; ++p) {
+        SparsePoint sp;
+        sp.position(0) = pos[3 * p];
+        sp.position(1) = pos[3 * p + 1];
+        sp.position(2) = pos[3 * p + 2];
+        for (int k = toff[p]; k < toff[p + 1]; ++k) sp.image_ids.push_back(timg[k]);
+        sp.track_length = toff[p + 1] - toff[p];
+        sfm.points.push_back(sp);
+    }
+    return sfm;
+}
+
 }  // namespace
 
 extern "C" {
+
+// selectSourceViews: per returned view its reference id, source count, sources
+// (HP 8 slots each), scores, baseline angles and depth range.
+int pmref_select_sources(const double* cams_krt, const int* registered, int n_cams, const double* pos,
+                         const int* toff, const int* timg, int n_pts, int num_sources, int* out_ref, int* out_n,
+                         int* out_src, float* out_score, float* out_angle, float* out_dmin, float* out_dmax,
+                         int* n_out) {
+    SfMResult sfm = make_sfm(cams_krt, registered, n_cams, pos, toff, timg, n_pts);
+    std::vector<MVSViewParams> v = selectSourceViews(sfm, num_sources);
+    for (size_t i = 0; i < v.size(); ++i) {
+        out_ref[i] = v[i].ref_image_id;
+        out_n[i] = static_cast<int>(v[i].source_views.size());
+        for (size_t k = 0; k < v[i].source_views.size() && k < 8; ++k) {
+            out_src[8 * i + k] = v[i].source_views[k].image_id;
+            out_score[8 * i + k] = v[i].source_views[k].score;
+            out_angle[8 * i + k] = v[i].source_views[k].baseline_deg;
+        }
+        out_dmin[i] = v[i].depth_min;
+        out_dmax[i] = v[i].depth_max;
+    }
+    *n_out = static_cast<int>(v.size());
+    return 0;
+}
+
+// runPatchMatchMVS with mvs_iterations = 0 and the given patch size on W x H
+// grayscale images (one per camera): each returned view's id, depth and
+// normal (the random init with the SfM seeds painted over it).
+int pmref_run_stage(const float* const* grays, int W, int H, const double* cams_krt, const int* registered,
+                    int n_cams, const double* pos, const int* toff, const int* timg, int n_pts, int patch_size,
+                    int* out_ids, float* out_depth, float* out_normal, int* n_out) {
+    SfMResult sfm = make_sfm(cams_krt, registered, n_cams, pos, toff, timg, n_pts);
+    std::vector<ImageData> images(n_cams);
+    for (int c = 0; c < n_cams; ++c) {
+        images[c].gray = cv::Mat(H, W, CV_32F);
+        std::memcpy(images[c].gray.data, grays[c], static_cast<size_t>(W) * H * sizeof(float));
+        images[c].width = W;
+        images[c].height = H;
+        images[c].id = c;
+    }
+    PipelineConfig config;
+    config.mvs_iterations = 0;
+    config.mvs_patch_size = patch_size;
+    config.verbose = false;
+    config.save_intermediate = false;
+    std::vector<DepthMap> maps = runPatchMatchMVS(images, sfm.cameras, sfm, config);
+    const size_t n = static_cast<size_t>(W) * H;
+    for (size_t i = 0; i < maps.size(); ++i) {
+        out_ids[i] = maps[i].image_id;
+        std::memcpy(out_depth + i * n, maps[i].depth.data, n * sizeof(float));
+        std::memcpy(out_normal + i * 3 * n, maps[i].normal.data, 3 * n * sizeof(float));
+    }
+    *n_out = static_cast<int>(maps.size());
+    return 0;
+}
+
 
 // Per-view homography coefficients exactly as the reference computes them:
 // K^-1 in FP64 cast to FP32, then A = K_s R_rel K_ref^-1, b = K_s t_rel in FP32.
