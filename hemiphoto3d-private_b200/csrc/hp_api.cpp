@@ -114,9 +114,8 @@ hp_status fill_desc(hp_ctx* ctx, const hp_job* j, int jobno, hp::ViewDesc* d) {
                         si->second.W, si->second.H, ref.W, ref.H);
         d->src_tex[s] = si->second.tex32;
         d->src_tex16[s] = si->second.tex16;
-        d->src_quad[s] = si->second.quad16;
+        d->src_quad[s] = si->second.quads.base;
     }
-    d->quad_pitch = static_cast<int>(ref.quad_pitch / sizeof(uint2));
     if (j->use_coeffs) {
         std::memcpy(d->kinv, j->kinv, sizeof d->kinv);
         for (int s = 0; s < j->num_sources; ++s) std::memcpy(d->ab[s], j->ab[s], sizeof d->ab[s]);
@@ -330,7 +329,7 @@ void free_image(Image& im) {
     if (im.arr16) cudaFreeArray(im.arr16);
     if (im.f32) cudaFree(im.f32);
     if (im.f16) cudaFree(im.f16);
-    if (im.quad16) cudaFree(im.quad16);
+    free_quads(&im.quads);
     im = Image();
 }
 
@@ -522,10 +521,10 @@ hp_status hp_image_upload(hp_ctx* ctx, const void* data, int memory, int width, 
                                    cudaMemcpyDeviceToDevice, ctx->stream));
     HP_UP(cudaMemcpy2DToArrayAsync(im.arr16, 0, 0, im.f16, im.pitch16, width * sizeof(__half), height,
                                    cudaMemcpyDeviceToDevice, ctx->stream));
-    HP_UP(cudaMallocPitch(reinterpret_cast<void**>(&im.quad16), &im.quad_pitch, width * sizeof(uint2), height));
+    HP_UP(alloc_quads(ctx->device, width, height, &im.quads));
     HP_UP(counted(ctx, HP_KERNEL_OTHER, [&] {
-        return hp::launch_quads(im.f16, static_cast<int>(im.pitch16 / sizeof(__half)), width, height, im.quad16,
-                                static_cast<int>(im.quad_pitch / sizeof(uint2)), ctx->stream);
+        return hp::launch_quads(im.f16, static_cast<int>(im.pitch16 / sizeof(__half)), width, height, im.quads.base,
+                                ctx->stream);
     }));
     HP_UP(make_linear_texture(im.arr32, &im.tex32));
     HP_UP(make_linear_texture(im.arr16, &im.tex16));

@@ -17,6 +17,20 @@
 
 namespace hpx {
 
+// Block-tiled FP16 software-sampler quad plane in sparsely backed virtual
+// memory (hp_quads.cpp): quad (x, y) at element quad_block_offset(x, y).
+struct QuadPlane {
+    uint2* base = nullptr;       // start of the reserved span
+    size_t reserved = 0;         // bytes of virtual address space
+    size_t physical = 0;         // bytes of device memory mapped under it
+    std::vector<unsigned long long> handles;  // one physical allocation per 256-row block row
+    std::vector<size_t> offsets, sizes;
+    std::vector<char> mapped;
+};
+cudaError_t alloc_quads(int device, int W, int H, QuadPlane* q);
+void free_quads(QuadPlane* q);
+size_t quad_block_offset(int x, int y);
+
 struct Image {
     int W = 0, H = 0;
     float* f32 = nullptr;
@@ -25,10 +39,10 @@ struct Image {
     size_t pitch16 = 0;  // bytes
     cudaArray_t arr32 = nullptr, arr16 = nullptr;
     cudaTextureObject_t tex32 = 0, tex16 = 0;
-    // Software-sampler plane: texel (x, y) holds the 2x2 FP16 block
-    // {t(x,y), t(x+1,y)}, {t(x,y+1), t(x+1,y+1)} shifted by -0.5 (edges clamped).
-    uint2* quad16 = nullptr;
-    size_t quad_pitch = 0;  // bytes
+    // Software-sampler plane: quad (x, y) holds the 2x2 FP16 block
+    // {t(x,y), t(x+1,y)}, {t(x,y+1), t(x+1,y+1)} in difference form shifted by
+    // -0.5 (edges clamped), block-tiled (QuadPlane).
+    QuadPlane quads;
 };
 
 // Grow-only device buffer.

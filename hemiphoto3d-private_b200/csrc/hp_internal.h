@@ -25,8 +25,7 @@ struct ViewDesc {
     const __half* ref16;              // FP16 reference image, row pitch ref16_pitch halves
     cudaTextureObject_t src_tex[HP_MAX_SOURCES];    // FP32 sources, linear filter
     cudaTextureObject_t src_tex16[HP_MAX_SOURCES];  // FP16 sources, linear filter
-    const uint2* src_quad[HP_MAX_SOURCES];          // FP16 sources, software-sampler quads
-    int quad_pitch;                                 // uint2 per quad row
+    const uint2* src_quad[HP_MAX_SOURCES];          // FP16 sources, block-tiled software-sampler quads
     float kinv[9];
     float ab[HP_MAX_SOURCES][12];     // A (9), b (3) per source
     float4* hyp;                      // H*W
@@ -128,9 +127,8 @@ cudaError_t persistent_occupancy_f32(int radius, int stride, int* blocks_per_sm)
 cudaError_t persistent_occupancy_f16(int radius, int stride, int* blocks_per_sm);
 cudaError_t launch_propagate_f16(const BatchList& bl, const SolveConsts& sc, int iteration, int color,
                                  cudaStream_t st);
-// FP16 plane -> software-sampler quad plane (see hpx::Image::quad16).
-cudaError_t launch_quads(const __half* src16, int pitch16, int W, int H, uint2* quads, int quad_pitch,
-                         cudaStream_t st);
+// FP16 plane -> block-tiled software-sampler quad plane (see hpx::QuadPlane).
+cudaError_t launch_quads(const __half* src16, int pitch16, int W, int H, uint2* quads, cudaStream_t st);
 // SfM seeds (host list uploaded to `seeds`) painted over the view's hypotheses; `map` is
 // W*H ints of scratch.
 cudaError_t launch_seed(const ViewDesc& v, const hp_seed* seeds, int num_seeds, int radius, int* map,

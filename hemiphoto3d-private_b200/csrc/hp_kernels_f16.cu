@@ -128,9 +128,12 @@ struct Plane {
 // A warped coordinate c (texel centres at integers) becomes fixed point with
 // 8 fractional bits by one FMA: the bits of RN(c + 49152) are
 // 0x47400000 + RN(256 c) for 0 <= c < 16384.  Two byte permutes then give
-//  - the quad index: bits 8..23 are 0x4000 + floor(c), folded into the base
-//    pointer of the quad plane, and
-//  - the weight as an FP16 number: 0x47 above the fraction byte is the FP16
+//  - the quad's element offset: bytes 1 and 2 are the low and high bytes of
+//    0x4000 + floor(c); the quad plane is tiled in 256 x 256 blocks so that
+//    (x_lo, y_lo, x_hi, y_hi) of the two coordinates, in that byte order, is
+//    the offset itself (hpx::QuadPlane), with the 0x40 bias of both high
+//    bytes folded into the base pointer, and
+//  - the weights as FP16 numbers: 0x47 above the fraction byte is the FP16
 //    encoding of 7 + frac/256, exact, so one FP16 subtraction of 7 leaves the
 //    8-bit fraction (the texture unit's weight resolution).
 // The quad plane stores each 2x2 texel block in difference form, shifted by
@@ -139,15 +142,14 @@ struct Plane {
 constexpr float SOFT_MAGIC = 49152.0f;
 constexpr unsigned SOFT_ORIGIN = 0x47400000u;  // bits of SOFT_MAGIC: coordinate 0
 
-__device__ __forceinline__ const uint2* soft_base(const uint2* quad, int pitch) {
-    // quad - (0x4000 * pitch + 0x4000), formed on the integer address.
+__device__ __forceinline__ const uint2* soft_base(const uint2* quad) {
+    // quad - (0x40 << 16 | 0x40 << 24) elements, formed on the integer address.
     return reinterpret_cast<const uint2*>(reinterpret_cast<uintptr_t>(quad) -
-                                          static_cast<uintptr_t>(0x4000u) * (static_cast<uintptr_t>(pitch) + 1u) *
-                                              sizeof(uint2));
+                                          static_cast<uintptr_t>(0x40400000u) * sizeof(uint2));
 }
 
-__device__ __forceinline__ unsigned soft_offset(unsigned bu, unsigned bv, int pitch) {
-    return __byte_perm(bv, 0u, 0x4421) * static_cast<unsigned>(pitch) + __byte_perm(bu, 0u, 0x4421);
+__device__ __forceinline__ unsigned soft_offset(unsigned bu, unsigned bv) {
+    return __byte_perm(bu, bv, 0x6251);  // bu.b1, bv.b1, bu.b2, bv.b2
 }
 
 __device__ __forceinline__ __half soft_lerp(uint2 q, unsigned wbits) {
@@ -171,9 +173,9 @@ __device__ __forceinline__ __half soft_lerp(uint2 q, unsigned wbits) {
 // a result.  SOFT selects the software sampler; P then holds the homography
 // without the texture's +0.5 texel-centre offset.
 template <int R, int ST, bool CHECK, bool SOFT>
-__device__ __forceinline__ float source_cost(const Plane& P, cudaTextureObject_t tex, const uint2* qbase, int qpitch,
-                                             RefStats st, const __half2* s_win, const float* s_ref, int tw, int lx,
-                                             int ly, int x, int y, float fW, float fH) {
+__device__ __forceinline__ float source_cost(const Plane& P, cudaTextureObject_t tex, const uint2* qbase, RefStats st,
+                                             const __half2* s_win, const float* s_ref, int tw, int lx, int ly, int x,
+                                             int y, float fW, float fH) {
     constexpr int SIDE = Win<R, ST>::SIDE;
     constexpr int PAIRS = Win<R, ST>::PAIRS;
     constexpr int N = Win<R, ST>::N;
@@ -253,7 +255,7 @@ __device__ __forceinline__ float source_cost(const Plane& P, cudaTextureObject_t
                         bv = skip ? SOFT_ORIGIN : bv;
                     }
                     wb[jj] = __byte_perm(bu, bv, 0x7430);
-                    q[jj] = __ldg(qbase + soft_offset(bu, bv, qpitch));
+                    q[jj] = __ldg(qbase + soft_offset(bu, bv));
                     wx = __fadd_rn(wx, hx0);
                     wy = __fadd_rn(wy, hx1);
                     wz = __fadd_rn(wz, hx2);
@@ -377,16 +379,16 @@ __device__ __forceinline__ float cost_f16(RefStats st, const __half2* s_win, con
         const bool all_inside = __all_sync(__activemask(), inside);
         float c;
         if (soft) {
-            const uint2* qb = soft_base(v->src_quad[s], v->quad_pitch);
-            c = all_inside ? source_cost<R, ST, false, true>(P, 0, qb, v->quad_pitch, st, s_win, s_ref, tw, lx, ly, x,
+            const uint2* qb = soft_base(v->src_quad[s]);
+            c = all_inside ? source_cost<R, ST, false, true>(P, 0, qb, st, s_win, s_ref, tw, lx, ly, x,
                                                              y, fW, fH)
-                           : source_cost<R, ST, true, true>(P, 0, qb, v->quad_pitch, st, s_win, s_ref, tw, lx, ly, x,
+                           : source_cost<R, ST, true, true>(P, 0, qb, st, s_win, s_ref, tw, lx, ly, x,
                                                             y, fW, fH);
         } else {
             const cudaTextureObject_t tex = v->src_tex16[s];
-            c = all_inside ? source_cost<R, ST, false, false>(P, tex, nullptr, 0, st, s_win, s_ref, tw, lx, ly, x, y,
+            c = all_inside ? source_cost<R, ST, false, false>(P, tex, nullptr, st, s_win, s_ref, tw, lx, ly, x, y,
                                                               fW, fH)
-                           : source_cost<R, ST, true, false>(P, tex, nullptr, 0, st, s_win, s_ref, tw, lx, ly, x, y,
+                           : source_cost<R, ST, true, false>(P, tex, nullptr, st, s_win, s_ref, tw, lx, ly, x, y,
                                                              fW, fH);
         }
         if (c < top2) {

@@ -50,8 +50,10 @@ __global__ void to_planes_kernel(const void* __restrict__ src, int dtype, int W,
 // each formed exactly in FP32 from the FP16 texels and rounded once to FP16,
 // so a sample is t00 + fx (t10 - t00) + fy ((t01 - t00) + fx dxy): two FP16
 // FMAs.  The -0.5 shift keeps the interpolated values within [-0.5, 0.5].
-__global__ void quads_kernel(const __half* __restrict__ src, int pitch16, int W, int H, uint2* __restrict__ quads,
-                             int quad_pitch) {
+// Quad (x, y) is stored at x_lo | y_lo << 8 | x_hi << 16 | y_hi << 24 (bytes of
+// x and y): 256 x 256 blocks, the layout the sampler addresses with one byte
+// permute (hpx::QuadPlane).
+__global__ void quads_kernel(const __half* __restrict__ src, int pitch16, int W, int H, uint2* __restrict__ quads) {
     const size_t n = static_cast<size_t>(W) * H;
     for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
          i += static_cast<size_t>(gridDim.x) * blockDim.x) {
@@ -66,7 +68,8 @@ __global__ void quads_kernel(const __half* __restrict__ src, int pitch16, int W,
         uint2 q;
         memcpy(&q.x, &a, sizeof q.x);
         memcpy(&q.y, &b, sizeof q.y);
-        quads[static_cast<size_t>(y) * quad_pitch + x] = q;
+        quads[static_cast<size_t>(x & 255) | (static_cast<size_t>(y & 255) << 8) |
+              (static_cast<size_t>(x >> 8) << 16) | (static_cast<size_t>(y >> 8) << 24)] = q;
     }
 }
 
@@ -130,9 +133,8 @@ cudaError_t launch_to_f32(const void* src, int dtype, int W, int H, float* dst, 
     return cudaGetLastError();
 }
 
-cudaError_t launch_quads(const __half* src16, int pitch16, int W, int H, uint2* quads, int quad_pitch,
-                         cudaStream_t st) {
-    quads_kernel<<<stream_grid(), 256, 0, st>>>(src16, pitch16, W, H, quads, quad_pitch);
+cudaError_t launch_quads(const __half* src16, int pitch16, int W, int H, uint2* quads, cudaStream_t st) {
+    quads_kernel<<<stream_grid(), 256, 0, st>>>(src16, pitch16, W, H, quads);
     return cudaGetLastError();
 }
 
