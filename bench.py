@@ -45,7 +45,7 @@ METRIC = "depth-map Mpix*iter/s on 1 B200 (FP16-acc vs plain FP32)"
 # Serving form: Poisson arrivals, each request one depth-map solve on the FP16-acc path.
 # Batched form: one plan over views of uneven sizes, autotuned schedule, replayed as a CUDA graph.
 BATCHED = dict(name="batched_uneven_64", views=64, sizes=[[640, 480], [1280, 720], [1920, 1080], [4000, 3000]],
-               sources=[2, 8], iterations=[6, 12], radius=7, stride=2, views_per_size=9, runs=3, tune_repeats=2)
+               sources=[2, 8], iterations=[6, 12], radius=7, stride=2, views_per_size=9, runs=2, tune_repeats=1)
 SERVING = dict(name="serving_poisson", sizes=[[640, 480], [1920, 1080], [4000, 3000]], sources=[2, 8],
                iterations=[4, 12], radius=7, stride=2, requests=240, rate_per_s=10.0, views_per_size=9,
                mem_fraction=0.8)
@@ -116,6 +116,27 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------------------------------------
+def rank_job_keys(rank: int, n_views: int):
+    """(RNG seed, view id) of each of a rank's jobs.  Views are independent, so under torchrun every rank
+    solves its own batch: the same scene, keyed differently, so no two ranks compute the same streams."""
+    return [(42 + 1_000_003 * rank, r + 1000 * rank) for r in range(n_views)]
+
+
+def max_over_ranks(x: float, dist, device) -> float:
+    """The largest value over all ranks (device time of a step); x itself when running alone."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(world: int, units_per_rank: float, steps: int, max_ms: float) -> float:
+    """Whole-job Mpix*iter/s: all ranks' units over the slowest rank's time."""
+    return world * units_per_rank * steps / (max_ms / 1e3)
+
+
 def build_scene(views: int):
     scene = importlib.import_module(PKG + ".scene")
     # The full 20-view arc is always rendered, so a reduced --views case keeps the workload's geometry.
@@ -198,12 +219,12 @@ def run_engine(args, rank, world, local_rank):
 
     def make_jobs(id_list):
         jobs = []
-        for r in range(n_views):
+        for r, (seed, view_id) in enumerate(rank_job_keys(rank, n_views)):
             srcs = s.sources[r]
             cam = lambda i: hp.make_camera(s.views[i].cam.K, s.views[i].cam.R, s.views[i].cam.t)
             jobs.append(hp.make_job(id_list[r], [id_list[i] for i in srcs], cam(r), [cam(i) for i in srcs],
-                                    *WORKLOAD["depth_range"], seed=42 + 1_000_003 * rank,
-                                    view_id=r + 1000 * rank, iterations=WORKLOAD["iterations"]))
+                                    *WORKLOAD["depth_range"], seed=seed, view_id=view_id,
+                                    iterations=WORKLOAD["iterations"]))
         return jobs
 
     jobs = make_jobs(ids)
@@ -236,12 +257,8 @@ def run_engine(args, rank, world, local_rank):
             e1.synchronize()
         barrier()
         ctx.set_profiling(False)
-        ms = e0.elapsed_time(e1)
+        ms = max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
         prof = ctx.profile()
-        if dist is not None:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
         return ms, prof, clk.summary()
 
     head = args.precision
@@ -250,7 +267,8 @@ def run_engine(args, rank, world, local_rank):
     variants = {}
     if not args.no_variants:
         ms2, prof2, clocks2 = timed(other, args.steps, max(1, args.warmup))
-        variants[other] = {"value": world * units_per_step * args.steps / (ms2 / 1e3), "ms_per_step": ms2 / args.steps,
+        variants[other] = {"value": job_throughput(world, units_per_step, args.steps, ms2),
+                           "ms_per_step": ms2 / args.steps,
                            "propagate_ms_per_launch": prof2["propagate"]["device_ms"] / max(1, prof2["propagate"]["timed"]),
                            "clocks": clocks2}
 
@@ -290,11 +308,7 @@ def run_engine(args, rank, world, local_rank):
         e2e_step()
     e1.record(stream)
     e1.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    if dist is not None:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
     barrier()
     h2d = sum(int(t.numel()) for t in pinned_imgs)
     d2h = n_views * H * W * (4 + 12 + 4)
@@ -325,7 +339,7 @@ def run_engine(args, rank, world, local_rank):
     fetch_rate = visits * taps_per_visit / (prop_ms * 1e-3)
     fma_peak = onchip.get("fma_per_s")
 
-    value = world * units_per_step * args.steps / (ms / 1e3)
+    value = job_throughput(world, units_per_step, args.steps, ms)
     line = {
         "metric": METRIC,
         "value": round(value, 2),
@@ -345,7 +359,7 @@ def run_engine(args, rank, world, local_rank):
                    "depth_range": WORKLOAD["depth_range"], "images": "u8", "parallelism": f"views/{world} ranks",
                    "mpix_iter_per_step": round(units_per_step * world, 3),
                    "l2": "inputs larger than L2 (20 x 2.07 Mpix images + 830 MB state per step), no flush"},
-        "e2e": {"value": round(world * units_per_step * args.e2e_steps / (e2e_ms / 1e3), 2), "unit": "Mpix*iter/s",
+        "e2e": {"value": round(job_throughput(world, units_per_step, args.e2e_steps, e2e_ms), 2), "unit": "Mpix*iter/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": args.e2e_steps},
         "roofline": {"bound": "hbm", "achieved": round(achieved_hbm, 2), "peak": hbm_peak, "unit": "GB/s",
                      "frac": round(achieved_hbm / hbm_peak, 5), "peak_source": hbm_src,
@@ -596,7 +610,7 @@ def main():
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180))
     try:
         line = run_engine(args, rank, world, local_rank)
         if line:
