@@ -27,7 +27,7 @@ struct ViewDesc {
     cudaTextureObject_t src_tex16[HP_MAX_SOURCES];  // FP16 sources, linear filter
     const uint2* src_quad[HP_MAX_SOURCES];          // FP16 sources, block-tiled software-sampler quads
     float kinv[9];
-    float ab[HP_MAX_SOURCES][12];     // A (9), b (3) per source
+    alignas(16) float ab[HP_MAX_SOURCES][12];  // A (9), b (3) per source; 16-byte aligned rows
     float4* hyp;                      // H*W
     float* cost;                      // H*W
     int ref_pitch, ref16_pitch;

@@ -337,12 +337,15 @@ __device__ __forceinline__ float cost_f16(RefStats st, const __half2* s_win, con
     const float m1 = __fmul_rn(__fmaf_rn(k[1], cnx, __fmaf_rn(k[4], cny, __fmul_rn(k[7], cnz))), ind);
     const float m2 = __fmul_rn(__fmaf_rn(k[2], cnx, __fmaf_rn(k[5], cny, __fmul_rn(k[8], cnz))), ind);
     const float fW = static_cast<float>(v->W), fH = static_cast<float>(v->H);
-    const float xa = static_cast<float>(x - R), xb = static_cast<float>(x - R + (Win<R, ST>::SIDE - 1) * ST);
-    const float ya = static_cast<float>(y - R), yb = static_cast<float>(y - R + (Win<R, ST>::SIDE - 1) * ST);
+    const float xa = static_cast<float>(x - R);
+    const float ya = static_cast<float>(y - R);
     float top0 = 2.0f, top1 = 2.0f, top2 = 2.0f;
     const int S = v->S;
     for (int s = 0; s < S; ++s) {
-        const float* A = v->ab[s];
+        // A (9) and b (3) of the source: three 16-byte loads (ViewDesc::ab is 16-byte aligned).
+        const float4* A4 = reinterpret_cast<const float4*>(v->ab[s]);
+        const float4 q0 = __ldg(A4), q1 = __ldg(A4 + 1), q2 = __ldg(A4 + 2);
+        const float A[12] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w};
         // Uniform over the launch: every lane of a warp takes the same sampler.
         const bool soft = (soft_mask >> s) & 1u;
         const float lo = soft ? 0.0f : 0.5f;  // texel-centre offset of the sampler's coordinate
@@ -350,27 +353,47 @@ __device__ __forceinline__ float cost_f16(RefStats st, const __half2* s_win, con
         P.h[6] = __fmaf_rn(A[11], m0, A[6]);
         P.h[7] = __fmaf_rn(A[11], m1, A[7]);
         P.h[8] = __fmaf_rn(A[11], m2, A[8]);
-        P.h[0] = __fmaf_rn(lo, P.h[6], __fmaf_rn(A[9], m0, A[0]));
-        P.h[1] = __fmaf_rn(lo, P.h[7], __fmaf_rn(A[9], m1, A[1]));
-        P.h[2] = __fmaf_rn(lo, P.h[8], __fmaf_rn(A[9], m2, A[2]));
-        P.h[3] = __fmaf_rn(lo, P.h[6], __fmaf_rn(A[10], m0, A[3]));
-        P.h[4] = __fmaf_rn(lo, P.h[7], __fmaf_rn(A[10], m1, A[4]));
-        P.h[5] = __fmaf_rn(lo, P.h[8], __fmaf_rn(A[10], m2, A[5]));
+        P.h[0] = __fmaf_rn(A[9], m0, A[0]);
+        P.h[1] = __fmaf_rn(A[9], m1, A[1]);
+        P.h[2] = __fmaf_rn(A[9], m2, A[2]);
+        P.h[3] = __fmaf_rn(A[10], m0, A[3]);
+        P.h[4] = __fmaf_rn(A[10], m1, A[4]);
+        P.h[5] = __fmaf_rn(A[10], m2, A[5]);
+        if (!soft) {  // texture taps: fold the +0.5 texel-centre offset into rows 0 and 1
+            P.h[0] = __fmaf_rn(0.5f, P.h[6], P.h[0]);
+            P.h[1] = __fmaf_rn(0.5f, P.h[7], P.h[1]);
+            P.h[2] = __fmaf_rn(0.5f, P.h[8], P.h[2]);
+            P.h[3] = __fmaf_rn(0.5f, P.h[6], P.h[3]);
+            P.h[4] = __fmaf_rn(0.5f, P.h[7], P.h[4]);
+            P.h[5] = __fmaf_rn(0.5f, P.h[8], P.h[5]);
+        }
         // Corner test: in front of the source (w_z > 1e-6) with all four
         // corners inside [lo, W - 1 + lo) x [lo, H - 1 + lo) by a 0.05 px
-        // margin (which covers the rounding of the row-stepped taps), tested
-        // as w_x >= ulo w_z etc. without a division.  The warp of the window
-        // rectangle is then the convex quad of its corners, so every tap is
-        // valid by the per-tap rules too.
+        // margin (which covers the rounding of the row-stepped taps and of the
+        // corners themselves, stepped here from the first along the window's
+        // edges), tested as w_x >= ulo w_z etc. without a division.  The warp
+        // of the window rectangle is then the convex quad of its corners, so
+        // every tap is valid by the per-tap rules too.
         const float ulo = __fadd_rn(lo, 0.05f), uhi = __fsub_rn(__fadd_rn(fW, lo), 1.05f);
         const float vhi = __fsub_rn(__fadd_rn(fH, lo), 1.05f);
+        constexpr float SPAN = static_cast<float>((Win<R, ST>::SIDE - 1) * ST);
+        float cz[4], cx[4], cy[4];
+        cz[0] = __fmaf_rn(P.h[6], xa, __fmaf_rn(P.h[7], ya, P.h[8]));
+        cx[0] = __fmaf_rn(P.h[0], xa, __fmaf_rn(P.h[1], ya, P.h[2]));
+        cy[0] = __fmaf_rn(P.h[3], xa, __fmaf_rn(P.h[4], ya, P.h[5]));
+        cz[1] = __fmaf_rn(P.h[6], SPAN, cz[0]);
+        cx[1] = __fmaf_rn(P.h[0], SPAN, cx[0]);
+        cy[1] = __fmaf_rn(P.h[3], SPAN, cy[0]);
+        cz[2] = __fmaf_rn(P.h[7], SPAN, cz[0]);
+        cx[2] = __fmaf_rn(P.h[1], SPAN, cx[0]);
+        cy[2] = __fmaf_rn(P.h[4], SPAN, cy[0]);
+        cz[3] = __fmaf_rn(P.h[7], SPAN, cz[1]);
+        cx[3] = __fmaf_rn(P.h[1], SPAN, cx[1]);
+        cy[3] = __fmaf_rn(P.h[4], SPAN, cy[1]);
         bool inside = true;
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
-            const float px = (c & 1) ? xb : xa, py = (c & 2) ? yb : ya;
-            const float wz = __fmaf_rn(P.h[6], px, __fmaf_rn(P.h[7], py, P.h[8]));
-            const float wxc = __fmaf_rn(P.h[0], px, __fmaf_rn(P.h[1], py, P.h[2]));
-            const float wyc = __fmaf_rn(P.h[3], px, __fmaf_rn(P.h[4], py, P.h[5]));
+            const float wz = cz[c], wxc = cx[c], wyc = cy[c];
             inside = inside && wz > 1e-6f && wxc >= __fmul_rn(ulo, wz) && wxc < __fmul_rn(uhi, wz) &&
                      wyc >= __fmul_rn(ulo, wz) && wyc < __fmul_rn(vhi, wz);
         }
