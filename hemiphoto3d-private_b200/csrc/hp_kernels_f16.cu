@@ -464,17 +464,29 @@ __global__ void __launch_bounds__(CTA_THREADS, HP_F16_MIN_BLOCKS) cost16_kernel(
     tile_cost16<R, ST>(v, tile_x, tile_y, sc, s_ref, s_win);
 }
 
-// One red-black half-pass.  The neighbour phase is compacted per warp exactly
-// as in the FP32 kernel (see propagate_kernel there): lanes list the
-// neighbour planes they must score, the warp scores the union 32 items at a
-// time (an item borrows its owner's window statistics by shuffle and the
-// owner's column of s_win), and owners fold the costs in L, R, U, D order.
+// One red-black half-pass.  The neighbour phase is compacted across the CTA:
+// every lane lists the neighbour planes its pixel must score (duplicates of
+// the current plane or of an earlier neighbour skipped), the lists of all
+// eight warps are concatenated in shared memory, and the warps score the
+// union 32 items at a time (warp w takes items [32 (w + 8 k), 32 (w + 8 k) +
+// 32)).  An item reads its owner pixel's window statistics and s_win column
+// from shared memory and leaves its cost in the owner's slot, so owners then
+// fold the costs in L, R, U, D order exactly as if they had scored them
+// themselves: results do not depend on which lane scored what.
 constexpr int WARPS = CTA_THREADS / 32;
+
+// Shared memory of the half-pass beyond the reference tile and window.
+struct PassSmem {
+    float cost[WARPS][32 * 4];        // neighbour cost, slot (lane << 2 | cand) of the owner's warp
+    unsigned short items[WARPS * 128];  // CTA item list: warp << 7 | lane << 2 | cand
+    float2 stat[CTA_THREADS];         // (mean, ssd) of each thread's pixel window
+    int warp_total[WARPS];
+};
 
 template <int R, int ST>
 __device__ __forceinline__ void tile_propagate16(const ViewDesc* v, int tile_x, int tile_y, const SolveConsts& sc,
                                                  int iteration, int color, float* s_ref, __half2* s_win,
-                                                 float (*s_cost)[32 * 4], unsigned char (*s_items)[32 * 4]) {
+                                                 PassSmem& sm) {
     constexpr int tw = TILE_W + 2 * R, th = TILE_H + 2 * R;
     const int x0 = tile_x * TILE_W, y0 = tile_y * TILE_H;
     load_ref_tile16(s_ref, tw, th, v, x0, y0, R);
@@ -482,11 +494,10 @@ __device__ __forceinline__ void tile_propagate16(const ViewDesc* v, int tile_x, 
     const int W = v->W, H = v->H;
     const int ly = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int y = y0 + ly;
-    if (y >= H) return;  // uniform per warp
     const int parity = (y + color) & 1;
     const int lx = 2 * lane + parity;
     const int x = x0 + lx;
-    const bool active = x < W;
+    const bool active = y < H && x < W;  // every thread takes part in the CTA barriers below
     const size_t idx = static_cast<size_t>(y) * W + x;
     const float dmin = v->dmin, dmax = v->dmax;
     RefStats st{0.f, 0.f};
@@ -515,6 +526,7 @@ __device__ __forceinline__ void tile_propagate16(const ViewDesc* v, int tile_x, 
             if (!dup) need |= 1u << cand;
         }
     }
+    sm.stat[threadIdx.x] = make_float2(st.mean, st.ssd);
     const int cnt = __popc(need);
     int incl = cnt;
 #pragma unroll
@@ -522,35 +534,42 @@ __device__ __forceinline__ void tile_propagate16(const ViewDesc* v, int tile_x, 
         const int t = __shfl_up_sync(0xffffffffu, incl, o);
         if (lane >= o) incl += t;
     }
-    const int total = __shfl_sync(0xffffffffu, incl, 31);
-    {
-        int k = incl - cnt;
-        for (int cand = 0; cand < 4; ++cand)
-            if (need & (1u << cand)) s_items[ly][k++] = static_cast<unsigned char>((lane << 2) | cand);
+    if (lane == 31) sm.warp_total[ly] = incl;
+    __syncthreads();  // warp totals, window statistics and s_win columns are complete
+    int offset = 0, total = 0;
+#pragma unroll
+    for (int w = 0; w < WARPS; ++w) {
+        const int t = sm.warp_total[w];
+        offset += w < ly ? t : 0;
+        total += t;
     }
-    __syncwarp();
-    for (int base = 0; base < total; base += 32) {
+    {
+        int k = offset + incl - cnt;
+        for (int cand = 0; cand < 4; ++cand)
+            if (need & (1u << cand)) sm.items[k++] = static_cast<unsigned short>((ly << 7) | (lane << 2) | cand);
+    }
+    __syncthreads();  // the CTA's item list is complete
+    for (int base = ly * 32; base < total; base += CTA_THREADS) {
         const int w = base + lane;
-        const int item = w < total ? s_items[ly][w] : 0;
-        const int owner = item >> 2, cand = item & 3;
-        RefStats ost;
-        ost.mean = __shfl_sync(0xffffffffu, st.mean, owner);
-        ost.ssd = __shfl_sync(0xffffffffu, st.ssd, owner);
         if (w < total) {
-            const int olx = 2 * owner + parity, ox = x0 + olx;
+            const int item = sm.items[w];
+            const int oly = item >> 7, owner = (item >> 2) & 31, cand = item & 3;
+            const int oy = y0 + oly, olx = 2 * owner + ((oy + color) & 1), ox = x0 + olx;
+            const float2 os = sm.stat[oly * 32 + owner];
             const int nxp = ox + (cand == 0 ? -1 : (cand == 1 ? 1 : 0));
-            const int nyp = y + (cand == 2 ? -1 : (cand == 3 ? 1 : 0));
+            const int nyp = oy + (cand == 2 ? -1 : (cand == 3 ? 1 : 0));
             const float4 h = v->hyp[static_cast<size_t>(nyp) * W + nxp];
-            s_cost[ly][item] = cost_f16<R, ST>(ost, s_win + ly * 32 + owner, s_ref, tw, olx, ly, ox, y, h.x, h.y,
-                                               h.z, h.w, v, sc.top_k, sc.soft_mask);
+            sm.cost[oly][item & 127] = cost_f16<R, ST>(RefStats{os.x, os.y}, s_win + oly * 32 + owner, s_ref, tw,
+                                                       olx, oly, ox, oy, h.x, h.y, h.z, h.w, v, sc.top_k,
+                                                       sc.soft_mask);
         }
     }
-    __syncwarp();
+    __syncthreads();  // every neighbour cost is in its owner's slot
     if (!active) return;
 #pragma unroll
     for (int cand = 0; cand < 4; ++cand) {
         if (need & (1u << cand)) {
-            const float c = s_cost[ly][(lane << 2) | cand];
+            const float c = sm.cost[ly][(lane << 2) | cand];
             if (c < best_cost) {
                 const int nxp = x + (cand == 0 ? -1 : (cand == 1 ? 1 : 0));
                 const int nyp = y + (cand == 2 ? -1 : (cand == 3 ? 1 : 0));
@@ -595,11 +614,10 @@ __global__ void __launch_bounds__(CTA_THREADS, HP_F16_MIN_BLOCKS) propagate16_ke
                                                                                      int iteration, int color) {
     __shared__ float s_ref[MAX_TW * MAX_TH];
     __shared__ __half2 s_win[Win<R, ST>::IN_SMEM ? WIN_PAIRS_MAX * CTA_THREADS : 1];
-    __shared__ float s_cost[WARPS][32 * 4];
-    __shared__ unsigned char s_items[WARPS][32 * 4];
+    __shared__ PassSmem sm;
     int tile_x, tile_y;
     const ViewDesc* v = locate_tile16(bl, blockIdx.x, &tile_x, &tile_y);
-    tile_propagate16<R, ST>(v, tile_x, tile_y, sc, iteration, color, s_ref, s_win, s_cost, s_items);
+    tile_propagate16<R, ST>(v, tile_x, tile_y, sc, iteration, color, s_ref, s_win, sm);
 }
 
 // Persistent form (see Schedule and the FP32 persistent kernel): the stage
@@ -608,8 +626,7 @@ template <int R, int ST>
 __global__ void __launch_bounds__(CTA_THREADS, HP_F16_MIN_BLOCKS) persistent16_kernel(Schedule s) {
     __shared__ float s_ref[MAX_TW * MAX_TH];
     __shared__ __half2 s_win[Win<R, ST>::IN_SMEM ? WIN_PAIRS_MAX * CTA_THREADS : 1];
-    __shared__ float s_cost[WARPS][32 * 4];
-    __shared__ unsigned char s_items[WARPS][32 * 4];
+    __shared__ PassSmem sm;
     __shared__ int s_ticket;
     for (;;) {
         if (threadIdx.x == 0) s_ticket = sched_next(s);
@@ -624,7 +641,7 @@ __global__ void __launch_bounds__(CTA_THREADS, HP_F16_MIN_BLOCKS) persistent16_k
             tile_cost16<R, ST>(v, t.tx, t.ty, s.sc, s_ref, s_win);
         } else if (t.stage <= 2 * v->iterations) {
             const int k = t.stage - 1;
-            tile_propagate16<R, ST>(v, t.tx, t.ty, s.sc, k >> 1, k & 1, s_ref, s_win, s_cost, s_items);
+            tile_propagate16<R, ST>(v, t.tx, t.ty, s.sc, k >> 1, k & 1, s_ref, s_win, sm);
         } else {
             tile_unpack(v, t.tx, t.ty);
         }
