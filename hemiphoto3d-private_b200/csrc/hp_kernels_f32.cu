@@ -242,17 +242,25 @@ __global__ void __launch_bounds__(CTA_THREADS, HP_F32_MIN_BLOCKS) cost_kernel(Ba
 // same pixel, same plane, same arithmetic, same cost).  Lanes skip different
 // candidates, so scoring them lane by lane would leave warps half idle while
 // every texture instruction still costs nearly a full warp's worth of filter
-// throughput.  Instead the warp writes the union of its (pixel, neighbour) items
-// to a list in shared memory and scores it 32 items at a time, then each owner
-// folds its costs in L, R, U, D order with the same strict-less rule - the
-// result is that of the sequential loop.  The refinement perturbations
+// throughput.  Instead the CTA's eight warps write the union of their (pixel,
+// neighbour) items to one list in shared memory and score it 32 items at a
+// time (warp w takes items [32 (w + 8 k), 32 (w + 8 k) + 32)), each cost
+// landing in its owner's slot; then each owner folds its costs in L, R, U, D
+// order with the same strict-less rule - the result is that of the
+// sequential loop.  The refinement perturbations
 // (:583-648) follow per lane: every lane has exactly refine_steps of them.
 constexpr int WARPS = CTA_THREADS / 32;
 
+// Shared memory of the half-pass beyond the reference tile.
+struct PassSmem {
+    float cost[WARPS][32 * 4];          // neighbour cost, slot (lane << 2 | cand) of the owner's warp
+    unsigned short items[WARPS * 128];  // CTA item list: warp << 7 | lane << 2 | cand
+    int warp_total[WARPS];
+};
+
 template <int R, int ST>
 __device__ __forceinline__ void tile_propagate(const ViewDesc* v, int tile_x, int tile_y, const SolveConsts& sc,
-                                               int iteration, int color, float* s_ref, float (*s_cost)[32 * 4],
-                                               unsigned char (*s_items)[32 * 4]) {
+                                               int iteration, int color, float* s_ref, PassSmem& sm) {
     constexpr int tw = TILE_W + 2 * R, th = TILE_H + 2 * R;
     const int x0 = tile_x * TILE_W, y0 = tile_y * TILE_H;
     load_ref_tile(s_ref, tw, th, v, x0, y0, R);
@@ -260,11 +268,10 @@ __device__ __forceinline__ void tile_propagate(const ViewDesc* v, int tile_x, in
     const int W = v->W, H = v->H;
     const int ly = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int y = y0 + ly;
-    if (y >= H) return;  // uniform per warp
     const int parity = (y + color) & 1;
     const int lx = 2 * lane + parity;
     const int x = x0 + lx;
-    const bool active = x < W;
+    const bool active = y < H && x < W;  // every thread takes part in the CTA barriers below
     const size_t idx = static_cast<size_t>(y) * W + x;
     const float dmin = v->dmin, dmax = v->dmax;
 
@@ -292,7 +299,7 @@ __device__ __forceinline__ void tile_propagate(const ViewDesc* v, int tile_x, in
             if (!dup) need |= 1u << cand;
         }
     }
-    // Warp-wide exclusive scan of the item counts; owners write their items.
+    // Exclusive scan of the item counts over the warp, then over the CTA's warps; owners write their items.
     const int cnt = __popc(need);
     int incl = cnt;
 #pragma unroll
@@ -300,31 +307,39 @@ __device__ __forceinline__ void tile_propagate(const ViewDesc* v, int tile_x, in
         const int t = __shfl_up_sync(0xffffffffu, incl, o);
         if (lane >= o) incl += t;
     }
-    const int total = __shfl_sync(0xffffffffu, incl, 31);
-    {
-        int k = incl - cnt;
-        for (int cand = 0; cand < 4; ++cand)
-            if (need & (1u << cand)) s_items[ly][k++] = static_cast<unsigned char>((lane << 2) | cand);
+    if (lane == 31) sm.warp_total[ly] = incl;
+    __syncthreads();
+    int offset = 0, total = 0;
+#pragma unroll
+    for (int w = 0; w < WARPS; ++w) {
+        const int t = sm.warp_total[w];
+        offset += w < ly ? t : 0;
+        total += t;
     }
-    __syncwarp();
-    for (int base = 0; base < total; base += 32) {
+    {
+        int k = offset + incl - cnt;
+        for (int cand = 0; cand < 4; ++cand)
+            if (need & (1u << cand)) sm.items[k++] = static_cast<unsigned short>((ly << 7) | (lane << 2) | cand);
+    }
+    __syncthreads();
+    for (int base = ly * 32; base < total; base += CTA_THREADS) {
         const int w = base + lane;
         if (w < total) {
-            const int item = s_items[ly][w];
-            const int owner = item >> 2, cand = item & 3;
-            const int olx = 2 * owner + parity, ox = x0 + olx;
+            const int item = sm.items[w];
+            const int oly = item >> 7, owner = (item >> 2) & 31, cand = item & 3;
+            const int oy = y0 + oly, olx = 2 * owner + ((oy + color) & 1), ox = x0 + olx;
             const int nxp = ox + (cand == 0 ? -1 : (cand == 1 ? 1 : 0));
-            const int nyp = y + (cand == 2 ? -1 : (cand == 3 ? 1 : 0));
+            const int nyp = oy + (cand == 2 ? -1 : (cand == 3 ? 1 : 0));
             const float4 h = v->hyp[static_cast<size_t>(nyp) * W + nxp];
-            s_cost[ly][item] = cost_f32<R, ST>(s_ref, tw, olx, ly, ox, y, h.x, h.y, h.z, h.w, v, sc.top_k);
+            sm.cost[oly][item & 127] = cost_f32<R, ST>(s_ref, tw, olx, oly, ox, oy, h.x, h.y, h.z, h.w, v, sc.top_k);
         }
     }
-    __syncwarp();
+    __syncthreads();
     if (!active) return;
 #pragma unroll
     for (int cand = 0; cand < 4; ++cand) {
         if (need & (1u << cand)) {
-            const float c = s_cost[ly][(lane << 2) | cand];
+            const float c = sm.cost[ly][(lane << 2) | cand];
             if (c < best_cost) {
                 const int nxp = x + (cand == 0 ? -1 : (cand == 1 ? 1 : 0));
                 const int nyp = y + (cand == 2 ? -1 : (cand == 3 ? 1 : 0));
@@ -369,11 +384,10 @@ template <int R, int ST>
 __global__ void __launch_bounds__(CTA_THREADS, HP_F32_MIN_BLOCKS) propagate_kernel(BatchList bl, SolveConsts sc,
                                                                                    int iteration, int color) {
     __shared__ float s_ref[MAX_TW * MAX_TH];
-    __shared__ float s_cost[WARPS][32 * 4];
-    __shared__ unsigned char s_items[WARPS][32 * 4];
+    __shared__ PassSmem sm;
     int tile_x, tile_y;
     const ViewDesc* v = locate_tile(bl, blockIdx.x, &tile_x, &tile_y);
-    tile_propagate<R, ST>(v, tile_x, tile_y, sc, iteration, color, s_ref, s_cost, s_items);
+    tile_propagate<R, ST>(v, tile_x, tile_y, sc, iteration, color, s_ref, sm);
 }
 
 // Persistent form: one launch runs every stage of every view of a solve
@@ -383,8 +397,7 @@ __global__ void __launch_bounds__(CTA_THREADS, HP_F32_MIN_BLOCKS) propagate_kern
 template <int R, int ST>
 __global__ void __launch_bounds__(CTA_THREADS, HP_F32_MIN_BLOCKS) persistent_kernel(Schedule s) {
     __shared__ float s_ref[MAX_TW * MAX_TH];
-    __shared__ float s_cost[WARPS][32 * 4];
-    __shared__ unsigned char s_items[WARPS][32 * 4];
+    __shared__ PassSmem sm;
     __shared__ int s_ticket;
     for (;;) {
         if (threadIdx.x == 0) s_ticket = sched_next(s);
@@ -399,7 +412,7 @@ __global__ void __launch_bounds__(CTA_THREADS, HP_F32_MIN_BLOCKS) persistent_ker
             tile_cost<R, ST>(v, t.tx, t.ty, s.sc, s_ref);
         } else if (t.stage <= 2 * v->iterations) {
             const int k = t.stage - 1;
-            tile_propagate<R, ST>(v, t.tx, t.ty, s.sc, k >> 1, k & 1, s_ref, s_cost, s_items);
+            tile_propagate<R, ST>(v, t.tx, t.ty, s.sc, k >> 1, k & 1, s_ref, sm);
         } else {
             tile_unpack(v, t.tx, t.ty);
         }
