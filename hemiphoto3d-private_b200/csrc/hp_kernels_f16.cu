@@ -390,18 +390,33 @@ __device__ __forceinline__ float cost_f16(RefStats st, const __half2* s_win, con
         cz[3] = __fmaf_rn(P.h[7], SPAN, cz[1]);
         cx[3] = __fmaf_rn(P.h[1], SPAN, cx[1]);
         cy[3] = __fmaf_rn(P.h[4], SPAN, cy[1]);
-        bool inside = true;
+        // Fully outside: in front at every corner and every corner beyond the
+        // same edge of the valid region by the margin.  The window's warp is
+        // the convex quad of its corners, so every tap is invalid, the count
+        // is 0 and the reference's rule makes the source cost 2 - no tap needs
+        // sampling.
+        const float olo = __fsub_rn(lo, 0.05f), ohi = __fadd_rn(__fadd_rn(fW, lo), -0.95f);
+        const float ovhi = __fadd_rn(__fadd_rn(fH, lo), -0.95f);
+        bool inside = true, front = true, left = true, right = true, top = true, bottom = true;
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             const float wz = cz[c], wxc = cx[c], wyc = cy[c];
             inside = inside && wz > 1e-6f && wxc >= __fmul_rn(ulo, wz) && wxc < __fmul_rn(uhi, wz) &&
                      wyc >= __fmul_rn(ulo, wz) && wyc < __fmul_rn(vhi, wz);
+            front = front && wz > 1e-6f;
+            left = left && wxc < __fmul_rn(olo, wz);
+            right = right && wxc >= __fmul_rn(ohi, wz);
+            top = top && wyc < __fmul_rn(olo, wz);
+            bottom = bottom && wyc >= __fmul_rn(ovhi, wz);
         }
-        // One form per warp: the checked form gives the unchecked form's bits
-        // whenever every tap is valid, so lanes that are inside lose nothing.
-        const bool all_inside = __all_sync(__activemask(), inside);
-        float c;
-        if (soft) {
+        const bool outside = front && (left || right || top || bottom);
+        // One form per warp for the lanes that sample: the checked form gives
+        // the unchecked form's bits whenever every tap is valid, so lanes that
+        // are inside lose nothing.
+        const bool all_inside = __all_sync(__activemask(), inside || outside);
+        float c = 2.0f;
+        if (outside) {
+        } else if (soft) {
             const uint2* qb = soft_base(v->src_quad[s]);
             c = all_inside ? source_cost<R, ST, false, true>(P, 0, qb, st, s_win, s_ref, tw, lx, ly, x,
                                                              y, fW, fH)
