@@ -48,7 +48,7 @@ BATCHED = dict(name="batched_uneven_64", views=64, sizes=[[640, 480], [1280, 720
                sources=[2, 8], iterations=[6, 12], radius=7, stride=2, views_per_size=9, runs=2, tune_repeats=1)
 SERVING = dict(name="serving_poisson", sizes=[[640, 480], [1920, 1080], [4000, 3000]], sources=[2, 8],
                iterations=[4, 12], radius=7, stride=2, requests=240, rate_per_s=10.0, views_per_size=9,
-               mem_fraction=0.8)
+               mem_fraction=0.8, passes_per_step=8)
 
 
 def parse():
@@ -68,6 +68,9 @@ def parse():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-plan leg (N = 1 only)")
     ap.add_argument("--serve-requests", type=int, default=SERVING["requests"])
     ap.add_argument("--serve-rate", type=float, default=SERVING["rate_per_s"], help="Poisson arrivals per second")
+    ap.add_argument("--serve-passes", type=int, default=SERVING["passes_per_step"], help="server stages per step")
+    ap.add_argument("--serve-only", action="store_true", help="run only the serving leg (N = 1)")
+    ap.add_argument("--serve-split", type=int, default=0, help="server: one launch per stage offset")
     return ap.parse_args()
 
 
@@ -510,7 +513,8 @@ def run_serving(args, hp, device: int):
                           seed=7 + i, view_id=r, iterations=it)
         reqs.append((t, job, w, h, w * h * it))
     params = hp.default_params(radius=SERVING["radius"], stride=SERVING["stride"], precision=hp.PRECISION_F16ACC)
-    srv = hp.Server(ctx, params, mem_fraction=SERVING["mem_fraction"])
+    srv = hp.Server(ctx, params, mem_fraction=SERVING["mem_fraction"], passes_per_step=args.serve_passes,
+                    split_launches=args.serve_split)
     # Warm-up: one request of each size, not counted.
     for sc, ids, cams, w, h in pools:
         m = hp.maps_of(torch.empty(h, w, device="cuda"), torch.empty(h, w, 3, device="cuda"),
@@ -564,6 +568,7 @@ def run_serving(args, hp, device: int):
         if st["device_ms"] else None,
         "device_busy_frac": round(st["device_ms"] / 1e3 / wall, 3), "wall_s": round(wall, 1),
         "peak_active": st["peak_active"], "steps": st["steps"], "launches": st["launches"],
+        "passes_per_step": args.serve_passes,
         "peak_state_gb": round(st["peak_state_bytes"] / 1e9, 2),
         "config": {"sizes": SERVING["sizes"], "sources": SERVING["sources"], "iterations": SERVING["iterations"],
                    "window": "15x15", "stride": SERVING["stride"], "precision": "f16acc",
@@ -602,6 +607,10 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if world != args.gpus:
         print(f"warning: --gpus {args.gpus} but WORLD_SIZE {world}", file=sys.stderr)
+    if args.serve_only:
+        hp = importlib.import_module(PKG)
+        print(json.dumps({"serving": run_serving(args, hp, local_rank)}))
+        return
     if args.impl == "reference":
         line = run_reference(args, rank, world)
         if line:

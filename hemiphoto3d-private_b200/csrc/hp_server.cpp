@@ -528,7 +528,7 @@ void hp_server_options_default(hp_server_options* o) {
     o->max_active = 64;
     o->mem_fraction = 0.8f;
     o->mem_limit = 0;
-    o->passes_per_step = 4;
+    o->passes_per_step = 8;
     o->split_launches = 0;
     o->ctas_per_sm = 0;
     o->inflight_steps = 2;
@@ -548,7 +548,7 @@ hp_status hp_server_create(hp_ctx* ctx, const hp_params* params, const hp_server
         o = *options;
         if (o.max_active == 0) o.max_active = 64;
         if (o.mem_fraction == 0.f) o.mem_fraction = 0.8f;
-        if (o.passes_per_step == 0) o.passes_per_step = 4;
+        if (o.passes_per_step == 0) o.passes_per_step = 8;
         if (o.inflight_steps == 0) o.inflight_steps = 2;
         if (o.wait_limit_ms == 0) o.wait_limit_ms = 2000;
     }
