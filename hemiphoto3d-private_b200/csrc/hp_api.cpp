@@ -66,6 +66,9 @@ hp_status check_params(hp_ctx* ctx, const hp_params* p) {
         return fail(ctx, HP_ERR_INVALID_ARG, "refine_steps %d outside 0..4", p->refine_steps);
     if (!(p->iter_decay > 0.f && p->iter_decay <= 1.f) || !(p->step_decay > 0.f && p->step_decay <= 1.f))
         return fail(ctx, HP_ERR_INVALID_ARG, "decay factors must lie in (0, 1]");
+    if ((p->tile_w != 0 && p->tile_w != hp::TILE_W) || (p->tile_h != 0 && p->tile_h != hp::TILE_H))
+        return fail(ctx, HP_ERR_UNSUPPORTED, "tile %dx%d: the kernels use %dx%d tiles", p->tile_w, p->tile_h,
+                    hp::TILE_W, hp::TILE_H);
     return HP_OK;
 }
 

@@ -87,8 +87,8 @@ typedef struct hp_params {
     int refine_steps;    /* random perturbations per pixel visit, 0..4 */
     float iter_decay;    /* perturbation range factor per iteration */
     float step_decay;    /* perturbation range factor per refinement step */
-    int tile_w;          /* pixels per CTA row, 0 = engine choice (autotuned) */
-    int tile_h;          /* rows per CTA, 0 = engine choice */
+    int tile_w;          /* pixels per CTA row: 0 or 64 (the kernels' one tile shape: a warp per */
+    int tile_h;          /* row of 32 same-colour pixels, 8 rows); 0 or 8.  Others: HP_ERR_UNSUPPORTED */
     /* FP16-acc path only: bit s set = source s is sampled by the software
      * bilinear sampler (quad-packed FP16 texels, fixed-point weights, FP16
      * interpolation) instead of the texture unit.  The software sampler
