@@ -155,6 +155,7 @@ def _load() -> C.CDLL:
         "hp_ctx_profile_reset": (C.c_int, [C.c_void_p]),
         "hp_image_upload": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, P(C.c_int)]),
         "hp_image_release": (C.c_int, [C.c_void_p, C.c_int]),
+        "hp_ctx_set_image_cache": (C.c_int, [C.c_void_p, C.c_uint64]),
         "hp_image_size": (C.c_int, [C.c_void_p, C.c_int, P(C.c_int), P(C.c_int)]),
         "hp_setup_homographies": (C.c_int, [P(Camera), P(Camera), C.c_int, P(C.c_double), P(C.c_double)]),
         "hp_solve": (C.c_int, [C.c_void_p, P(Job), C.c_int, P(Params), P(Maps)]),
@@ -215,6 +216,7 @@ EXPORTS = (
     "hp_plan_get_info", "hp_plan_destroy", "hp_schedule_build", "hp_server_options_default", "hp_server_create",
     "hp_submit", "hp_poll", "hp_server_drain", "hp_server_stats_get", "hp_server_stats_reset",
     "hp_server_last_error", "hp_server_destroy", "hp_server_simulate", "hp_select_sources", "hp_project_seeds",
+    "hp_ctx_set_image_cache",
 )
 STATIC_MAX_PIXELS = 1280 * 1024  # HP_STATIC_MAX_PIXELS
 
@@ -315,6 +317,10 @@ class Context:
 
     def synchronize(self):
         self._check(lib.hp_ctx_synchronize(self._h), "hp_ctx_synchronize")
+
+    def set_image_cache(self, limit_bytes: int):
+        """Bytes of released images kept for reuse by later uploads of the same size (0: none)."""
+        self._check(lib.hp_ctx_set_image_cache(self._h, int(limit_bytes)), "hp_ctx_set_image_cache")
 
     def mem_info(self):
         f, t = C.c_size_t(), C.c_size_t()

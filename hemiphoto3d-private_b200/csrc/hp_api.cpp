@@ -325,6 +325,11 @@ hp_status launch_pass(hp_ctx* ctx, const hp::BatchList& bl, const hp_params* p, 
 
 namespace hpx {
 
+size_t image_bytes(const Image& im) {
+    const size_t px = static_cast<size_t>(im.W) * im.H;
+    return im.pitch32 * im.H + im.pitch16 * im.H + px * (sizeof(float) + sizeof(__half)) + im.quads.physical;
+}
+
 void free_image(Image& im) {
     if (im.tex32) cudaDestroyTextureObject(im.tex32);
     if (im.tex16) cudaDestroyTextureObject(im.tex16);
@@ -410,6 +415,8 @@ hp_status hp_ctx_destroy(hp_ctx* ctx) {
         DeviceGuard g(ctx->device);
         cudaStreamSynchronize(ctx->stream);
         for (auto& kv : ctx->images) free_image(kv.second);
+        for (auto& im : ctx->image_cache) free_image(im);
+        ctx->upload.release();
         ctx->state.release();
         ctx->descs.release();
         ctx->lists.release();
@@ -489,11 +496,7 @@ hp_status hp_image_upload(hp_ctx* ctx, const void* data, int memory, int width, 
     Image im;
     im.W = width;
     im.H = height;
-    void* raw = nullptr;
-    auto cleanup = [&]() {
-        if (raw && memory == HP_MEMORY_HOST) cudaFree(raw);
-        free_image(im);
-    };
+    auto cleanup = [&]() { free_image(im); };
     cudaError_t e;
 #define HP_UP(call)                                                                                   \
     do {                                                                                              \
@@ -506,34 +509,50 @@ hp_status hp_image_upload(hp_ctx* ctx, const void* data, int memory, int width, 
     } while (0)
     const void* src = data;
     if (memory == HP_MEMORY_HOST) {
-        HP_UP(cudaMalloc(&raw, bytes));
-        HP_UP(cudaMemcpyAsync(raw, data, bytes, cudaMemcpyHostToDevice, ctx->stream));
-        src = raw;
+        HP_UP(ctx->upload.ensure(bytes));
+        HP_UP(cudaMemcpyAsync(ctx->upload.p, data, bytes, cudaMemcpyHostToDevice, ctx->stream));
+        src = ctx->upload.p;
     }
-    HP_UP(cudaMallocPitch(reinterpret_cast<void**>(&im.f32), &im.pitch32, width * sizeof(float), height));
-    HP_UP(cudaMallocPitch(reinterpret_cast<void**>(&im.f16), &im.pitch16, width * sizeof(__half), height));
+    // A released image of the same size lends its buffers (and texture objects) to this one.
+    bool reused = false;
+    for (size_t k = 0; k < ctx->image_cache.size(); ++k) {
+        if (ctx->image_cache[k].W == width && ctx->image_cache[k].H == height) {
+            im = ctx->image_cache[k];
+            ctx->image_cache_bytes -= image_bytes(im);
+            ctx->image_cache.erase(ctx->image_cache.begin() + static_cast<long>(k));
+            reused = true;
+            break;
+        }
+    }
+    if (!reused) {
+        HP_UP(cudaMallocPitch(reinterpret_cast<void**>(&im.f32), &im.pitch32, width * sizeof(float), height));
+        HP_UP(cudaMallocPitch(reinterpret_cast<void**>(&im.f16), &im.pitch16, width * sizeof(__half), height));
+    }
     HP_UP(counted(ctx, HP_KERNEL_OTHER, [&] {
         return hp::launch_to_f32(src, dtype, width, height, im.f32, static_cast<int>(im.pitch32 / sizeof(float)),
                                  im.f16, static_cast<int>(im.pitch16 / sizeof(__half)), ctx->stream);
     }));
-    cudaChannelFormatDesc d32 = cudaCreateChannelDesc<float>();
-    cudaChannelFormatDesc d16 = cudaCreateChannelDescHalf();
-    HP_UP(cudaMallocArray(&im.arr32, &d32, width, height));
-    HP_UP(cudaMallocArray(&im.arr16, &d16, width, height));
+    if (!reused) {
+        cudaChannelFormatDesc d32 = cudaCreateChannelDesc<float>();
+        cudaChannelFormatDesc d16 = cudaCreateChannelDescHalf();
+        HP_UP(cudaMallocArray(&im.arr32, &d32, width, height));
+        HP_UP(cudaMallocArray(&im.arr16, &d16, width, height));
+    }
     HP_UP(cudaMemcpy2DToArrayAsync(im.arr32, 0, 0, im.f32, im.pitch32, width * sizeof(float), height,
                                    cudaMemcpyDeviceToDevice, ctx->stream));
     HP_UP(cudaMemcpy2DToArrayAsync(im.arr16, 0, 0, im.f16, im.pitch16, width * sizeof(__half), height,
                                    cudaMemcpyDeviceToDevice, ctx->stream));
-    HP_UP(alloc_quads(ctx->device, width, height, &im.quads));
+    if (!reused) HP_UP(alloc_quads(ctx->device, width, height, &im.quads));
     HP_UP(counted(ctx, HP_KERNEL_OTHER, [&] {
         return hp::launch_quads(im.f16, static_cast<int>(im.pitch16 / sizeof(__half)), width, height, im.quads.base,
                                 ctx->stream);
     }));
-    HP_UP(make_linear_texture(im.arr32, &im.tex32));
-    HP_UP(make_linear_texture(im.arr16, &im.tex16));
+    if (!reused) {
+        HP_UP(make_linear_texture(im.arr32, &im.tex32));
+        HP_UP(make_linear_texture(im.arr16, &im.tex16));
+    }
     HP_UP(cudaStreamSynchronize(ctx->stream));
 #undef HP_UP
-    if (raw && memory == HP_MEMORY_HOST) cudaFree(raw);
     int id = ctx->next_id++;
     ctx->images[id] = im;
     *image_id = id;
@@ -546,8 +565,32 @@ hp_status hp_image_release(hp_ctx* ctx, int image_id) {
     if (it == ctx->images.end()) return fail(ctx, HP_ERR_NOT_FOUND, "image_release: unknown image %d", image_id);
     DeviceGuard g(ctx->device);
     cudaStreamSynchronize(ctx->stream);
-    free_image(it->second);
+    // Keep it for reuse when the cache has room (evicting the oldest entries), else free it.
+    const size_t b = image_bytes(it->second);
+    while (!ctx->image_cache.empty() && ctx->image_cache_bytes + b > ctx->image_cache_limit) {
+        ctx->image_cache_bytes -= image_bytes(ctx->image_cache.front());
+        free_image(ctx->image_cache.front());
+        ctx->image_cache.erase(ctx->image_cache.begin());
+    }
+    if (b <= ctx->image_cache_limit) {
+        ctx->image_cache.push_back(it->second);
+        ctx->image_cache_bytes += b;
+    } else {
+        free_image(it->second);
+    }
     ctx->images.erase(it);
+    return HP_OK;
+}
+
+hp_status hp_ctx_set_image_cache(hp_ctx* ctx, uint64_t limit_bytes) {
+    if (!ctx) return HP_ERR_INVALID_ARG;
+    DeviceGuard g(ctx->device);
+    ctx->image_cache_limit = static_cast<size_t>(limit_bytes);
+    while (!ctx->image_cache.empty() && ctx->image_cache_bytes > ctx->image_cache_limit) {
+        ctx->image_cache_bytes -= image_bytes(ctx->image_cache.front());
+        free_image(ctx->image_cache.front());
+        ctx->image_cache.erase(ctx->image_cache.begin());
+    }
     return HP_OK;
 }
 

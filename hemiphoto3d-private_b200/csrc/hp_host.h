@@ -78,6 +78,13 @@ struct hp_ctx {
     hpx::DevBuf lists;   // active-view lists and tile prefixes
     hpx::DevBuf staging; // host-memory results pass through here
     hpx::DevBuf seedbuf; // SfM seeds of one job and their W*H index map
+    hpx::DevBuf upload;  // host images land here before conversion
+    // Released images kept for reuse by the next upload of the same size
+    // (their planes, arrays, texture objects and quad plane), oldest first,
+    // up to image_cache_limit bytes.
+    std::vector<hpx::Image> image_cache;
+    size_t image_cache_bytes = 0;
+    size_t image_cache_limit = size_t(4) << 30;
     // Profiler: launch counts always; with profiling on, CUDA events bracket
     // each launch and are read back at the next synchronisation point.
     bool profiling = false;
@@ -160,6 +167,8 @@ hp::SolveConsts consts_of(const hp_params* p);
 // Validate a job and fill the image/camera part of its descriptor.
 hp_status fill_desc(hp_ctx* ctx, const hp_job* j, int jobno, hp::ViewDesc* d);
 void free_image(Image& im);
+// Device bytes an image holds (planes, arrays, quad plane).
+size_t image_bytes(const Image& im);
 cudaError_t make_linear_texture(cudaArray_t arr, cudaTextureObject_t* tex);
 
 }  // namespace hpx

@@ -192,6 +192,14 @@ hp_status hp_ctx_profile_reset(hp_ctx* ctx);
 hp_status hp_image_upload(hp_ctx* ctx, const void* data, int memory, int width, int height,
                           int dtype, int* image_id);
 hp_status hp_image_release(hp_ctx* ctx, int image_id);
+/* Released images keep their device buffers (planes, texture arrays and
+ * objects, quad plane) in a per-context cache, up to limit_bytes (default
+ * 4 GiB, oldest evicted first), and the next upload of the same size reuses
+ * them instead of allocating: a stream of per-request uploads then costs
+ * copies and conversions only.  0 disables the cache and frees what it holds.
+ * No reference counterpart (the reference creates and destroys its textures
+ * on every call, patchmatch_mvs.cu:789-819). */
+hp_status hp_ctx_set_image_cache(hp_ctx* ctx, uint64_t limit_bytes);
 hp_status hp_image_size(hp_ctx* ctx, int image_id, int* width, int* height);
 
 /* FP64 homography setup, replacing eigenToGPUCamera + precomputeSourceViews

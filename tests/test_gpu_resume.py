@@ -61,6 +61,7 @@ def test_uploads_release_their_device_memory(hp, rctx, small_scene):
     import torch
     img = small_scene.views[0].image
     big = np.ascontiguousarray(np.resize(img, (1500, 2100)).astype(np.uint8))
+    rctx.set_image_cache(0)  # released images are freed, not kept for reuse
     rctx.synchronize()
     torch.cuda.synchronize()
     free0, _ = rctx.mem_info()
@@ -72,9 +73,50 @@ def test_uploads_release_their_device_memory(hp, rctx, small_scene):
             rctx.release(i)
         rctx.synchronize()
         assert abs(rctx.mem_info()[0] - free0) <= 64 << 20, (free0, rctx.mem_info()[0])
+    # With the cache on, released images are kept and the next uploads of that size take them over.
+    rctx.set_image_cache(4 << 30)
+    for i in [rctx.upload(big) for _ in range(8)]:
+        rctx.release(i)
+    kept = rctx.mem_info()[0]
+    assert free0 - kept >= 8 * big.size * 18
+    ids = [rctx.upload(big) for _ in range(8)]
+    assert rctx.mem_info()[0] >= kept - (16 << 20), "uploads of a cached size allocated new memory"
+    for i in ids:
+        rctx.release(i)
+    rctx.set_image_cache(0)
+    assert abs(rctx.mem_info()[0] - free0) <= 64 << 20
 
 
 def test_upload_size_limit(hp, rctx):
     """Image sides are capped at 16384 px (the software sampler's fixed-point coordinate range)."""
     with pytest.raises(hp.HpError):
         rctx.upload(np.zeros((2, 16385), np.uint8))
+
+
+def test_image_cache_reuse_gives_identical_results(hp, small_scene):
+    """Released images lend their buffers to later uploads of the same size; solves over reused buffers
+    (holding the same or different pixels) equal solves over fresh ones, and the cache stays bounded."""
+    s = small_scene
+    r, srcs = 0, s.sources[0]
+
+    def solve(ctx, ids):
+        job = hp.make_job(ids[r], [ids[i] for i in srcs], hp.make_camera(*cam_of(s, r)),
+                          [hp.make_camera(*cam_of(s, i)) for i in srcs], *s.depth_range, seed=3, view_id=r,
+                          iterations=3)
+        m, d, n, c = hp.host_maps(s.height, s.width)
+        ctx.solve([job], hp.default_params(radius=5, stride=2, precision=1), [m])
+        return d, c
+
+    with hp.Context(0) as fresh:
+        want = solve(fresh, [fresh.upload(v.image) for v in s.views])
+        flipped = [np.ascontiguousarray(v.image[:, ::-1]) for v in s.views]
+        want_flipped = solve(fresh, [fresh.upload(x) for x in flipped])
+    with hp.Context(0) as ctx:
+        ids = [ctx.upload(x) for x in flipped]
+        for i in ids:
+            ctx.release(i)  # cached
+        got = solve(ctx, [ctx.upload(v.image) for v in s.views])  # reuses the flipped images' buffers
+        assert all(np.array_equal(a, b) for a, b in zip(got, want))
+        ctx.set_image_cache(0)
+        got2 = solve(ctx, [ctx.upload(x) for x in flipped])
+        assert all(np.array_equal(a, b) for a, b in zip(got2, want_flipped))
