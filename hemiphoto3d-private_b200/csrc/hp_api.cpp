@@ -141,6 +141,38 @@ hp_status fill_desc(hp_ctx* ctx, const hp_job* j, int jobno, hp::ViewDesc* d) {
     return HP_OK;
 }
 
+hp_status check_seeds(hp_ctx* ctx, const hp_job* j, int jobno) {
+    if (j->num_seeds == 0) return HP_OK;
+    if (j->num_seeds < 0 || j->num_seeds > (1 << 26) || !j->seeds || j->seed_radius < 0 || j->seed_radius > 4096)
+        return fail(ctx, HP_ERR_INVALID_ARG, "job %d: seeds (%d, radius %d) invalid", jobno, j->num_seeds,
+                    j->seed_radius);
+    return HP_OK;
+}
+
+size_t seed_area_bytes(const hp_job* j, int W, int H) {
+    if (j->num_seeds <= 0) return 0;
+    auto a = [](size_t x) { return (x + 255) & ~size_t(255); };
+    return a(static_cast<size_t>(j->num_seeds) * sizeof(hp_seed)) + a(static_cast<size_t>(W) * H * sizeof(int));
+}
+
+cudaError_t stage_seeds(const hp_job* j, void* area, hp::ViewDesc* d, cudaStream_t st) {
+    d->seeds = nullptr;
+    d->seed_map = nullptr;
+    if (j->num_seeds <= 0) return cudaSuccess;
+    const size_t list = ((static_cast<size_t>(j->num_seeds) * sizeof(hp_seed)) + 255) & ~size_t(255);
+    hp_seed* seeds = static_cast<hp_seed*>(area);
+    int* map = reinterpret_cast<int*>(static_cast<char*>(area) + list);
+    // A pageable source: the copy has completed when the call returns.
+    cudaError_t e = cudaMemcpyAsync(seeds, j->seeds, static_cast<size_t>(j->num_seeds) * sizeof(hp_seed),
+                                    cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = hp::launch_seed_map(seeds, j->num_seeds, j->seed_radius, d->W, d->H, map, st);
+    if (e == cudaSuccess) {
+        d->seeds = seeds;
+        d->seed_map = map;
+    }
+    return e;
+}
+
 }  // namespace hpx
 
 namespace {
@@ -156,7 +188,7 @@ struct Prepared {
     int max_iter = 0;
 };
 
-hp_status prepare(hp_ctx* ctx, const hp_job* jobs, int n, Prepared* P) {
+hp_status prepare(hp_ctx* ctx, const hp_job* jobs, int n, Prepared* P, bool with_seeds = false) {
     P->host.resize(n);
     size_t state_bytes = 0;
     std::vector<size_t> offs(n);
@@ -174,6 +206,20 @@ hp_status prepare(hp_ctx* ctx, const hp_job* jobs, int n, Prepared* P) {
         size_t px = static_cast<size_t>(P->host[k].W) * P->host[k].H;
         P->host[k].hyp = reinterpret_cast<float4*>(base);
         P->host[k].cost = reinterpret_cast<float*>(base + px * sizeof(float4));
+    }
+    if (with_seeds) {  // SfM seed lists and index maps, read by the initialisation stage
+        size_t seed_bytes = 0;
+        for (int k = 0; k < n; ++k) {
+            hp_status st = check_seeds(ctx, &jobs[k], k);
+            if (st != HP_OK) return st;
+            seed_bytes += seed_area_bytes(&jobs[k], P->host[k].W, P->host[k].H);
+        }
+        if (seed_bytes) HP_CUDA(ctx->seedbuf.ensure(seed_bytes));
+        size_t off = 0;
+        for (int k = 0; k < n; ++k) {
+            HP_CUDA(stage_seeds(&jobs[k], static_cast<char*>(ctx->seedbuf.p) + off, &P->host[k], ctx->stream));
+            off += seed_area_bytes(&jobs[k], P->host[k].W, P->host[k].H);
+        }
     }
     HP_CUDA(ctx->descs.ensure(n * sizeof(hp::ViewDesc)));
     P->dev = static_cast<hp::ViewDesc*>(ctx->descs.p);
@@ -205,36 +251,6 @@ hp_status prepare(hp_ctx* ctx, const hp_job* jobs, int n, Prepared* P) {
     // The staging vectors above are pageable: the copies complete before return.
     HP_CUDA(cudaStreamSynchronize(ctx->stream));
     flush_profile(ctx);
-    return HP_OK;
-}
-
-// Seed fields of a job: none, or a host list with a sane radius.
-hp_status check_seeds(hp_ctx* ctx, const hp_job* j, int jobno) {
-    if (j->num_seeds == 0) return HP_OK;
-    if (j->num_seeds < 0 || j->num_seeds > (1 << 26) || !j->seeds || j->seed_radius < 0 || j->seed_radius > 4096)
-        return fail(ctx, HP_ERR_INVALID_ARG, "job %d: seeds (%d, radius %d) invalid", jobno, j->num_seeds,
-                    j->seed_radius);
-    return HP_OK;
-}
-
-// Paint every job's SfM seeds over its freshly initialised hypotheses
-// (runPatchMatchMVS, patchmatch_mvs.cu:1111-1177), one job at a time.
-hp_status apply_seeds(hp_ctx* ctx, const hp_job* jobs, int n, const Prepared& P) {
-    for (int k = 0; k < n; ++k) {
-        const hp_job& j = jobs[k];
-        if (j.num_seeds <= 0) continue;
-        const hp::ViewDesc& v = P.host[k];
-        const size_t seed_bytes = (static_cast<size_t>(j.num_seeds) * sizeof(hp_seed) + 255) & ~size_t(255);
-        HP_CUDA(ctx->seedbuf.ensure(seed_bytes + static_cast<size_t>(v.W) * v.H * sizeof(int)));
-        hp_seed* d_seeds = static_cast<hp_seed*>(ctx->seedbuf.p);
-        int* d_map = reinterpret_cast<int*>(static_cast<char*>(ctx->seedbuf.p) + seed_bytes);
-        // Pageable source: the copy is complete when the call returns, before the next job reuses the buffer.
-        HP_CUDA(cudaMemcpyAsync(d_seeds, j.seeds, static_cast<size_t>(j.num_seeds) * sizeof(hp_seed),
-                                cudaMemcpyHostToDevice, ctx->stream));
-        HP_CUDA(counted(ctx, HP_KERNEL_OTHER,
-                        [&] { return hp::launch_seed(v, d_seeds, j.num_seeds, j.seed_radius, d_map, ctx->stream); }));
-        HP_CUDA(cudaStreamSynchronize(ctx->stream));
-    }
     return HP_OK;
 }
 
@@ -634,14 +650,12 @@ hp_status hp_solve(hp_ctx* ctx, const hp_job* jobs, int num_jobs, const hp_param
     for (int k = 0; k < num_jobs; ++k) {
         if (!out[k].depth || !out[k].normal || !out[k].cost)
             return fail(ctx, HP_ERR_INVALID_ARG, "solve: output maps of job %d incomplete", k);
-        if ((st = check_seeds(ctx, &jobs[k], k)) != HP_OK) return st;
     }
     DeviceGuard g(ctx->device);
     Prepared P;
-    if ((st = prepare(ctx, jobs, num_jobs, &P)) != HP_OK) return st;
+    if ((st = prepare(ctx, jobs, num_jobs, &P, true)) != HP_OK) return st;
     hp::BatchList all = batch_of(P, 0);
     HP_CUDA(counted(ctx, HP_KERNEL_INIT, [&] { return hp::launch_init(all, ctx->stream); }));
-    if ((st = apply_seeds(ctx, jobs, num_jobs, P)) != HP_OK) return st;
     if ((st = launch_cost(ctx, all, params)) != HP_OK) return st;
     for (int it = 0; it < P.max_iter; ++it) {
         hp::BatchList bl = batch_of(P, 1 + it);
@@ -660,12 +674,10 @@ hp_status hp_init_hypotheses(hp_ctx* ctx, const hp_job* job, const hp_params* pa
     if (!job || !out || !out->depth || !out->normal) return fail(ctx, HP_ERR_INVALID_ARG, "init: null argument");
     hp_status st = check_params(ctx, params);
     if (st != HP_OK) return st;
-    if ((st = check_seeds(ctx, job, 0)) != HP_OK) return st;
     DeviceGuard g(ctx->device);
     Prepared P;
-    if ((st = prepare(ctx, job, 1, &P)) != HP_OK) return st;
+    if ((st = prepare(ctx, job, 1, &P, true)) != HP_OK) return st;
     HP_CUDA(counted(ctx, HP_KERNEL_INIT, [&] { return hp::launch_init(batch_of(P, 0), ctx->stream); }));
-    if ((st = apply_seeds(ctx, job, 1, P)) != HP_OK) return st;
     if ((st = export_maps(ctx, P, 0, out, true, false)) != HP_OK) return st;
     HP_CUDA(cudaStreamSynchronize(ctx->stream));
     flush_profile(ctx);

@@ -166,6 +166,12 @@ hp_status check_params(hp_ctx* ctx, const hp_params* p);
 hp::SolveConsts consts_of(const hp_params* p);
 // Validate a job and fill the image/camera part of its descriptor.
 hp_status fill_desc(hp_ctx* ctx, const hp_job* j, int jobno, hp::ViewDesc* d);
+// SfM seeds of a job: validation, the device bytes its seed list and W x H
+// index map take, and staging them (upload + map build on `st`) into `area`,
+// which sets d->seeds / d->seed_map (left null for a job without seeds).
+hp_status check_seeds(hp_ctx* ctx, const hp_job* j, int jobno);
+size_t seed_area_bytes(const hp_job* j, int W, int H);
+cudaError_t stage_seeds(const hp_job* j, void* area, hp::ViewDesc* d, cudaStream_t st);
 void free_image(Image& im);
 // Device bytes an image holds (planes, arrays, quad plane).
 size_t image_bytes(const Image& im);

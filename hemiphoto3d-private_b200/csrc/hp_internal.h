@@ -43,6 +43,10 @@ struct ViewDesc {
     float* out_depth;
     float* out_normal;
     float* out_cost;
+    // SfM seeding (null when the job has none): per pixel the index of the
+    // seed whose plane replaces the random initial one, -1 for none.
+    const int* seed_map;
+    const hp_seed* seeds;
 };
 
 // Solver constants for one launch.
@@ -129,10 +133,10 @@ cudaError_t launch_propagate_f16(const BatchList& bl, const SolveConsts& sc, int
                                  cudaStream_t st);
 // FP16 plane -> block-tiled software-sampler quad plane (see hpx::QuadPlane).
 cudaError_t launch_quads(const __half* src16, int pitch16, int W, int H, uint2* quads, cudaStream_t st);
-// SfM seeds (host list uploaded to `seeds`) painted over the view's hypotheses; `map` is
-// W*H ints of scratch.
-cudaError_t launch_seed(const ViewDesc& v, const hp_seed* seeds, int num_seeds, int radius, int* map,
-                        cudaStream_t st);
+// SfM seed index map of a W x H view: per pixel the last-listed of the (device) seeds whose
+// (2 radius + 1)^2 square covers it, -1 for none.
+cudaError_t launch_seed_map(const hp_seed* seeds, int num_seeds, int radius, int W, int H, int* map,
+                            cudaStream_t st);
 cudaError_t launch_unpack(const ViewDesc* views_host_copy, int view, float* depth, float* normal, float* cost,
                           cudaStream_t st);
 cudaError_t launch_pack(const ViewDesc* views_host_copy, int view, const float* depth, const float* normal,

@@ -321,8 +321,7 @@ hp_status hp_plan_create(hp_ctx* ctx, const hp_job* jobs, int num_jobs, const hp
     p->host.resize(num_jobs);
     p->out.assign(out, out + num_jobs);
     for (int k = 0; k < num_jobs; ++k) {
-        if (jobs[k].num_seeds != 0)
-            return fail(ctx, HP_ERR_UNSUPPORTED, "plan_create: job %d carries SfM seeds (use hp_solve)", k);
+        if ((st = check_seeds(ctx, &jobs[k], k)) != HP_OK) return st;
         if ((st = fill_desc(ctx, &jobs[k], k, &p->host[k])) != HP_OK) return st;
         p->iters.push_back(jobs[k].iterations);
         p->max_iter = std::max(p->max_iter, jobs[k].iterations);
@@ -375,6 +374,11 @@ hp_status hp_plan_create(hp_ctx* ctx, const hp_job* jobs, int num_jobs, const hp
         if (out[k].memory == HP_MEMORY_HOST)
             bytes = align256(bytes + static_cast<size_t>(p->host[k].W) * p->host[k].H * 5 * sizeof(float));
     }
+    std::vector<size_t> off_seed(num_jobs);  // SfM seed lists and index maps, built once here
+    for (int k = 0; k < num_jobs; ++k) {
+        off_seed[k] = bytes;
+        bytes = align256(bytes + seed_area_bytes(&jobs[k], p->host[k].W, p->host[k].H));
+    }
     const size_t off_desc = bytes;
     bytes = align256(bytes + num_jobs * sizeof(hp::ViewDesc));
     const size_t off_lists = bytes;
@@ -407,6 +411,9 @@ hp_status hp_plan_create(hp_ctx* ctx, const hp_job* jobs, int num_jobs, const hp
             v.out_cost = sd + 4 * px;
         }
     }
+    for (int k = 0; k < num_jobs; ++k)
+        HP_CUDA(stage_seeds(&jobs[k], base + off_seed[k], &p->host[k], ctx->stream));
+    HP_CUDA(cudaStreamSynchronize(ctx->stream));
     p->d_done = reinterpret_cast<int*>(base + off_flags);
     p->d_views = reinterpret_cast<hp::ViewDesc*>(base + off_desc);
     p->d_lists = reinterpret_cast<int*>(base + off_lists);

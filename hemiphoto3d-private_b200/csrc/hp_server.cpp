@@ -118,6 +118,8 @@ struct SrvReq {
     hp_maps out{};
     void* mem = nullptr;
     float* staging = nullptr;  // host outputs: depth, normal, cost on the device
+    std::vector<hp_seed> seeds;  // the job's SfM seeds, copied at submission
+    int seed_radius = 0;
     double pix_iter = 0.0;
     bool failed = false;
     Clock::time_point t_submit, t_admit;
@@ -192,12 +194,12 @@ uint64_t admission_budget(hp_server* s) {
     return b > 0 ? static_cast<uint64_t>(b) : 0;
 }
 
-uint64_t request_bytes(const hp::ViewDesc& d, bool host_out) {
+uint64_t request_bytes(const hp::ViewDesc& d, bool host_out, size_t seed_bytes) {
     const size_t px = static_cast<size_t>(d.W) * d.H;
     size_t b = align256(px * (sizeof(float4) + sizeof(float)));
     b = align256(b + static_cast<size_t>(d.tiles_x) * d.tiles_y * sizeof(int));
     if (host_out) b = align256(b + px * 5 * sizeof(float));
-    return b;
+    return align256(b + seed_bytes);
 }
 
 void complete(hp_server* s, SrvReq* r, int status, Clock::time_point now) {
@@ -247,6 +249,15 @@ cudaError_t materialise(hp_server* s, SrvReq* r) {
         v.out_depth = r->staging;
         v.out_normal = r->staging + px;
         v.out_cost = r->staging + 4 * px;
+        off = align256(off + px * 5 * sizeof(float));
+    }
+    if (!r->seeds.empty()) {  // SfM seed list and index map, read by the initialisation stage
+        hp_job sj{};
+        sj.seeds = r->seeds.data();
+        sj.num_seeds = static_cast<int>(r->seeds.size());
+        sj.seed_radius = r->seed_radius;
+        cudaError_t e = stage_seeds(&sj, base + off, &v, s->stream);
+        if (e != cudaSuccess) return e;
     }
     return cudaMemsetAsync(v.done, 0xff, flags, s->stream);  // -1: no stage finished
 }
@@ -625,7 +636,6 @@ hp_status hp_submit(hp_server* s, const hp_job* job, const hp_maps* out, uint64_
     };
     if (!job || !out || !request_id) return bad(HP_ERR_INVALID_ARG, "submit: null argument");
     if (!out->depth || !out->normal || !out->cost) return bad(HP_ERR_INVALID_ARG, "submit: output maps incomplete");
-    if (job->num_seeds != 0) return bad(HP_ERR_UNSUPPORTED, "submit: jobs with SfM seeds go through hp_solve");
     if (out->memory != HP_MEMORY_HOST && out->memory != HP_MEMORY_DEVICE)
         return bad(HP_ERR_INVALID_ARG, "submit: unknown memory kind");
     std::unique_ptr<SrvReq> r(new SrvReq);
@@ -635,15 +645,21 @@ hp_status hp_submit(hp_server* s, const hp_job* job, const hp_maps* out, uint64_
         return HP_ERR_CANCELLED;
     }
     // The context's images are read under the server lock (fill_desc reports through the context).
-    hp_status st = fill_desc(s->ctx, job, 0, &r->desc);
+    hp_status st = check_seeds(s->ctx, job, 0);
+    if (st == HP_OK) st = fill_desc(s->ctx, job, 0, &r->desc);
     if (st != HP_OK) {
         s->err = std::string("submit: ") + s->ctx->err;
         return st;
     }
+    if (job->num_seeds > 0) {
+        r->seeds.assign(job->seeds, job->seeds + job->num_seeds);
+        r->seed_radius = job->seed_radius;
+    }
     r->out = *out;
     r->core.tiles = r->desc.tiles_x * r->desc.tiles_y;
     r->core.stages = 2 * job->iterations + 2;
-    r->core.bytes = request_bytes(r->desc, out->memory == HP_MEMORY_HOST);
+    r->core.bytes = request_bytes(r->desc, out->memory == HP_MEMORY_HOST,
+                                  seed_area_bytes(job, r->desc.W, r->desc.H));
     r->core.user = r.get();
     r->pix_iter = static_cast<double>(r->desc.W) * r->desc.H * job->iterations;
     const uint64_t cap = s->opt.mem_limit ? s->opt.mem_limit

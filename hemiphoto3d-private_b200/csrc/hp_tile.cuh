@@ -11,6 +11,7 @@ namespace hp {
 // Initial hypotheses of one tile: depth uniform in [dmin, dmax]; normal from
 // theta in [0, 2pi) and cos(phi) in (0, 1), flipped to face the camera,
 // normalised (init_depth_normal_kernel, src/dense_recon/patchmatch_mvs.cu:164-216).
+// Pixels the view's SfM seed map covers take their seed's plane instead.
 // Every operation is explicitly rounded, so the result does not depend on the
 // including translation unit's flags (no intermediate is ever subnormal:
 // depths lie in [dmin, dmax] and normal components are at least ~1e-10).
@@ -22,6 +23,14 @@ __device__ __forceinline__ void tile_init(const ViewDesc* v, int tile_x, int til
         const int x = tile_x * TILE_W + j * 32 + lane;
         if (x >= v->W) continue;
         const uint32_t idx = static_cast<uint32_t>(y * v->W + x);
+        if (v->seed_map) {  // SfM seed (runPatchMatchMVS, patchmatch_mvs.cu:1111-1177)
+            const int k = v->seed_map[idx];
+            if (k >= 0) {
+                const hp_seed sd = v->seeds[k];
+                v->hyp[idx] = make_float4(sd.depth, sd.normal[0], sd.normal[1], sd.normal[2]);
+                continue;
+            }
+        }
         const uint4 r = philox4x32_10(make_uint4(idx, v->view_id, 0u, 0u), v->seed_lo, v->seed_hi);
         const float depth = __fmaf_rn(u01(r.x), __fsub_rn(v->dmax, v->dmin), v->dmin);
         const float3 ray = view_ray(v->kinv, x, y);

@@ -73,9 +73,10 @@ __global__ void quads_kernel(const __half* __restrict__ src, int pitch16, int W,
     }
 }
 
-// SfM seeding, pass 1: for every pixel, the largest index of a seed whose
-// (2r+1)^2 square covers it (atomicMax keeps the last-listed seed, as painting
-// the squares in list order would).  One CTA per seed.
+// SfM seeding: for every pixel, the largest index of a seed whose (2r+1)^2
+// square covers it (atomicMax keeps the last-listed seed, as painting the
+// squares in list order would).  One CTA per seed.  The initialisation stage
+// (tile_init) then takes the seed's plane instead of a random one.
 __global__ void seed_map_kernel(const hp_seed* __restrict__ seeds, int radius, int W, int H, int* __restrict__ map) {
     const int k = blockIdx.x;
     const hp_seed s = seeds[k];
@@ -88,17 +89,6 @@ __global__ void seed_map_kernel(const hp_seed* __restrict__ seeds, int radius, i
     }
 }
 
-// Pass 2: covered pixels take their seed's plane.
-__global__ void seed_fill_kernel(const hp_seed* __restrict__ seeds, const int* __restrict__ map, size_t n,
-                                 float4* __restrict__ hyp) {
-    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
-         i += static_cast<size_t>(gridDim.x) * blockDim.x) {
-        const int k = map[i];
-        if (k < 0) continue;
-        const hp_seed s = seeds[k];
-        hyp[i] = make_float4(s.depth, s.normal[0], s.normal[1], s.normal[2]);
-    }
-}
 
 __global__ void unpack_kernel(const float4* __restrict__ hyp, const float* __restrict__ cost_in, size_t n,
                               float* __restrict__ depth, float* __restrict__ normal, float* __restrict__ cost) {
@@ -138,15 +128,12 @@ cudaError_t launch_quads(const __half* src16, int pitch16, int W, int H, uint2* 
     return cudaGetLastError();
 }
 
-cudaError_t launch_seed(const ViewDesc& v, const hp_seed* seeds, int num_seeds, int radius, int* map,
-                        cudaStream_t st) {
-    if (num_seeds <= 0) return cudaSuccess;
-    const size_t n = static_cast<size_t>(v.W) * v.H;
+cudaError_t launch_seed_map(const hp_seed* seeds, int num_seeds, int radius, int W, int H, int* map,
+                            cudaStream_t st) {
+    const size_t n = static_cast<size_t>(W) * H;
     cudaError_t e = cudaMemsetAsync(map, 0xff, n * sizeof(int), st);
-    if (e != cudaSuccess) return e;
-    seed_map_kernel<<<num_seeds, 256, 0, st>>>(seeds, radius, v.W, v.H, map);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    seed_fill_kernel<<<stream_grid(), 256, 0, st>>>(seeds, map, n, v.hyp);
+    if (e != cudaSuccess || num_seeds <= 0) return e;
+    seed_map_kernel<<<num_seeds, 256, 0, st>>>(seeds, radius, W, H, map);
     return cudaGetLastError();
 }
 

@@ -130,8 +130,8 @@ typedef struct hp_job {
      * of a seed's pixel takes that seed's depth and normal; where squares
      * overlap, the seed listed last wins.  Host memory, num_seeds records, as
      * hp_project_seeds makes them; NULL / 0 for none.  The reference's radius
-     * is 50.  hp_solve and hp_init_hypotheses apply seeds; plans and the
-     * server refuse jobs that carry them (HP_ERR_UNSUPPORTED). */
+     * is 50.  hp_solve, hp_init_hypotheses, plans and the server apply them
+     * (the list is copied; it need not outlive the call). */
     const hp_seed* seeds;
     int num_seeds;
     int seed_radius;

@@ -162,3 +162,43 @@ def test_seeded_stage_matches_reference(hp, scene_mod, small_scene):
             covered_total += int(mask.sum())
             assert np.array_equal(d[mask], rd[mask]) and np.array_equal(n[mask], rn[mask]), r
     assert covered_total > 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [0, 1])
+def test_seeded_jobs_in_plans_and_server_match_solve(hp, scene_mod, small_scene, precision):
+    """Seeded jobs give the same maps through hp_solve, a plan (both schedules) and the server."""
+    s = small_scene
+    cams = [(v.cam.K, v.cam.R, v.cam.t) for v in s.views]
+    pos, tracks = scene_mod.sparse_points(s, n=300, seed=8)
+    P = hp.SfmPoints(pos, tracks)
+    params = hp.default_params(radius=5, stride=2, precision=precision)
+    with hp.Context(0) as ctx:
+        ids = [ctx.upload(v.image) for v in s.views]
+        jobs = []
+        for r in (0, 3):
+            srcs = s.sources[r]
+            job = hp.make_job(ids[r], [ids[i] for i in srcs], hp.make_camera(*cams[r]),
+                              [hp.make_camera(*cams[i]) for i in srcs], *s.depth_range, seed=5, view_id=r,
+                              iterations=3)
+            jobs.append(hp.with_seeds(job, hp.project_seeds(hp.make_camera(*cams[r]), r, *s.depth_range, P), 20))
+        want = []
+        for j in jobs:
+            m, d, n, c = hp.host_maps(s.height, s.width)
+            ctx.solve([j], params, [m])
+            want.append((d, n, c))
+        for sched in (hp.SCHEDULE_PER_PASS, hp.SCHEDULE_PERSISTENT):
+            outs = [hp.host_maps(s.height, s.width) for _ in jobs]
+            with hp.Plan(ctx, jobs, params, [o[0] for o in outs], hp.plan_options(schedule=sched)) as plan:
+                plan.run()
+            for (_, d, n, c), (wd, wn, wc) in zip(outs, want):
+                assert np.array_equal(d, wd) and np.array_equal(n, wn) and np.array_equal(c, wc), sched
+        outs = [hp.host_maps(s.height, s.width) for _ in jobs]
+        with hp.Server(ctx, params, passes_per_step=3) as srv:
+            for j, o in zip(jobs, outs):
+                srv.submit(j, o[0])
+            srv.drain(timeout_ms=60000)
+            done = srv.poll(capacity=8)
+        assert len(done) == 2 and all(c["status"] == 0 for c in done)
+        for (_, d, n, c), (wd, wn, wc) in zip(outs, want):
+            assert np.array_equal(d, wd) and np.array_equal(n, wn) and np.array_equal(c, wc)
