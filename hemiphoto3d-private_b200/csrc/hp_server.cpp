@@ -278,6 +278,8 @@ bool enqueue_step(hp_server* s) {
         if (e != cudaSuccess) {
             s->core.drop(c);
             cudaGetLastError();
+            if (r->mem) cudaFreeAsync(r->mem, s->stream);  // allocated, then a later set-up step failed
+            r->mem = nullptr;
             set_err(s, "server: state allocation", e);
             complete(s, r, e == cudaErrorMemoryAllocation ? HP_ERR_OUT_OF_MEMORY : HP_ERR_CUDA, Clock::now());
         }
