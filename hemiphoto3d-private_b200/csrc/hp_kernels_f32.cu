@@ -117,6 +117,35 @@ __device__ __forceinline__ float cost_f32(const float* __restrict__ s_ref, int t
         const cudaTextureObject_t tex = v->src_tex[s];
         float sum_ref = 0.0f, sum_src = 0.0f, sum_ref2 = 0.0f, sum_src2 = 0.0f, sum_rs = 0.0f;
         int count = 0;
+        // A window whose warp lies wholly beyond one edge of the source has no
+        // valid tap, so the reference's count rule gives 2 for this source:
+        // skip its taps.  The test runs on the plane-induced homography
+        // H = A + b (K^-T n)^T / (n.P) at the window's corners, in front of
+        // the camera (w_z > 1e-6, so the warped window is the convex quad of
+        // its corners) and past the edge by 0.25 px, far above the rounding
+        // differences between this and the per-tap arithmetic below.
+        {
+            const float m0 = nK0 * inv_n_dot_P, m1 = nK1 * inv_n_dot_P, m2 = nK2 * inv_n_dot_P;
+            const float hz0 = fmaf(b2, m0, a6), hz1 = fmaf(b2, m1, a7), hz2 = fmaf(b2, m2, a8);
+            const float hx0 = fmaf(b0, m0, a0), hx1 = fmaf(b0, m1, a1), hx2 = fmaf(b0, m2, a2);
+            const float hy0 = fmaf(b1, m0, a3), hy1 = fmaf(b1, m1, a4), hy2 = fmaf(b1, m2, a5);
+            bool front = true, left = true, right = true, top_ = true, bottom = true;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const float px = fx + static_cast<float>((c & 1) ? (SIDE - 1) * ST - R : -R);
+                const float py = fy + static_cast<float>((c & 2) ? (SIDE - 1) * ST - R : -R);
+                const float wz = fmaf(hz0, px, fmaf(hz1, py, hz2));
+                const float wx = fmaf(hx0, px, fmaf(hx1, py, hx2));
+                const float wy = fmaf(hy0, px, fmaf(hy1, py, hy2));
+                front = front && wz > 1e-6f;
+                left = left && wx < -0.25f * wz;
+                right = right && wx >= (fw1 + 0.25f) * wz;
+                top_ = top_ && wy < -0.25f * wz;
+                bottom = bottom && wy >= (fh1 + 0.25f) * wz;
+            }
+            // Cost 2 would change nothing in the running top-3 (every entry is <= 2).
+            if (front && (left || right || top_ || bottom)) continue;
+        }
 #pragma unroll 1
         for (int i = 0; i < SIDE; ++i) {
             const float wpy = fy + static_cast<float>(i * ST - R);
