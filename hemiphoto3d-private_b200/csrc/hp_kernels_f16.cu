@@ -195,8 +195,10 @@ __device__ __forceinline__ float source_cost(const Plane& P, cudaTextureObject_t
 #pragma unroll 1
     for (int i = 0; i < SIDE; ++i) {
         const float py = __fadd_rn(sy0, static_cast<float>(i * ST));
-        float wx = __fmaf_rn(P.h[1], py, rx0);
-        float wy = __fmaf_rn(P.h[4], py, rx1);
+        // (w_x, w_y) advance as a pair: sm_100's paired FP32 instructions round
+        // each element as the scalar ones do, so the bits are the same.
+        const float2 wxy0 = __ffma2_rn(make_float2(P.h[1], P.h[4]), make_float2(py, py), make_float2(rx0, rx1));
+        float wx = wxy0.x, wy = wxy0.y;
         float wz = __fmaf_rn(P.h[7], py, rx2);
         unsigned ok = (1u << SIDE) - 1u;
         __half2 a1 = __float2half2_rn(0.f), a2 = a1, a3 = a1, a4 = a1, a5 = a1;
@@ -244,10 +246,13 @@ __device__ __forceinline__ float source_cost(const Plane& P, cudaTextureObject_t
                     const int j = 4 * ch + jj;
                     if (j >= SIDE) break;
                     const float iz = rcp_approx(wz);
-                    unsigned bu = __float_as_uint(__fmaf_rn(wx, iz, SOFT_MAGIC));
-                    unsigned bv = __float_as_uint(__fmaf_rn(wy, iz, SOFT_MAGIC));
+                    const float2 wxy = make_float2(wx, wy), izz = make_float2(iz, iz);
+                    const float2 fxy = __ffma2_rn(wxy, izz, make_float2(SOFT_MAGIC, SOFT_MAGIC));
+                    unsigned bu = __float_as_uint(fxy.x);
+                    unsigned bv = __float_as_uint(fxy.y);
                     if constexpr (CHECK) {
-                        const float u = __fmul_rn(wx, iz), v = __fmul_rn(wy, iz);
+                        const float2 uv = __fmul2_rn(wxy, izz);
+                        const float u = uv.x, v = uv.y;
                         const bool skip = fabsf(wz) < 1e-8f || !(u >= LO) || !(u < fW - 1.0f + LO) || !(v >= LO) ||
                                           !(v < fH - 1.0f + LO);
                         ok &= ~(static_cast<unsigned>(skip) << j);
@@ -256,8 +261,9 @@ __device__ __forceinline__ float source_cost(const Plane& P, cudaTextureObject_t
                     }
                     wb[jj] = __byte_perm(bu, bv, 0x7430);
                     q[jj] = __ldg(qbase + soft_offset(bu, bv));
-                    wx = __fadd_rn(wx, hx0);
-                    wy = __fadd_rn(wy, hx1);
+                    const float2 next = __fadd2_rn(wxy, make_float2(hx0, hx1));
+                    wx = next.x;
+                    wy = next.y;
                     wz = __fadd_rn(wz, hx2);
                 }
 #pragma unroll
