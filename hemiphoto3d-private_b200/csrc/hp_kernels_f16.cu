@@ -67,11 +67,19 @@ struct Win {
     static constexpr int SIDE = (2 * R) / ST + 1;
     static constexpr int N = SIDE * SIDE;
     static constexpr int PAIRS = (SIDE + 1) / 2;  // half2 per row (the last may be half empty)
-    static constexpr bool IN_SMEM = SIDE * PAIRS <= 32;
+    static constexpr int VEC = PAIRS <= 1 ? 1 : (PAIRS <= 2 ? 2 : 4);  // a row's pairs, padded, in one load
+    static constexpr bool IN_SMEM = PAIRS <= 4 && SIDE * VEC <= 32;
 };
+template <int V> struct WinRow;
+template <> struct WinRow<1> { using T = unsigned; };
+template <> struct WinRow<2> { using T = uint2; };
+template <> struct WinRow<4> { using T = uint4; };
 constexpr int WIN_PAIRS_MAX = 32;
 
-// Per-pixel window statistics; the mean-subtracted window itself goes to s_win.
+// Per-pixel window statistics; the mean-subtracted window itself goes to s_win,
+// laid out [row][thread][VEC half2]: one row of a pixel's residual pairs is one
+// vector load (16 bytes for 7 or 8 taps a row), and the lanes of a warp read
+// consecutive vectors.
 struct RefStats {
     float mean;  // window mean (the shift of every sum)
     float ssd;   // sum (r - mean)^2
@@ -97,14 +105,21 @@ __device__ __forceinline__ RefStats load_window(__half2* s_win, const float* s_r
     if constexpr (Win<R, ST>::IN_SMEM) {
         constexpr int PAIRS = Win<R, ST>::PAIRS;
 #pragma unroll 1
-        for (int i = 0; i < SIDE; ++i)
+        for (int i = 0; i < SIDE; ++i) {
+            constexpr int VEC = Win<R, ST>::VEC;
+            unsigned rw[VEC] = {};
 #pragma unroll
             for (int p = 0; p < PAIRS; ++p) {
                 const float a = __fsub_rn(s_ref[(ly + i * ST) * tw + lx + (2 * p) * ST], mean);
                 const float b =
                     (2 * p + 1 < SIDE) ? __fsub_rn(s_ref[(ly + i * ST) * tw + lx + (2 * p + 1) * ST], mean) : 0.f;
-                s_win[(i * PAIRS + p) * CTA_THREADS + threadIdx.x] = __floats2half2_rn(a, b);
+                const __half2 h = __floats2half2_rn(a, b);
+                memcpy(&rw[p], &h, sizeof h);
             }
+            typename WinRow<VEC>::T row;
+            memcpy(&row, rw, sizeof row);
+            *reinterpret_cast<typename WinRow<VEC>::T*>(s_win + (i * CTA_THREADS + threadIdx.x) * VEC) = row;
+        }
     }
     return RefStats{mean, ssd};
 }
@@ -201,12 +216,18 @@ __device__ __forceinline__ float source_cost(const Plane& P, cudaTextureObject_t
         float wx = wxy0.x, wy = wxy0.y;
         float wz = __fmaf_rn(P.h[7], py, rx2);
         unsigned ok = (1u << SIDE) - 1u;
-        __half2 a1 = __float2half2_rn(0.f), a2 = a1, a3 = a1, a4 = a1, a5 = a1;
+        constexpr int VEC = Win<R, ST>::VEC;
+        unsigned rw[VEC];
+        if constexpr (Win<R, ST>::IN_SMEM) {  // the row's reference residuals, one load
+            const auto row = *reinterpret_cast<const typename WinRow<VEC>::T*>(s_win + i * CTA_THREADS * VEC);
+            memcpy(rw, &row, sizeof row);
+        }
+        __half2 a1, a2, a3, a4, a5;  // set by the row's first pair
         // Folds the residual pair of taps (2p, 2p + 1) into the row sums.
         auto accumulate = [&](int p, __half2 e) {
             __half2 rq;
             if constexpr (Win<R, ST>::IN_SMEM) {
-                rq = s_win[(i * PAIRS + p) * CTA_THREADS];  // s_win points at the pixel's column
+                memcpy(&rq, &rw[p], sizeof rq);
             } else {
                 const float* row = s_ref + (ly + i * ST) * tw + lx;
                 const float ra = __fsub_rn(row[(2 * p) * ST], c0);
@@ -226,12 +247,22 @@ __device__ __forceinline__ float source_cost(const Plane& P, cudaTextureObject_t
                 bits &= m;
                 memcpy(&e, &bits, sizeof bits);
             }
-            a1 = __hadd2(a1, e);
-            a2 = __hfma2(e, e, a2);
-            a3 = __hfma2(rq, e, a3);
-            if constexpr (CHECK) {
-                a4 = __hadd2(a4, rq);
-                a5 = __hfma2(rq, rq, a5);
+            if (p == 0) {
+                a1 = e;
+                a2 = __hmul2(e, e);
+                a3 = __hmul2(rq, e);
+                if constexpr (CHECK) {
+                    a4 = rq;
+                    a5 = __hmul2(rq, rq);
+                }
+            } else {
+                a1 = __hadd2(a1, e);
+                a2 = __hfma2(e, e, a2);
+                a3 = __hfma2(rq, e, a3);
+                if constexpr (CHECK) {
+                    a4 = __hadd2(a4, rq);
+                    a5 = __hfma2(rq, rq, a5);
+                }
             }
         };
         if constexpr (SOFT) {
@@ -471,7 +502,7 @@ __device__ __forceinline__ void tile_cost16(const ViewDesc* v, int tile_x, int t
         const RefStats st = load_window<R, ST>(s_win, s_ref, tw, lx, ly);
         const size_t idx = static_cast<size_t>(y) * v->W + x;
         const float4 h = v->hyp[idx];
-        v->cost[idx] = cost_f16<R, ST>(st, s_win + threadIdx.x, s_ref, tw, lx, ly, x, y, h.x, h.y, h.z, h.w, v,
+        v->cost[idx] = cost_f16<R, ST>(st, s_win + threadIdx.x * Win<R, ST>::VEC, s_ref, tw, lx, ly, x, y, h.x, h.y, h.z, h.w, v,
                                        sc.top_k, sc.soft_mask);
     }
 }
@@ -479,7 +510,7 @@ __device__ __forceinline__ void tile_cost16(const ViewDesc* v, int tile_x, int t
 template <int R, int ST>
 __global__ void __launch_bounds__(CTA_THREADS, HP_F16_MIN_BLOCKS) cost16_kernel(BatchList bl, SolveConsts sc) {
     __shared__ float s_ref[MAX_TW * MAX_TH];
-    __shared__ __half2 s_win[Win<R, ST>::IN_SMEM ? WIN_PAIRS_MAX * CTA_THREADS : 1];
+    __shared__ __align__(16) __half2 s_win[Win<R, ST>::IN_SMEM ? WIN_PAIRS_MAX * CTA_THREADS : 1];
     int tile_x, tile_y;
     const ViewDesc* v = locate_tile16(bl, blockIdx.x, &tile_x, &tile_y);
     tile_cost16<R, ST>(v, tile_x, tile_y, sc, s_ref, s_win);
@@ -580,7 +611,7 @@ __device__ __forceinline__ void tile_propagate16(const ViewDesc* v, int tile_x, 
             const int nxp = ox + (cand == 0 ? -1 : (cand == 1 ? 1 : 0));
             const int nyp = oy + (cand == 2 ? -1 : (cand == 3 ? 1 : 0));
             const float4 h = v->hyp[static_cast<size_t>(nyp) * W + nxp];
-            sm.cost[oly][item & 127] = cost_f16<R, ST>(RefStats{os.x, os.y}, s_win + oly * 32 + owner, s_ref, tw,
+            sm.cost[oly][item & 127] = cost_f16<R, ST>(RefStats{os.x, os.y}, s_win + (oly * 32 + owner) * Win<R, ST>::VEC, s_ref, tw,
                                                        olx, oly, ox, oy, h.x, h.y, h.z, h.w, v, sc.top_k,
                                                        sc.soft_mask);
         }
@@ -617,7 +648,7 @@ __device__ __forceinline__ void tile_propagate16(const ViewDesc* v, int tile_x, 
         const float cz = __fmaf_rn(__fmaf_rn(u01(rr.w), 2.0f, -1.0f), nrange, best.w);
         float3 cn = normalize3_rn(cx, cy, cz);
         if (dot3_rn(cn, ray) > 0.0f) cn = make_float3(-cn.x, -cn.y, -cn.z);
-        const float c = cost_f16<R, ST>(st, s_win + threadIdx.x, s_ref, tw, lx, ly, x, y, cd, cn.x, cn.y, cn.z, v,
+        const float c = cost_f16<R, ST>(st, s_win + threadIdx.x * Win<R, ST>::VEC, s_ref, tw, lx, ly, x, y, cd, cn.x, cn.y, cn.z, v,
                                         sc.top_k, sc.soft_mask);
         if (c < best_cost) {
             best_cost = c;
@@ -634,7 +665,7 @@ template <int R, int ST>
 __global__ void __launch_bounds__(CTA_THREADS, HP_F16_MIN_BLOCKS) propagate16_kernel(BatchList bl, SolveConsts sc,
                                                                                      int iteration, int color) {
     __shared__ float s_ref[MAX_TW * MAX_TH];
-    __shared__ __half2 s_win[Win<R, ST>::IN_SMEM ? WIN_PAIRS_MAX * CTA_THREADS : 1];
+    __shared__ __align__(16) __half2 s_win[Win<R, ST>::IN_SMEM ? WIN_PAIRS_MAX * CTA_THREADS : 1];
     __shared__ PassSmem sm;
     int tile_x, tile_y;
     const ViewDesc* v = locate_tile16(bl, blockIdx.x, &tile_x, &tile_y);
@@ -646,7 +677,7 @@ __global__ void __launch_bounds__(CTA_THREADS, HP_F16_MIN_BLOCKS) propagate16_ke
 template <int R, int ST>
 __global__ void __launch_bounds__(CTA_THREADS, HP_F16_MIN_BLOCKS) persistent16_kernel(Schedule s) {
     __shared__ float s_ref[MAX_TW * MAX_TH];
-    __shared__ __half2 s_win[Win<R, ST>::IN_SMEM ? WIN_PAIRS_MAX * CTA_THREADS : 1];
+    __shared__ __align__(16) __half2 s_win[Win<R, ST>::IN_SMEM ? WIN_PAIRS_MAX * CTA_THREADS : 1];
     __shared__ PassSmem sm;
     __shared__ int s_ticket;
     for (;;) {
