@@ -14,8 +14,8 @@
 //    (the warp of a rectangle with one-signed depth is the convex quad of its
 //    corners) every tap is valid and the per-tap bounds tests are skipped.
 //  - The reference window is mean-subtracted per pixel once per visit and kept
-//    in shared memory as half2 pairs ([pair][thread], conflict-free) for
-//    windows of up to 64 taps.  Window sums use mean-shifted values
+//    in shared memory as half2 pairs ([row][thread][pairs], one vector load a
+//    row) for windows of up to 64 taps.  Window sums use mean-shifted values
 //    (compensated variance): FP16 products and per-row FP16 partial sums,
 //    flushed into FP32 accumulators every row.
 //  - Windows touching the source border mask invalid taps per the
@@ -679,26 +679,28 @@ __global__ void __launch_bounds__(CTA_THREADS, HP_F16_MIN_BLOCKS) persistent16_k
     __shared__ float s_ref[MAX_TW * MAX_TH];
     __shared__ __align__(16) __half2 s_win[Win<R, ST>::IN_SMEM ? WIN_PAIRS_MAX * CTA_THREADS : 1];
     __shared__ PassSmem sm;
-    __shared__ int s_ticket;
+    // The claimed tile lives in shared memory: thread 0 decodes it once and
+    // publishes it after the stage, so no thread carries it through the body.
+    __shared__ SchedTile s_tile;
+    __shared__ int s_ok;
     for (;;) {
-        if (threadIdx.x == 0) s_ticket = sched_next(s);
+        if (threadIdx.x == 0) s_ok = sched_claim(s, &s_tile);
         __syncthreads();
-        const int ticket = s_ticket;
-        if (ticket < 0) break;
-        const SchedTile t = decode_ticket(s, ticket);
-        const ViewDesc* v = t.v;
-        if (t.stage == 0) {
-            tile_init(v, t.tx, t.ty);
+        if (!s_ok) break;
+        const ViewDesc* v = s_tile.v;
+        const int stage = s_tile.stage, tx = s_tile.tx, ty = s_tile.ty;
+        if (stage == 0) {
+            tile_init(v, tx, ty);
             __syncthreads();
-            tile_cost16<R, ST>(v, t.tx, t.ty, s.sc, s_ref, s_win);
-        } else if (t.stage <= 2 * v->iterations) {
-            const int k = t.stage - 1;
-            tile_propagate16<R, ST>(v, t.tx, t.ty, s.sc, k >> 1, k & 1, s_ref, s_win, sm);
+            tile_cost16<R, ST>(v, tx, ty, s.sc, s_ref, s_win);
+        } else if (stage <= 2 * v->iterations) {
+            const int k = stage - 1;
+            tile_propagate16<R, ST>(v, tx, ty, s.sc, k >> 1, k & 1, s_ref, s_win, sm);
         } else {
-            tile_unpack(v, t.tx, t.ty);
+            tile_unpack(v, tx, ty);
         }
         __syncthreads();
-        if (threadIdx.x == 0) sched_publish(s, t);
+        if (threadIdx.x == 0) sched_publish(s, s_tile);
     }
 }
 

@@ -427,26 +427,28 @@ template <int R, int ST>
 __global__ void __launch_bounds__(CTA_THREADS, HP_F32_MIN_BLOCKS) persistent_kernel(Schedule s) {
     __shared__ float s_ref[MAX_TW * MAX_TH];
     __shared__ PassSmem sm;
-    __shared__ int s_ticket;
+    // The claimed tile lives in shared memory: thread 0 decodes it once and
+    // publishes it after the stage, so no thread carries it through the body.
+    __shared__ SchedTile s_tile;
+    __shared__ int s_ok;
     for (;;) {
-        if (threadIdx.x == 0) s_ticket = sched_next(s);
+        if (threadIdx.x == 0) s_ok = sched_claim(s, &s_tile);
         __syncthreads();
-        const int ticket = s_ticket;
-        if (ticket < 0) break;
-        const SchedTile t = decode_ticket(s, ticket);
-        const ViewDesc* v = t.v;
-        if (t.stage == 0) {
-            tile_init(v, t.tx, t.ty);
+        if (!s_ok) break;
+        const ViewDesc* v = s_tile.v;
+        const int stage = s_tile.stage, tx = s_tile.tx, ty = s_tile.ty;
+        if (stage == 0) {
+            tile_init(v, tx, ty);
             __syncthreads();
-            tile_cost<R, ST>(v, t.tx, t.ty, s.sc, s_ref);
-        } else if (t.stage <= 2 * v->iterations) {
-            const int k = t.stage - 1;
-            tile_propagate<R, ST>(v, t.tx, t.ty, s.sc, k >> 1, k & 1, s_ref, sm);
+            tile_cost<R, ST>(v, tx, ty, s.sc, s_ref);
+        } else if (stage <= 2 * v->iterations) {
+            const int k = stage - 1;
+            tile_propagate<R, ST>(v, tx, ty, s.sc, k >> 1, k & 1, s_ref, sm);
         } else {
-            tile_unpack(v, t.tx, t.ty);
+            tile_unpack(v, tx, ty);
         }
         __syncthreads();
-        if (threadIdx.x == 0) sched_publish(s, t);
+        if (threadIdx.x == 0) sched_publish(s, s_tile);
     }
 }
 

@@ -158,13 +158,17 @@ __device__ __forceinline__ void sched_publish(const Schedule& s, const SchedTile
     st_release_gpu(t.v->done + t.tile, t.stage);
 }
 
-// Thread 0: the CTA's next ticket, or -1 when the schedule is exhausted or
-// aborted (including a dependency wait of this ticket that ran out).
-__device__ __forceinline__ int sched_next(const Schedule& s) {
-    if (ld_relaxed_gpu(s.status + 1)) return -1;
+// Thread 0: claims the CTA's next ticket and decodes it into *out; false when
+// the schedule is exhausted or aborted (including a dependency wait of this
+// ticket that ran out).
+__device__ __forceinline__ bool sched_claim(const Schedule& s, SchedTile* out) {
+    if (ld_relaxed_gpu(s.status + 1)) return false;
     const int t = static_cast<int>(atomicAdd(s.counter, 1u));
-    if (t >= s.total) return -1;
-    return sched_wait(s, decode_ticket(s, t)) ? t : -1;
+    if (t >= s.total) return false;
+    const SchedTile d = decode_ticket(s, t);
+    if (!sched_wait(s, d)) return false;
+    *out = d;
+    return true;
 }
 
 }  // namespace hp
