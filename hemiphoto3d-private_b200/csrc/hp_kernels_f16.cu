@@ -132,6 +132,15 @@ __device__ __forceinline__ float rcp_approx(float x) {
     return r;
 }
 
+// Row flush: s + x + y for the FP16 pair (x, y), each add rounded to FP32.
+// sm_100's mixed-precision add takes the FP16 operand directly, so the flush
+// needs no conversions (two instructions instead of four).
+__device__ __forceinline__ float add_pair(float s, __half2 a) {
+    asm("add.rn.f32.f16 %0, %1, %0;" : "+f"(s) : "h"(__half_as_ushort(__low2half(a))));
+    asm("add.rn.f32.f16 %0, %1, %0;" : "+f"(s) : "h"(__half_as_ushort(__high2half(a))));
+    return s;
+}
+
 struct Plane {
     float h[9];  // homography with the +0.5 texel offset folded into rows 0, 1
 };
@@ -330,14 +339,12 @@ __device__ __forceinline__ float source_cost(const Plane& P, cudaTextureObject_t
                 accumulate(p, __floats2half2_rn(__fsub_rn(smp[2 * p], c0), __fsub_rn(smp[2 * p + 1], c0)));
             }
         }
-        const float2 f1 = __half22float2(a1), f2 = __half22float2(a2), f3 = __half22float2(a3);
-        s1 = __fadd_rn(s1, __fadd_rn(f1.x, f1.y));
-        s2 = __fadd_rn(s2, __fadd_rn(f2.x, f2.y));
-        s3 = __fadd_rn(s3, __fadd_rn(f3.x, f3.y));
+        s1 = add_pair(s1, a1);
+        s2 = add_pair(s2, a2);
+        s3 = add_pair(s3, a3);
         if constexpr (CHECK) {
-            const float2 f4 = __half22float2(a4), f5 = __half22float2(a5);
-            r1 = __fadd_rn(r1, __fadd_rn(f4.x, f4.y));
-            r2 = __fadd_rn(r2, __fadd_rn(f5.x, f5.y));
+            r1 = add_pair(r1, a4);
+            r2 = add_pair(r2, a5);
             count += __popc(ok);
         }
     }
