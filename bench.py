@@ -402,6 +402,7 @@ def run_engine(args, rank, world, local_rank):
         if onchip.get("smem_bytes_per_s"):
             var["roofline_l1"] = {"achieved": round(rate_v * 5 * b_v / 1e9, 1), "unit": "GB/s",
                                   "frac": round(rate_v * 5 * b_v / onchip["smem_bytes_per_s"], 4)}
+    line["fusion"] = run_fusion(hp, ctx, s, dev_maps, n_views, stream)
     if world == 1 and not args.no_serving:
         line["serving"] = run_serving(args, hp, local_rank)
     if world == 1 and not args.no_batched:
@@ -481,6 +482,50 @@ def run_batched(args, hp, ctx):
                          "state_gb": round(info["state_bytes"] / 1e9, 2)}
     res["f16acc_over_f32"] = round(res["f16acc"]["mpix_iter_per_s"] / res["f32"]["mpix_iter_per_s"], 3)
     return res
+
+
+def run_fusion(hp, ctx, s, dev_maps, n_views, stream):
+    """Depth-map fusion (hp_fuse_depth_maps) of the last timed solve's device maps: each view's MVS sources
+    as its neighbours, confidence 1 - cost/2, gray colour, device arrays in and out.  One call = counting
+    pass, scan, writing pass (and the host read of the total between them), timed with CUDA events on
+    the engine's stream.  The maps are unfiltered solver output."""
+    import ctypes as C
+    import torch
+    H, W = dev_maps[0].arrays[0].shape
+    cams = [hp.make_camera(v.cam.K, v.cam.R, v.cam.t) for v in s.views[:n_views]]
+    conf = [1 - m.arrays[2] / 2 for m in dev_maps]
+    grays = [torch.from_numpy(v.image_f32).cuda() for v in s.views[:n_views]]
+    keep, views = [], []
+    for r in range(n_views):
+        v = hp.FuseView()
+        v.cam = cams[r]
+        v.height, v.width = H, W
+        v.depth, v.normal = dev_maps[r].arrays[0].data_ptr(), dev_maps[r].arrays[1].data_ptr()
+        v.confidence, v.gray = conf[r].data_ptr(), grays[r].data_ptr()
+        nb = np.array([i for i in s.sources[r] if i < n_views], np.int32)
+        keep.append(nb)
+        v.neighbors, v.num_neighbors = nb.ctypes.data_as(C.POINTER(C.c_int)), len(nb)
+        views.append(v)
+    prm = hp.fuse_params(memory=hp.MEMORY_DEVICE)
+    out = hp.PointCloudC()
+    out.memory = hp.MEMORY_DEVICE
+    total = ctx.fuse_views(views, prm, out)
+    arrs = [torch.empty((max(total, 1), 3), device="cuda") for _ in range(3)]
+    out.positions, out.normals, out.colors = (a.data_ptr() for a in arrs)
+    out.capacity = total
+    ctx.fuse_views(views, prm, out)
+    times = []
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ctx.fuse_views(views, prm, out)
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    ms = float(np.median(times))
+    mpix = n_views * H * W / 1e6
+    return {"workload": f"{n_views} views {W}x{H}, {len(keep[0])} neighbours each", "ms": round(ms, 3),
+            "mpix_per_s": round(mpix / (ms / 1e3), 1), "points": int(total), "params": "defaults"}
 
 
 def run_serving(args, hp, device: int):

@@ -134,6 +134,22 @@ class ServerStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class FuseView(C.Structure):
+    _fields_ = [("cam", Camera), ("depth", C.c_void_p), ("normal", C.c_void_p), ("confidence", C.c_void_p),
+                ("gray", C.c_void_p), ("neighbors", C.POINTER(C.c_int)), ("num_neighbors", C.c_int),
+                ("width", C.c_int), ("height", C.c_int)]
+
+
+class FuseParams(C.Structure):
+    _fields_ = [("memory", C.c_int), ("min_views", C.c_int), ("min_confidence", C.c_float),
+                ("max_depth_rel", C.c_float), ("max_reproj_px", C.c_float), ("min_normal_cos", C.c_float)]
+
+
+class PointCloudC(C.Structure):
+    _fields_ = [("memory", C.c_int), ("positions", C.c_void_p), ("normals", C.c_void_p), ("colors", C.c_void_p),
+                ("capacity", C.c_int64), ("count", C.c_int64)]
+
+
 def _load() -> C.CDLL:
     if not os.path.exists(LIB_PATH):
         raise ImportError(
@@ -193,6 +209,8 @@ def _load() -> C.CDLL:
         "hp_server_destroy": (C.c_int, [C.c_void_p]),
         "hp_server_simulate": (C.c_int, [C.c_int, P(C.c_int), P(C.c_uint64), P(C.c_int), C.c_int, C.c_uint64,
                                          C.c_int, P(C.c_int), P(C.c_int), P(C.c_int)]),
+        "hp_fuse_params_default": (None, [P(FuseParams)]),
+        "hp_fuse_depth_maps": (C.c_int, [C.c_void_p, P(FuseView), C.c_int, P(FuseParams), P(PointCloudC)]),
         "hp_pfm_write": (C.c_int, [C.c_char_p, C.c_void_p, C.c_int, C.c_int, C.c_int]),
         "hp_pfm_read": (C.c_int, [C.c_char_p, C.c_void_p, C.c_size_t, P(C.c_int), P(C.c_int), P(C.c_int)]),
     }
@@ -216,7 +234,7 @@ EXPORTS = (
     "hp_plan_get_info", "hp_plan_destroy", "hp_schedule_build", "hp_server_options_default", "hp_server_create",
     "hp_submit", "hp_poll", "hp_server_drain", "hp_server_stats_get", "hp_server_stats_reset",
     "hp_server_last_error", "hp_server_destroy", "hp_server_simulate", "hp_select_sources", "hp_project_seeds",
-    "hp_ctx_set_image_cache",
+    "hp_ctx_set_image_cache", "hp_fuse_params_default", "hp_fuse_depth_maps",
 )
 STATIC_MAX_PIXELS = 1280 * 1024  # HP_STATIC_MAX_PIXELS
 
@@ -393,6 +411,74 @@ class Context:
         self._check(lib.hp_geometric_filter(self._h, C.byref(ref_cam), w, h, _ptr(depth), _ptr(normal),
                                             _ptr(confidence), n, cams, dps, nps, _mem(depth), depth_tol,
                                             normal_tol_cos, min_consistent), "hp_geometric_filter")
+
+    def fuse_views(self, views: Sequence[FuseView], params: FuseParams, out: PointCloudC) -> int:
+        """hp_fuse_depth_maps as is: fills ``out`` up to its capacity; returns the number of fused points."""
+        varr = (FuseView * len(views))(*views)
+        self._check(lib.hp_fuse_depth_maps(self._h, varr, len(views), C.byref(params), C.byref(out)),
+                    "hp_fuse_depth_maps")
+        return int(out.count)
+
+    def fuse(self, cameras: Sequence[Camera], depths, normals, confidences=None, grays=None, neighbors=None,
+             params: Optional[FuseParams] = None) -> "DensePointCloud":
+        """Fuses per-view maps (all host numpy or all device tensors; confidences / grays may be None or
+        hold None entries) into a DensePointCloud of the same kind.  ``neighbors``: per view a list of view
+        indices, or None for every other view.  Counts first, then writes into arrays of exactly that size."""
+        n = len(cameras)
+        prm = FuseParams.from_buffer_copy(params if params is not None else fuse_params())
+        prm.memory = _mem(depths[0])
+        keep, views = [], []
+        for i in range(n):
+            v = FuseView()
+            v.cam = cameras[i]
+            v.height, v.width = depths[i].shape[:2]
+            v.depth, v.normal = _ptr(depths[i]), _ptr(normals[i])
+            cf = confidences[i] if confidences is not None else None
+            g = grays[i] if grays is not None else None
+            v.confidence = _ptr(cf) if cf is not None else None
+            v.gray = _ptr(g) if g is not None else None
+            if neighbors is not None and neighbors[i] is not None:
+                nb = np.ascontiguousarray(neighbors[i], np.int32)
+                keep.append(nb)
+                v.neighbors = nb.ctypes.data_as(C.POINTER(C.c_int))
+                v.num_neighbors = len(nb)
+            views.append(v)
+        out = PointCloudC()
+        out.memory = prm.memory
+        total = self.fuse_views(views, prm, out)
+        if prm.memory == MEMORY_HOST:
+            arrs = [np.zeros((total, 3), np.float32) for _ in range(3)]
+        else:
+            import torch
+            arrs = [torch.zeros((total, 3), dtype=torch.float32, device=depths[0].device) for _ in range(3)]
+        if total:
+            out.positions, out.normals, out.colors = (_ptr(a) for a in arrs)
+            out.capacity = total
+            self.fuse_views(views, prm, out)
+        return DensePointCloud(*arrs)
+
+
+def fuse_params(**kw) -> FuseParams:
+    """hp_fuse_params_default() with keyword overrides (min_views, max_depth_rel, ...)."""
+    p = FuseParams()
+    lib.hp_fuse_params_default(C.byref(p))
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise TypeError(f"unknown fusion parameter {k}")
+        setattr(p, k, v)
+    return p
+
+
+@dataclass
+class DensePointCloud:
+    """DensePointCloud (include/types.h:93-106): world-frame positions, unit normals and colours, (N, 3)
+    float32 each (host numpy or device tensors)."""
+    positions: object
+    normals: object
+    colors: object
+
+    def size(self) -> int:
+        return int(self.positions.shape[0])
 
 
 def plan_options(**kw) -> PlanOptions:
@@ -803,6 +889,35 @@ def run_patchmatch_mvs(images: Sequence[np.ndarray], cameras: Sequence[Camera],
         for i in ids.values():
             ctx.release(i)
         return result
+    finally:
+        if own:
+            ctx.close()
+
+
+def _gray_f32(img) -> np.ndarray:
+    a = np.asarray(img)
+    if a.dtype == np.uint8:
+        return (a.astype(np.float32) / np.float32(255.0)).astype(np.float32)
+    return np.ascontiguousarray(a, np.float32)
+
+
+def fuse_depth_maps(depth_maps: Sequence[DepthMap], cameras, images=None, params: Optional[FuseParams] = None,
+                    neighbors=None, ctx: Optional[Context] = None) -> DensePointCloud:
+    """fuseDepthMaps(depth_maps, poses, images) (src/dense_recon/point_cloud.h:7; a stub in the reference,
+    point_cloud.cu:4-8) on the engine's fusion (hp_fuse_depth_maps).
+
+    ``cameras`` and ``images`` are indexed by each map's ``image_id`` (as the reference's poses and images
+    vectors are); the colour is the image's gray value (u8 scaled by 1/255, or float in [0, 1]).  Maps are
+    host arrays as run_patchmatch_mvs returns them; ``neighbors`` lists, per map, the positions (in
+    ``depth_maps``) of the maps to check, or None for all."""
+    own = ctx is None
+    ctx = ctx or Context(0)
+    try:
+        f32 = lambda a: np.ascontiguousarray(a, np.float32)
+        return ctx.fuse([cameras[dm.image_id] for dm in depth_maps], [f32(dm.depth) for dm in depth_maps],
+                        [f32(dm.normal) for dm in depth_maps], [f32(dm.confidence) for dm in depth_maps],
+                        None if images is None else [_gray_f32(images[dm.image_id]) for dm in depth_maps],
+                        neighbors, params)
     finally:
         if own:
             ctx.close()

@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -784,6 +785,177 @@ hp_status hp_geometric_filter(hp_ctx* ctx, const hp_camera* ref_cam, int width, 
     HP_CUDA(counted(ctx, HP_KERNEL_OTHER, [&] { return hp::launch_geometric_filter(a, sd, sn, sc, ctx->stream); }));
     HP_CUDA(cudaMemcpyAsync(depth, sd, px * 4, cudaMemcpyDeviceToHost, ctx->stream));
     HP_CUDA(cudaMemcpyAsync(confidence, sc, px * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    HP_CUDA(cudaStreamSynchronize(ctx->stream));
+    flush_profile(ctx);
+    return HP_OK;
+}
+
+void hp_fuse_params_default(hp_fuse_params* p) {
+    if (!p) return;
+    p->memory = HP_MEMORY_HOST;
+    p->min_views = 2;
+    p->min_confidence = 0.0f;
+    p->max_depth_rel = 0.01f;
+    p->max_reproj_px = 2.0f;
+    p->min_normal_cos = 0.98480775f;  // cos(10 deg)
+}
+
+hp_status hp_fuse_depth_maps(hp_ctx* ctx, const hp_fuse_view* views, int num_views, const hp_fuse_params* prm,
+                             hp_point_cloud* out) {
+    if (!ctx) return HP_ERR_INVALID_ARG;
+    if (!views || !prm || !out) return fail(ctx, HP_ERR_INVALID_ARG, "fuse: null argument");
+    if (num_views < 1) return fail(ctx, HP_ERR_INVALID_ARG, "fuse: no views");
+    if (prm->memory != HP_MEMORY_HOST && prm->memory != HP_MEMORY_DEVICE)
+        return fail(ctx, HP_ERR_INVALID_ARG, "fuse: map memory %d", prm->memory);
+    if (out->memory != HP_MEMORY_HOST && out->memory != HP_MEMORY_DEVICE)
+        return fail(ctx, HP_ERR_INVALID_ARG, "fuse: cloud memory %d", out->memory);
+    if (prm->min_views < 1) return fail(ctx, HP_ERR_INVALID_ARG, "fuse: min_views %d < 1", prm->min_views);
+    if (!(prm->max_depth_rel >= 0.f) || !(prm->max_reproj_px >= 0.f) ||
+        !(prm->min_normal_cos >= -1.f && prm->min_normal_cos <= 1.f) || std::isnan(prm->min_confidence))
+        return fail(ctx, HP_ERR_INVALID_ARG, "fuse: tolerance out of range");
+    if (out->capacity < 0) return fail(ctx, HP_ERR_INVALID_ARG, "fuse: negative capacity");
+    DeviceGuard g(ctx->device);
+    // Device scratch freed on every return path (cudaFree waits for the device).
+    struct Scratch {
+        void* p = nullptr;
+        ~Scratch() {
+            if (p) cudaFree(p);
+        }
+    };
+    const bool dev_in = prm->memory == HP_MEMORY_DEVICE;
+    std::vector<hp::FuseView> fv(num_views);
+    std::vector<int> nbs, vblock(num_views + 1);
+    long long blocks = 0;
+    size_t staged_floats = 0;
+    for (int i = 0; i < num_views; ++i) {
+        const hp_fuse_view& v = views[i];
+        if (v.width < 1 || v.height < 1 || v.width > 65536 || v.height > 65536)
+            return fail(ctx, HP_ERR_INVALID_ARG, "fuse: view %d size %dx%d", i, v.width, v.height);
+        if (!v.depth || !v.normal) return fail(ctx, HP_ERR_INVALID_ARG, "fuse: view %d without depth or normal", i);
+        double kinv[9];
+        if (!mat3_inv(v.cam.K, kinv)) return fail(ctx, HP_ERR_INVALID_ARG, "fuse: view %d has a singular K", i);
+        hp::FuseView& f = fv[i];
+        std::memset(&f, 0, sizeof f);
+        for (int k = 0; k < 9; ++k) {
+            f.K[k] = static_cast<float>(v.cam.K[k]);
+            f.kinv[k] = static_cast<float>(kinv[k]);
+            f.R[k] = static_cast<float>(v.cam.R[k]);
+        }
+        for (int k = 0; k < 3; ++k) f.t[k] = static_cast<float>(v.cam.t[k]);
+        f.W = v.width;
+        f.H = v.height;
+        f.nb_begin = static_cast<int>(nbs.size());
+        if (v.neighbors) {
+            if (v.num_neighbors < 0) return fail(ctx, HP_ERR_INVALID_ARG, "fuse: view %d neighbour count", i);
+            for (int k = 0; k < v.num_neighbors; ++k) {
+                const int j = v.neighbors[k];
+                if (j < 0 || j >= num_views || j == i)
+                    return fail(ctx, HP_ERR_INVALID_ARG, "fuse: view %d lists neighbour %d", i, j);
+                nbs.push_back(j);
+            }
+        } else {
+            for (int j = 0; j < num_views; ++j)
+                if (j != i) nbs.push_back(j);
+        }
+        f.nb_count = static_cast<int>(nbs.size()) - f.nb_begin;
+        vblock[i] = static_cast<int>(blocks);
+        const size_t px = static_cast<size_t>(v.width) * v.height;
+        blocks += static_cast<long long>((px + hp::FUSE_THREADS - 1) / hp::FUSE_THREADS);
+        if (blocks > INT_MAX) return fail(ctx, HP_ERR_INVALID_ARG, "fuse: too many pixels");
+        staged_floats += px * (4 + (v.confidence ? 1 : 0) + (v.gray ? 1 : 0));
+    }
+    vblock[num_views] = static_cast<int>(blocks);
+    if (dev_in) {
+        for (int i = 0; i < num_views; ++i) {
+            fv[i].depth = views[i].depth;
+            fv[i].normal = views[i].normal;
+            fv[i].conf = views[i].confidence;
+            fv[i].gray = views[i].gray;
+        }
+    } else {  // host maps go up once through the staging buffer
+        HP_CUDA(ctx->staging.ensure(staged_floats * sizeof(float)));
+        float* dst = static_cast<float*>(ctx->staging.p);
+        auto stage = [&](const float* src, size_t n, const float** field) {
+            *field = nullptr;
+            if (!src) return cudaSuccess;
+            const cudaError_t e = cudaMemcpyAsync(dst, src, n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream);
+            *field = dst;
+            dst += n;
+            return e;
+        };
+        for (int i = 0; i < num_views; ++i) {
+            const size_t px = static_cast<size_t>(views[i].width) * views[i].height;
+            HP_CUDA(stage(views[i].depth, px, &fv[i].depth));
+            HP_CUDA(stage(views[i].normal, 3 * px, &fv[i].normal));
+            HP_CUDA(stage(views[i].confidence, px, &fv[i].conf));
+            HP_CUDA(stage(views[i].gray, px, &fv[i].gray));
+        }
+    }
+    // Descriptor block: views | neighbours | first CTA per view | CTA counts | CTA offsets | total.
+    auto up8 = [](size_t b) { return (b + 7) / 8 * 8; };
+    const size_t o_nb = up8(sizeof(hp::FuseView) * num_views);
+    const size_t o_vb = o_nb + up8(sizeof(int) * std::max<size_t>(nbs.size(), 1));
+    const size_t o_cnt = o_vb + up8(sizeof(int) * (num_views + 1));
+    const size_t o_off = o_cnt + up8(sizeof(int) * blocks);
+    const size_t o_tot = o_off + sizeof(long long) * blocks;
+    Scratch desc;
+    HP_CUDA(cudaMalloc(&desc.p, o_tot + sizeof(long long)));
+    char* base = static_cast<char*>(desc.p);
+    HP_CUDA(cudaMemcpyAsync(base, fv.data(), sizeof(hp::FuseView) * num_views, cudaMemcpyHostToDevice, ctx->stream));
+    if (!nbs.empty())
+        HP_CUDA(cudaMemcpyAsync(base + o_nb, nbs.data(), sizeof(int) * nbs.size(), cudaMemcpyHostToDevice,
+                                ctx->stream));
+    HP_CUDA(cudaMemcpyAsync(base + o_vb, vblock.data(), sizeof(int) * (num_views + 1), cudaMemcpyHostToDevice,
+                            ctx->stream));
+    hp::FuseArgs a;
+    a.views = reinterpret_cast<const hp::FuseView*>(base);
+    a.neighbors = reinterpret_cast<const int*>(base + o_nb);
+    a.view_block = reinterpret_cast<const int*>(base + o_vb);
+    a.n_views = num_views;
+    a.min_views = prm->min_views;
+    a.min_conf = prm->min_confidence;
+    a.max_depth_rel = prm->max_depth_rel;
+    a.max_reproj_sq = prm->max_reproj_px * prm->max_reproj_px;
+    a.min_normal_cos = prm->min_normal_cos;
+    int* counts = reinterpret_cast<int*>(base + o_cnt);
+    long long* offsets = reinterpret_cast<long long*>(base + o_off);
+    long long* d_total = reinterpret_cast<long long*>(base + o_tot);
+    const int nb = static_cast<int>(blocks);
+    HP_CUDA(counted(ctx, HP_KERNEL_OTHER, [&] { return hp::launch_fuse_count(a, nb, counts, ctx->stream); }));
+    HP_CUDA(counted(ctx, HP_KERNEL_OTHER,
+                    [&] { return hp::launch_fuse_scan(counts, nb, offsets, d_total, ctx->stream); }));
+    long long total = 0;
+    HP_CUDA(cudaMemcpyAsync(&total, d_total, sizeof total, cudaMemcpyDeviceToHost, ctx->stream));
+    HP_CUDA(cudaStreamSynchronize(ctx->stream));
+    out->count = total;
+    const long long nw = std::min<long long>(total, out->capacity);
+    if (nw > 0 && (out->positions || out->normals || out->colors)) {
+        if (out->memory == HP_MEMORY_DEVICE) {
+            HP_CUDA(counted(ctx, HP_KERNEL_OTHER, [&] {
+                return hp::launch_fuse_write(a, nb, offsets, out->positions, out->normals, out->colors, nw,
+                                             ctx->stream);
+            }));
+        } else {  // written on the device, then copied out
+            const size_t per = static_cast<size_t>(nw) * 3;
+            Scratch tmp;
+            HP_CUDA(cudaMalloc(&tmp.p, 3 * per * sizeof(float)));
+            float* tp = static_cast<float*>(tmp.p);
+            float* tn = tp + per;
+            float* tc = tn + per;
+            HP_CUDA(counted(ctx, HP_KERNEL_OTHER, [&] {
+                return hp::launch_fuse_write(a, nb, offsets, out->positions ? tp : nullptr,
+                                             out->normals ? tn : nullptr, out->colors ? tc : nullptr, nw,
+                                             ctx->stream);
+            }));
+            if (out->positions)
+                HP_CUDA(cudaMemcpyAsync(out->positions, tp, per * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+            if (out->normals)
+                HP_CUDA(cudaMemcpyAsync(out->normals, tn, per * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+            if (out->colors)
+                HP_CUDA(cudaMemcpyAsync(out->colors, tc, per * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+            HP_CUDA(cudaStreamSynchronize(ctx->stream));
+        }
+    }
     HP_CUDA(cudaStreamSynchronize(ctx->stream));
     flush_profile(ctx);
     return HP_OK;

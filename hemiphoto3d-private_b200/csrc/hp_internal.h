@@ -115,6 +115,27 @@ struct FilterArgs {
     int min_consistent;
 };
 
+// Depth-map fusion (hp_fuse_depth_maps): one view's device maps and its
+// camera cast to FP32 (kinv is the FP64 inverse of K, then cast).
+struct FuseView {
+    const float* depth;
+    const float* normal;
+    const float* conf;  // may be null
+    const float* gray;  // may be null
+    float K[9], kinv[9], R[9], t[3];
+    int W, H;
+    int nb_begin, nb_count;  // this view's slice of FuseArgs::neighbors
+};
+struct FuseArgs {
+    const FuseView* views;  // device, n_views
+    const int* neighbors;   // device
+    const int* view_block;  // device, n_views + 1: first CTA of each view's pixels
+    int n_views;
+    int min_views;
+    float min_conf, max_depth_rel, max_reproj_sq, min_normal_cos;
+};
+constexpr int FUSE_THREADS = 256;  // pixels per CTA of the fusion kernels
+
 }  // namespace hp
 
 // Kernel launchers (defined in the .cu files), all on the given stream.
@@ -145,4 +166,11 @@ cudaError_t launch_geometric_filter(const FilterArgs& a, float* depth, const flo
                                     cudaStream_t st);
 cudaError_t launch_to_f32(const void* src, int dtype, int W, int H, float* dst, int dst_pitch, __half* dst16,
                           int dst16_pitch, cudaStream_t st);
+// Fusion: per-CTA counts of emitted points, their exclusive prefix (and the
+// total), then the points written at their offsets (index < capacity only).
+cudaError_t launch_fuse_count(const FuseArgs& a, int blocks, int* block_counts, cudaStream_t st);
+cudaError_t launch_fuse_scan(const int* block_counts, int blocks, long long* block_offsets, long long* total,
+                             cudaStream_t st);
+cudaError_t launch_fuse_write(const FuseArgs& a, int blocks, const long long* block_offsets, float* positions,
+                              float* normals, float* colors, long long capacity, cudaStream_t st);
 }  // namespace hp

@@ -474,6 +474,62 @@ hp_status hp_select_sources(const hp_camera* cams, const int* registered, int nu
 hp_status hp_project_seeds(const hp_camera* cam, int ref, float depth_min, float depth_max,
                            const hp_sparse_points* points, hp_seed* out, int capacity, int* num_seeds);
 
+/* ---- Depth-map fusion: the stage's consumer ------------------------------
+ * Fills the reference's fuseDepthMaps(depth_maps, poses, images)
+ * (src/dense_recon/point_cloud.h:7, a stub returning an empty cloud at
+ * src/dense_recon/point_cloud.cu:4-8) and its DensePointCloud output
+ * (include/types.h:93-106: positions, normals, colours as float3 arrays).
+ *
+ * A pixel of view i with depth > 0 (and confidence >= min_confidence) is
+ * back-projected to X with its normal rotated to the world frame.  Each
+ * neighbour j takes X to its pixel q (rounded projection), and agrees when
+ *   q is inside view j with depth > 0 (and confidence >= min_confidence),
+ *   |z_j(X) - depth_j(q)| <= max_depth_rel * depth_j(q),
+ *   q's back-projection lands within max_reproj_px of the pixel in view i,
+ *   the two world normals have cosine >= min_normal_cos.
+ * The point is emitted when at least min_views views agree (the view itself
+ * counts) and no agreeing neighbour has a lower index than i; that lowest view
+ * emits the surface point instead, so with symmetric neighbour lists each is
+ * emitted once.  Position, normal and colour are the means over the agreeing
+ * views (the normal renormalised; the colour the gray value, replicated to
+ * three channels).  Points come in (view, row, column) order; FP32 arithmetic
+ * with every operation rounded as written (no contraction), so results do not
+ * depend on the launch configuration. */
+typedef struct hp_fuse_view {
+    hp_camera cam;
+    const float* depth;       /* H*W, 0 = invalid (e.g. after hp_geometric_filter) */
+    const float* normal;      /* H*W*3, camera frame, as hp_solve writes them */
+    const float* confidence;  /* H*W, or NULL: every pixel eligible */
+    const float* gray;        /* H*W intensity in [0, 1] for the colour, or NULL: colour 0 */
+    const int* neighbors;     /* host array of view indices to check, or NULL: every other view */
+    int num_neighbors;
+    int width, height;
+} hp_fuse_view;
+
+typedef struct hp_fuse_params {
+    int memory;               /* hp_memory of every view's map pointers */
+    int min_views;            /* agreeing views, the view itself included (default 2) */
+    float min_confidence;     /* default 0 */
+    float max_depth_rel;      /* default 0.01 */
+    float max_reproj_px;      /* default 2 */
+    float min_normal_cos;     /* default cos(10 deg); -1 turns the normal test off */
+} hp_fuse_params;
+
+typedef struct hp_point_cloud {
+    int memory;               /* hp_memory of the three arrays */
+    float* positions;         /* capacity*3 world-frame points, or NULL */
+    float* normals;           /* capacity*3 unit world-frame normals, or NULL */
+    float* colors;            /* capacity*3, or NULL */
+    int64_t capacity;         /* points the arrays hold */
+    int64_t count;            /* out: points fused; those at index >= capacity are not written */
+} hp_point_cloud;
+
+void hp_fuse_params_default(hp_fuse_params* p);
+/* Fuses num_views depth maps into out (see above).  With capacity 0 it only
+ * counts, so a caller can size the arrays and call again. */
+hp_status hp_fuse_depth_maps(hp_ctx* ctx, const hp_fuse_view* views, int num_views,
+                             const hp_fuse_params* params, hp_point_cloud* out);
+
 /* Replaces saveDepthMapPFM / loadDepthMapPFM (patchmatch_mvs.cu:990-1022):
  * 'Pf' (channels 1) or 'PF' (channels 3) little-endian PFM, rows bottom-up. */
 hp_status hp_pfm_write(const char* path, const float* data, int width, int height, int channels);

@@ -682,3 +682,185 @@ void orc_geometric_filter(const orc_camera* ref, int W, int H, float* depth, con
             }
         }
 }
+
+/* ---- depth-map fusion (the rule of hp_fuse_depth_maps) ------------------- */
+
+typedef struct fuse_cam {
+    float K[9], kinv[9], R[9], t[3];
+} fuse_cam;
+
+/* R^T (x, y, z) */
+static void fuse_rot_to_world(const float* R, float x, float y, float z, float* o) {
+    o[0] = fmaf(R[0], x, fmaf(R[3], y, R[6] * z));
+    o[1] = fmaf(R[1], x, fmaf(R[4], y, R[7] * z));
+    o[2] = fmaf(R[2], x, fmaf(R[5], y, R[8] * z));
+}
+
+/* R^T (d K^-1 [x y 1] - t) */
+static void fuse_to_world(const fuse_cam* c, float fx, float fy, float d, float* o) {
+    const float* k = c->kinv;
+    const float cx = d * fmaf(k[0], fx, fmaf(k[1], fy, k[2]));
+    const float cy = d * fmaf(k[3], fx, fmaf(k[4], fy, k[5]));
+    const float cz = d * fmaf(k[6], fx, fmaf(k[7], fy, k[8]));
+    fuse_rot_to_world(c->R, cx - c->t[0], cy - c->t[1], cz - c->t[2], o);
+}
+
+/* R X + t */
+static void fuse_to_camera(const fuse_cam* c, const float* X, float* o) {
+    const float* R = c->R;
+    o[0] = fmaf(R[0], X[0], fmaf(R[1], X[1], fmaf(R[2], X[2], c->t[0])));
+    o[1] = fmaf(R[3], X[0], fmaf(R[4], X[1], fmaf(R[5], X[2], c->t[1])));
+    o[2] = fmaf(R[6], X[0], fmaf(R[7], X[1], fmaf(R[8], X[2], c->t[2])));
+}
+
+/* K p */
+static void fuse_to_pixel(const float* K, const float* p, float* o) {
+    o[0] = fmaf(K[0], p[0], fmaf(K[1], p[1], K[2] * p[2]));
+    o[1] = fmaf(K[3], p[0], fmaf(K[4], p[1], K[5] * p[2]));
+    o[2] = fmaf(K[6], p[0], fmaf(K[7], p[1], K[8] * p[2]));
+}
+
+/* One pixel; 1 with the point in out[7] (position, normal, colour) when it is emitted. */
+static int fuse_pixel(const orc_fuse_view* views, const fuse_cam* cams, const int* const* nb, const int* nbn,
+                      int i, int x, int y, int min_views, float min_conf, float max_depth_rel, float max_reproj_sq,
+                      float min_normal_cos, float* out) {
+    const orc_fuse_view* v = &views[i];
+    const fuse_cam* cv = &cams[i];
+    const size_t idx = (size_t)y * v->W + x;
+    const float d = v->depth[idx];
+    if (!(d > 0.0f)) return 0;
+    if (v->confidence && !(v->confidence[idx] >= min_conf)) return 0;
+    const float fx = (float)x, fy = (float)y;
+    float X[3], n[3];
+    fuse_to_world(cv, fx, fy, d, X);
+    fuse_rot_to_world(cv->R, v->normal[3 * idx], v->normal[3 * idx + 1], v->normal[3 * idx + 2], n);
+    float s[3] = {X[0], X[1], X[2]}, sn[3] = {n[0], n[1], n[2]};
+    float sc = v->gray ? v->gray[idx] : 0.0f;
+    int count = 1;
+    for (int k = 0; k < nbn[i]; ++k) {
+        const int j = nb[i][k];
+        const orc_fuse_view* w = &views[j];
+        const fuse_cam* cw = &cams[j];
+        float p[3], h[3];
+        fuse_to_camera(cw, X, p);
+        if (!(p[2] > 0.0f)) continue;
+        fuse_to_pixel(cw->K, p, h);
+        if (!(h[2] > 0.0f)) continue;
+        const float u = h[0] / h[2], vv = h[1] / h[2];
+        if (!(u >= -0.5f && u <= (float)w->W && vv >= -0.5f && vv <= (float)w->H)) continue;
+        const int qx = (int)rintf(u), qy = (int)rintf(vv);
+        if (qx < 0 || qx >= w->W || qy < 0 || qy >= w->H) continue;
+        const size_t q = (size_t)qy * w->W + qx;
+        const float dj = w->depth[q];
+        if (!(dj > 0.0f)) continue;
+        if (w->confidence && !(w->confidence[q] >= min_conf)) continue;
+        if (!(fabsf(p[2] - dj) <= max_depth_rel * dj)) continue;
+        float Y[3], r[3], g[3], m[3];
+        fuse_to_world(cw, (float)qx, (float)qy, dj, Y);
+        fuse_to_camera(cv, Y, r);
+        if (!(r[2] > 0.0f)) continue;
+        fuse_to_pixel(cv->K, r, g);
+        if (!(g[2] > 0.0f)) continue;
+        const float du = g[0] / g[2] - fx, dv = g[1] / g[2] - fy;
+        if (!(fmaf(du, du, dv * dv) <= max_reproj_sq)) continue;
+        fuse_rot_to_world(cw->R, w->normal[3 * q], w->normal[3 * q + 1], w->normal[3 * q + 2], m);
+        if (!(fmaf(n[0], m[0], fmaf(n[1], m[1], n[2] * m[2])) >= min_normal_cos)) continue;
+        if (j < i) return 0;
+        s[0] += Y[0];
+        s[1] += Y[1];
+        s[2] += Y[2];
+        sn[0] += m[0];
+        sn[1] += m[1];
+        sn[2] += m[2];
+        sc += w->gray ? w->gray[q] : 0.0f;
+        ++count;
+    }
+    if (count < min_views) return 0;
+    const float c = (float)count;
+    out[0] = s[0] / c;
+    out[1] = s[1] / c;
+    out[2] = s[2] / c;
+    const float len = sqrtf(fmaf(sn[0], sn[0], fmaf(sn[1], sn[1], sn[2] * sn[2])));
+    out[3] = len > 0.0f ? sn[0] / len : 0.0f;
+    out[4] = len > 0.0f ? sn[1] / len : 0.0f;
+    out[5] = len > 0.0f ? sn[2] / len : 0.0f;
+    out[6] = sc / c;
+    return 1;
+}
+
+long long orc_fuse(const orc_fuse_view* views, int num_views, int min_views, float min_confidence,
+                   float max_depth_rel, float max_reproj_px, float min_normal_cos, float* positions,
+                   float* normals, float* colors, long long capacity) {
+    if (num_views < 1) return 0;
+    fuse_cam* cams = (fuse_cam*)calloc((size_t)num_views, sizeof(fuse_cam));
+    const int** nb = (const int**)calloc((size_t)num_views, sizeof(int*));
+    int* nbn = (int*)calloc((size_t)num_views, sizeof(int));
+    int* all = (int*)calloc((size_t)num_views * (size_t)num_views, sizeof(int));
+    int rows = 0;
+    for (int i = 0; i < num_views; ++i) {
+        double kinv[9];
+        if (mat3_inv(views[i].cam.K, kinv)) memset(kinv, 0, sizeof kinv);
+        for (int k = 0; k < 9; ++k) {
+            cams[i].K[k] = (float)views[i].cam.K[k];
+            cams[i].kinv[k] = (float)kinv[k];
+            cams[i].R[k] = (float)views[i].cam.R[k];
+        }
+        for (int k = 0; k < 3; ++k) cams[i].t[k] = (float)views[i].cam.t[k];
+        if (views[i].neighbors) {
+            nb[i] = views[i].neighbors;
+            nbn[i] = views[i].num_neighbors;
+        } else {
+            int* list = all + (size_t)i * num_views;
+            for (int j = 0; j < num_views; ++j)
+                if (j != i) list[nbn[i]++] = j;
+            nb[i] = list;
+        }
+        rows += views[i].H;
+    }
+    const float max_reproj_sq = max_reproj_px * max_reproj_px;
+    /* Pass 1: points per (view, row); pass 2: each row writes at its prefix offset. */
+    long long* row_off = (long long*)calloc((size_t)rows + 1, sizeof(long long));
+    int* row_view = (int*)calloc((size_t)rows, sizeof(int));
+    int* row_y = (int*)calloc((size_t)rows, sizeof(int));
+    for (int i = 0, r = 0; i < num_views; ++i)
+        for (int y = 0; y < views[i].H; ++y, ++r) {
+            row_view[r] = i;
+            row_y[r] = y;
+        }
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int r = 0; r < rows; ++r) {
+        const int i = row_view[r], y = row_y[r];
+        long long n = 0;
+        float pt[7];
+        for (int x = 0; x < views[i].W; ++x)
+            n += fuse_pixel(views, cams, nb, nbn, i, x, y, min_views, min_confidence, max_depth_rel, max_reproj_sq,
+                            min_normal_cos, pt);
+        row_off[r + 1] = n;
+    }
+    for (int r = 0; r < rows; ++r) row_off[r + 1] += row_off[r];
+    const long long total = row_off[rows];
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int r = 0; r < rows; ++r) {
+        const int i = row_view[r], y = row_y[r];
+        long long o = row_off[r];
+        if (o >= capacity) continue;
+        float pt[7];
+        for (int x = 0; x < views[i].W && o < capacity; ++x) {
+            if (!fuse_pixel(views, cams, nb, nbn, i, x, y, min_views, min_confidence, max_depth_rel, max_reproj_sq,
+                            min_normal_cos, pt))
+                continue;
+            if (positions) memcpy(positions + 3 * o, pt, 3 * sizeof(float));
+            if (normals) memcpy(normals + 3 * o, pt + 3, 3 * sizeof(float));
+            if (colors) colors[3 * o] = colors[3 * o + 1] = colors[3 * o + 2] = pt[6];
+            ++o;
+        }
+    }
+    free(row_off);
+    free(row_view);
+    free(row_y);
+    free(all);
+    free(nbn);
+    free(nb);
+    free(cams);
+    return total;
+}

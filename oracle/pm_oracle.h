@@ -109,6 +109,28 @@ void orc_geometric_filter(const orc_camera* ref, int W, int H, float* depth, con
                           const float* const* src_normals, float depth_tol, float normal_tol_cos,
                           int min_consistent);
 
+/* Depth-map fusion into a point cloud, the rule hp_fuse_depth_maps states in
+ * include/hpmvs.h (the reference's fuseDepthMaps, src/dense_recon/point_cloud.h:7,
+ * is a stub): a pixel's world point, checked in each neighbour for depth,
+ * reprojection and normal agreement, emitted as the mean of the agreeing
+ * points by the lowest-index agreeing view, in (view, row, column) order.
+ * Same FP32 operation order as the engine's kernel.  Returns the number of
+ * points; writes the first `capacity` of them (any output may be NULL). */
+typedef struct orc_fuse_view {
+    orc_camera cam;
+    const float* depth;
+    const float* normal;      /* camera frame */
+    const float* confidence;  /* or NULL */
+    const float* gray;        /* or NULL */
+    const int* neighbors;     /* or NULL: every other view */
+    int num_neighbors;
+    int W, H;
+} orc_fuse_view;
+
+long long orc_fuse(const orc_fuse_view* views, int num_views, int min_views, float min_confidence,
+                   float max_depth_rel, float max_reproj_px, float min_normal_cos, float* positions,
+                   float* normals, float* colors, long long capacity);
+
 int orc_num_threads(void);
 void orc_set_num_threads(int n);
 

@@ -35,6 +35,12 @@ class OrcView(C.Structure):
     ]
 
 
+class OrcFuseView(C.Structure):
+    _fields_ = [("cam", OrcCamera), ("depth", C.POINTER(C.c_float)), ("normal", C.POINTER(C.c_float)),
+                ("confidence", C.POINTER(C.c_float)), ("gray", C.POINTER(C.c_float)),
+                ("neighbors", C.POINTER(C.c_int)), ("num_neighbors", C.c_int), ("W", C.c_int), ("H", C.c_int)]
+
+
 class OrcRefine(C.Structure):
     _fields_ = [("refine_steps", C.c_int), ("iter_decay", C.c_float), ("step_decay", C.c_float)]
 
@@ -80,6 +86,8 @@ def lib():
                                       P(OrcRefine), fp, fp, fp]),
             "orc_geometric_filter": (None, [P(OrcCamera), C.c_int, C.c_int, fp, fp, fp, C.c_int, P(OrcCamera),
                                             P(fp), P(fp), C.c_float, C.c_float, C.c_int]),
+            "orc_fuse": (C.c_longlong, [P(OrcFuseView), C.c_int, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float,
+                                        fp, fp, fp, C.c_longlong]),
             "orc_num_threads": (C.c_int, []),
             "orc_set_num_threads": (None, [C.c_int]),
         }
@@ -212,6 +220,38 @@ def geometric_filter(ref_cam, depth, normal, conf, src_cams, src_depths, src_nor
     nps = (FP * max(1, n))(*[_fp(a) for a in src_normals])
     lib().orc_geometric_filter(C.byref(camera(*ref_cam)), w, h, _fp(depth), _fp(normal), _fp(conf), n, cams, dps,
                                nps, depth_tol, normal_tol_cos, min_consistent)
+
+
+def fuse(maps, cams, neighbors=None, min_views=2, min_confidence=0.0, max_depth_rel=0.01, max_reproj_px=2.0,
+         min_normal_cos=0.98480775):
+    """Depth-map fusion (orc_fuse).  maps: per view (depth (H, W), normal (H, W, 3), confidence or None,
+    gray or None), float32; cams: per view (K, R, t); neighbors: per view a list of view indices, or None for
+    every other view.  Returns (positions, normals, colors), each (N, 3) float32."""
+    n = len(maps)
+    keep = []
+    views = (OrcFuseView * n)()
+    for i, (d, nr, cf, g) in enumerate(maps):
+        arrs = [np.ascontiguousarray(a, np.float32) if a is not None else None for a in (d, nr, cf, g)]
+        keep.append(arrs)
+        v = views[i]
+        v.cam = camera(*cams[i])
+        v.depth, v.normal = _fp(arrs[0]), _fp(arrs[1])
+        v.confidence = _fp(arrs[2]) if arrs[2] is not None else None
+        v.gray = _fp(arrs[3]) if arrs[3] is not None else None
+        v.H, v.W = arrs[0].shape
+        if neighbors is not None and neighbors[i] is not None:
+            nb = np.ascontiguousarray(neighbors[i], np.int32)
+            keep.append(nb)
+            v.neighbors = nb.ctypes.data_as(C.POINTER(C.c_int))
+            v.num_neighbors = len(nb)
+    args = (views, n, min_views, min_confidence, max_depth_rel, max_reproj_px, min_normal_cos)
+    total = lib().orc_fuse(*args, None, None, None, 0)
+    pos = np.zeros((total, 3), np.float32)
+    nrm = np.zeros((total, 3), np.float32)
+    col = np.zeros((total, 3), np.float32)
+    if total:
+        lib().orc_fuse(*args, _fp(pos), _fp(nrm), _fp(col), total)
+    return pos, nrm, col
 
 
 def set_tex_rounding(mode: int):
