@@ -1,7 +1,8 @@
 // hpmvs_stage.hpp - header-only C++ adapter: the reference's dense stage
 //     std::vector<DepthMap> runPatchMatchMVS(images, cameras, sfm, config)
-// (src/dense_recon/patchmatch_mvs.h:39-44) implemented on the B200 engine's
-// C ABI (hpmvs.h).  It is meant to be included by the reference's
+// (src/dense_recon/patchmatch_mvs.h:39-44), and its consumer fuseDepthMaps
+// (src/dense_recon/point_cloud.h:7), implemented on the B200 engine's C ABI
+// (hpmvs.h).  It is meant to be included by the reference's
 // patchmatch_mvs.cu, whose data model (types.h: ImageData, CameraPose,
 // DepthMap, PipelineConfig; sfm/camera_pose.h: SfMResult) and host-side
 // selectSourceViews it uses; it compiles wherever those headers do.
@@ -172,6 +173,61 @@ inline std::vector<DepthMap> runPatchMatchMVS(const std::vector<ImageData>& imag
     hp_ctx_destroy(ctx);
     if (st != HP_OK) maps.clear();
     return maps;
+}
+
+// fuseDepthMaps(depth_maps, poses, images) (src/dense_recon/point_cloud.h:7, a
+// stub at point_cloud.cu:4-8) on hp_fuse_depth_maps: poses and images are
+// indexed by each map's image_id, every other map is a neighbour, and the
+// tolerances are the engine's defaults.  The colour is the gray value.
+inline DensePointCloud fuseDepthMaps(const std::vector<DepthMap>& depth_maps, const std::vector<CameraPose>& poses,
+                                     const std::vector<ImageData>& images, hp_status* status = nullptr,
+                                     int gpu_id = 0) {
+    static_assert(sizeof(Eigen::Vector3f) == 3 * sizeof(float), "DensePointCloud arrays are packed float3");
+    hp_status st_local = HP_OK;
+    hp_status& st = status ? *status : st_local;
+    DensePointCloud cloud;
+    if (depth_maps.empty()) return cloud;
+    std::vector<hp_fuse_view> v(depth_maps.size());
+    for (size_t i = 0; i < depth_maps.size(); ++i) {
+        const DepthMap& dm = depth_maps[i];
+        const size_t id = static_cast<size_t>(dm.image_id);
+        if (id >= poses.size()) {
+            st = HP_ERR_INVALID_ARG;
+            return cloud;
+        }
+        std::memset(&v[i], 0, sizeof v[i]);
+        v[i].cam = to_hp_camera(poses[id]);
+        v[i].depth = reinterpret_cast<const float*>(dm.depth.data);
+        v[i].normal = reinterpret_cast<const float*>(dm.normal.data);  // camera frame, as the stage writes it
+        v[i].confidence = dm.confidence.empty() ? nullptr : reinterpret_cast<const float*>(dm.confidence.data);
+        v[i].gray = id < images.size() && !images[id].gray.empty()
+                        ? reinterpret_cast<const float*>(images[id].gray.data)
+                        : nullptr;
+        v[i].width = dm.width;
+        v[i].height = dm.height;
+    }
+    hp_ctx* ctx = nullptr;
+    if ((st = hp_ctx_create(gpu_id, &ctx)) != HP_OK) return cloud;
+    hp_fuse_params fp;
+    hp_fuse_params_default(&fp);
+    fp.memory = HP_MEMORY_HOST;
+    hp_point_cloud pc;
+    std::memset(&pc, 0, sizeof pc);
+    pc.memory = HP_MEMORY_HOST;
+    st = hp_fuse_depth_maps(ctx, v.data(), static_cast<int>(v.size()), &fp, &pc);  // counts
+    if (st == HP_OK && pc.count > 0) {
+        cloud.positions.resize(static_cast<size_t>(pc.count));
+        cloud.normals.resize(static_cast<size_t>(pc.count));
+        cloud.colors.resize(static_cast<size_t>(pc.count));
+        pc.positions = reinterpret_cast<float*>(cloud.positions.data());
+        pc.normals = reinterpret_cast<float*>(cloud.normals.data());
+        pc.colors = reinterpret_cast<float*>(cloud.colors.data());
+        pc.capacity = pc.count;
+        st = hp_fuse_depth_maps(ctx, v.data(), static_cast<int>(v.size()), &fp, &pc);
+    }
+    hp_ctx_destroy(ctx);
+    if (st != HP_OK) cloud = DensePointCloud();
+    return cloud;
 }
 
 }  // namespace hpmvs_stage

@@ -136,15 +136,16 @@ def test_pfm_errors(hp, tmp_path):
 
 
 def test_stage_adapter_compiles_against_reference_headers(tmp_path):
-    """include/hpmvs_stage.hpp (runPatchMatchMVS on the C ABI) compiles inside the reference's
+    """include/hpmvs_stage.hpp (runPatchMatchMVS and fuseDepthMaps on the C ABI) compiles inside the reference's
     own translation-unit context: its types.h / patchmatch_mvs.h, with the test-only stand-ins
     for the Eigen and OpenCV headers those include."""
     ref = "/root/reference"
     if not os.path.isdir(os.path.join(ref, "src", "dense_recon")):
         pytest.skip("reference tree not present")
     src = tmp_path / "adapter.cpp"
-    src.write_text('#include "dense_recon/patchmatch_mvs.h"\n#include "hpmvs_stage.hpp"\n'
-                   'auto* p = &hpmvs_stage::runPatchMatchMVS;\n')
+    src.write_text('#include "dense_recon/patchmatch_mvs.h"\n#include "dense_recon/point_cloud.h"\n'
+                   '#include "hpmvs_stage.hpp"\n'
+                   'auto* p = &hpmvs_stage::runPatchMatchMVS;\nauto* q = &hpmvs_stage::fuseDepthMaps;\n')
     subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-I", os.path.join(ROOT, "oracle", "ref_harness", "shim"),
                     "-I", os.path.join(ref, "include"), "-I", os.path.join(ref, "src"), "-I", os.path.join(ROOT, "include"),
                     "-I", "/usr/local/cuda/include", str(src)], check=True)
