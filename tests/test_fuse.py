@@ -229,3 +229,20 @@ def test_capacity_and_invalid_arguments(hp, po, small_scene):
         sing.cam = hp.make_camera(np.zeros((3, 3)), np.eye(3), np.zeros(3))
         with pytest.raises(hp.HpError):
             ctx.fuse_views([sing] + views[1:], prm, hp.PointCloudC())
+
+
+@pytest.mark.gpu
+def test_fuse_depth_maps_on_the_stage_output(hp, po, small_scene):
+    """fuse_depth_maps(depth_maps, cameras, images) - the reference's fuseDepthMaps signature - on the
+    DepthMaps run_patchmatch_mvs returns (host maps, filtered, confidence 1 - cost / 2)."""
+    s = small_scene
+    n = len(s.views)
+    cams = [hp.make_camera(*cam_of(s, i)) for i in range(n)]
+    images = [v.image for v in s.views]
+    views = [hp.ViewParams(r, list(s.sources[r]), *s.depth_range) for r in range(n)]
+    maps = hp.run_patchmatch_mvs(images, cams, views, hp.MVSConfig(mvs_iterations=4, mvs_patch_size=11))
+    cloud = hp.fuse_depth_maps(maps, cams, images)
+    want = po.fuse([(dm.depth, dm.normal, dm.confidence, hp._gray_f32(images[dm.image_id])) for dm in maps],
+                   [cam_of(s, dm.image_id) for dm in maps])
+    assert cloud.size() > 0
+    assert _same((cloud.positions, cloud.normals, cloud.colors), want)
