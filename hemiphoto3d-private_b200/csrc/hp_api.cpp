@@ -861,7 +861,9 @@ hp_status hp_fuse_depth_maps(hp_ctx* ctx, const hp_fuse_view* views, int num_vie
         vblock[i] = static_cast<int>(blocks);
         const size_t px = static_cast<size_t>(v.width) * v.height;
         blocks += static_cast<long long>((px + hp::FUSE_THREADS - 1) / hp::FUSE_THREADS);
-        if (blocks > INT_MAX) return fail(ctx, HP_ERR_INVALID_ARG, "fuse: too many pixels");
+        // The one-CTA scan splits the per-CTA counts into 1024 chunks with int
+        // offsets; 2^30 CTAs (2.7e11 pixels) keeps those offsets in range.
+        if (blocks > (1ll << 30)) return fail(ctx, HP_ERR_INVALID_ARG, "fuse: too many pixels");
         staged_floats += px * (4 + (v.confidence ? 1 : 0) + (v.gray ? 1 : 0));
     }
     vblock[num_views] = static_cast<int>(blocks);
