@@ -109,6 +109,24 @@ def test_edge_cases(po, small_scene):
     assert len(po.fuse(maps, cams, min_normal_cos=0.99999)[0]) < len(base[0])
 
 
+def test_oracle_fusion_is_independent_of_thread_count(po, small_scene):
+    """Points come in (view, row, column) order whatever the parallel split: one thread and eight
+    give the same arrays."""
+    s = small_scene
+    maps = _gt_maps(s, noise=0.002, seed=9)
+    cams = [cam_of(s, i) for i in range(len(maps))]
+    n0 = po.num_threads()
+    try:
+        po.set_num_threads(1)
+        one = po.fuse(maps, cams)
+        po.set_num_threads(8)
+        many = po.fuse(maps, cams)
+    finally:
+        po.set_num_threads(n0)
+    assert len(one[0]) > 0
+    assert all(np.array_equal(a, b) for a, b in zip(one, many))
+
+
 def test_fusion_entry_points_are_exported_and_defaults(hp):
     for name in ("hp_fuse_params_default", "hp_fuse_depth_maps"):
         assert hasattr(hp.lib, name) and name in hp.EXPORTS
