@@ -245,9 +245,17 @@ def solve_static(job: Job, params: Params, ref_image, src_textures: Sequence[int
     memory.  ``ref_image`` is a contiguous device FP32 tensor (H, W); ``src_textures`` are texture-object
     handles over the FP32 source images (linear filter, clamp, unnormalised coordinates); ``out`` holds device
     maps.  No device memory is allocated: the state lives in a fixed array of HP_STATIC_MAX_PIXELS pixels."""
+    if len(src_textures) != job.num_sources:
+        raise ValueError(f"solve_static: {len(src_textures)} source textures for a job with {job.num_sources} sources")
+    import torch
+    if not (isinstance(ref_image, torch.Tensor) and ref_image.is_cuda and ref_image.dtype == torch.float32
+            and ref_image.dim() == 2):
+        raise ValueError("solve_static: ref_image must be a 2-D float32 CUDA tensor")
+    if ref_image.stride(1) != 1:
+        raise ValueError("solve_static: ref_image rows must be contiguous")
     h, w = ref_image.shape
     tex = (C.c_ulonglong * len(src_textures))(*src_textures)
-    st = lib.hp_solve_static(device, stream or None, C.byref(job), int(ref_image.data_ptr()), w, w, h, tex,
+    st = lib.hp_solve_static(device, stream or None, C.byref(job), int(ref_image.data_ptr()), int(ref_image.stride(0)), w, h, tex,
                              C.byref(params), C.byref(out))
     if st != OK:
         raise HpError(st, "hp_solve_static")

@@ -13,20 +13,25 @@
 // HP_STATIC_SCRATCH_BYTES, created when the library's device code is loaded
 // on a GPU and held by every GPU that loads it until the process exits.  Host
 // code may not use the array's name as a device address (on the host it is
-// only a stand-in symbol), so the first call on each device looks up the
-// real address with cudaGetSymbolAddress while that device is current and
-// caches it; that first call therefore does the set-up and should come
-// before any stream capture.
+// only a stand-in symbol), so the first call in each CUDA context looks up the
+// real address with cudaGetSymbolAddress while that context is current and
+// caches it under the context's process-unique id (cuCtxGetId); that first
+// call therefore does the set-up and should come before any stream capture.
+// A context created later on the same device - after cudaDeviceReset, or a
+// driver-API context the caller made current - has a new id, so its first
+// call looks the address up again instead of using a stale one.
 //
 // Every call shares the one array and overwrites it: the state a call needs
 // is fully written before it is read (the init kernel writes every plane, the
 // cost kernel every cost, descriptors are copied in), so nothing needs to
-// start at zero.  The call waits for its own work before returning, but two
-// calls running at the same time (from different host threads, on any
-// streams) would use the same array and corrupt each other: callers must
-// serialise them.
+// start at zero.  The call waits for its own work before returning, also when
+// it fails after queuing some of it, but two calls running at the same time
+// (from different host threads, on any streams) would use the same array and
+// corrupt each other: callers must serialise them.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstring>
 #include <mutex>
 
@@ -43,18 +48,53 @@ static __device__ __align__(256) unsigned char g_static_scratch[HP_STATIC_SCRATC
 
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
-void* g_scratch_addr[kMaxDevices] = {};
+struct ScratchSlot {
+    unsigned long long ctx_id = 0;  // cuCtxGetId of the context the address belongs to (0: none yet)
+    void* addr = nullptr;
+};
+ScratchSlot g_scratch[kMaxDevices];
 
-// Device address of g_static_scratch on `device` (which must be current).
+// Driver entry points for the current context's id, reached through the
+// runtime so the library does not link libcuda.
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+template <class F>
+F driver_entry(const char* name) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint(name, &p, cudaEnableDefault, &q) != cudaSuccess || q != cudaDriverEntryPointSuccess)
+        return nullptr;
+    return reinterpret_cast<F>(p);
+}
+
+// Id of the context current on this thread; 0 when it cannot be told (then the
+// address is looked up on every call rather than cached).
+unsigned long long current_context_id() {
+    static const CtxGetCurrentFn get_current = driver_entry<CtxGetCurrentFn>("cuCtxGetCurrent");
+    static const CtxGetIdFn get_id = driver_entry<CtxGetIdFn>("cuCtxGetId");
+    if (!get_current || !get_id) return 0;
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&c) != CUDA_SUCCESS || !c || get_id(c, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
+
+// Device address of g_static_scratch in the context current on `device`.
 cudaError_t scratch_address(int device, unsigned char** out) {
+    // Before the runtime has made a context current the id reads 0, and the
+    // lookup below (which makes one current) is simply repeated next call.
+    const unsigned long long id = current_context_id();
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_addr[device]) {
+    ScratchSlot& slot = g_scratch[device];
+    if (id == 0 || slot.ctx_id != id) {
         void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
         if (e != cudaSuccess) return e;
-        g_scratch_addr[device] = p;
+        slot.addr = p;
+        slot.ctx_id = id;
     }
-    *out = static_cast<unsigned char*>(g_scratch_addr[device]);
+    *out = static_cast<unsigned char*>(slot.addr);
     return cudaSuccess;
 }
 
@@ -76,7 +116,8 @@ extern "C" hp_status hp_solve_static(int device, void* stream, const hp_job* job
         return HP_ERR_INVALID_ARG;
     if (job->num_seeds != 0) return HP_ERR_UNSUPPORTED;  // the seed index map would need scratch
     if (job->num_sources < 1 || job->num_sources > HP_MAX_SOURCES || !(job->depth_min > 0.f) ||
-        !(job->depth_max > job->depth_min) || job->iterations < 0 || job->iterations > 1000)
+        !(job->depth_max > job->depth_min) || !std::isfinite(job->depth_max) || job->iterations < 0 ||
+        job->iterations > 1000)
         return HP_ERR_INVALID_ARG;
 
     int prev = -1;
@@ -88,8 +129,8 @@ extern "C" hp_status hp_solve_static(int device, void* stream, const hp_job* job
     } restore{prev != device ? prev : -1};
 
     unsigned char* base = nullptr;
-    cudaError_t e = scratch_address(device, &base);
-    if (e != cudaSuccess) return fail(e);
+    const cudaError_t se = scratch_address(device, &base);
+    if (se != cudaSuccess) return fail(se);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
 
     // Descriptor, built on the host and copied into the scratch header.
@@ -127,9 +168,16 @@ extern "C" hp_status hp_solve_static(int device, void* stream, const hp_job* job
     static_assert(sizeof(hp::ViewDesc) + 64 <= kHeaderBytes, "scratch header too small");
     const size_t list_off = (sizeof(hp::ViewDesc) + 255) & ~size_t(255);
     const int list[3] = {0, 0, d.tiles_x * d.tiles_y};
-    if ((e = cudaMemcpyAsync(base, &d, sizeof d, cudaMemcpyHostToDevice, st)) != cudaSuccess) return fail(e);
+    // Once anything is queued, a failure still waits for what was queued (it
+    // may be using the shared array) before returning.
+    auto bail = [st](cudaError_t err) {
+        cudaStreamSynchronize(st);
+        return fail(err);
+    };
+    cudaError_t e = cudaMemcpyAsync(base, &d, sizeof d, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return bail(e);
     if ((e = cudaMemcpyAsync(base + list_off, list, sizeof list, cudaMemcpyHostToDevice, st)) != cudaSuccess)
-        return fail(e);
+        return bail(e);
 
     hp::BatchList bl;
     bl.views = reinterpret_cast<const hp::ViewDesc*>(base);
@@ -145,12 +193,12 @@ extern "C" hp_status hp_solve_static(int device, void* stream, const hp_job* job
     sc.iter_decay = params->iter_decay;
     sc.step_decay = params->step_decay;
 
-    if ((e = hp::launch_init(bl, st)) != cudaSuccess) return fail(e);
-    if ((e = hp::launch_cost_f32(bl, sc, st)) != cudaSuccess) return fail(e);
+    if ((e = hp::launch_init(bl, st)) != cudaSuccess) return bail(e);
+    if ((e = hp::launch_cost_f32(bl, sc, st)) != cudaSuccess) return bail(e);
     for (int it = 0; it < job->iterations; ++it)
         for (int color = 0; color < 2; ++color)
-            if ((e = hp::launch_propagate_f32(bl, sc, it, color, st)) != cudaSuccess) return fail(e);
-    if ((e = hp::launch_unpack(&d, 0, out->depth, out->normal, out->cost, st)) != cudaSuccess) return fail(e);
+            if ((e = hp::launch_propagate_f32(bl, sc, it, color, st)) != cudaSuccess) return bail(e);
+    if ((e = hp::launch_unpack(&d, 0, out->depth, out->normal, out->cost, st)) != cudaSuccess) return bail(e);
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return fail(e);
     return HP_OK;
 }

@@ -266,9 +266,14 @@ hp_status hp_geometric_filter(hp_ctx* ctx, const hp_camera* ref_cam, int width, 
  *                     unnormalised coordinates, element read mode
  *   params            precision must be HP_PRECISION_F32
  *   out               device maps (memory HP_MEMORY_DEVICE)
- * The first call on a device looks up the scratch array's address; make it
- * before any stream capture.  All calls share the one array, so calls that
- * overlap in time (several host threads) race: serialise them. */
+ * The first call in a CUDA context looks up the scratch array's address in
+ * that context and caches it; make it before any stream capture.  The cache is
+ * keyed by the context's id, so after cudaDeviceReset (or with another context
+ * made current) the next call looks the address up again: the address a
+ * previous context had is never reused.  Completion: the call waits for every
+ * copy and kernel it queued, on success and on failure alike.  All calls share
+ * the one array, so calls that overlap in time (several host threads) race:
+ * serialise them. */
 hp_status hp_solve_static(int device, void* stream, const hp_job* job, const float* ref_image, int ref_pitch,
                           int width, int height, const unsigned long long* src_textures, const hp_params* params,
                           hp_maps* out);

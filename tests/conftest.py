@@ -16,6 +16,9 @@ for p in (ROOT, os.path.join(ROOT, "oracle"), os.path.join(ROOT, "oracle", "ref_
         sys.path.insert(0, p)
 
 PKG = "hemiphoto3d-private_b200"
+# The reference checkout, present only where fixtures are generated and its
+# headers compiled against; HP_REFERENCE_TREE overrides the default.
+REFERENCE_TREE = os.environ.get("HP_REFERENCE_TREE", "/root/reference")
 
 
 def pytest_configure(config):

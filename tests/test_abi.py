@@ -12,7 +12,7 @@ import tempfile
 import numpy as np
 import pytest
 
-from conftest import ROOT
+from conftest import REFERENCE_TREE, ROOT
 
 HEADER = os.path.join(ROOT, "include", "hpmvs.h")
 
@@ -139,7 +139,7 @@ def test_stage_adapter_compiles_against_reference_headers(tmp_path):
     """include/hpmvs_stage.hpp (runPatchMatchMVS and fuseDepthMaps on the C ABI) compiles inside the reference's
     own translation-unit context: its types.h / patchmatch_mvs.h, with the test-only stand-ins
     for the Eigen and OpenCV headers those include."""
-    ref = "/root/reference"
+    ref = REFERENCE_TREE
     if not os.path.isdir(os.path.join(ref, "src", "dense_recon")):
         pytest.skip("reference tree not present")
     src = tmp_path / "adapter.cpp"

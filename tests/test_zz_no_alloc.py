@@ -88,3 +88,13 @@ def test_static_scratch_solve_matches_solve(hp, scene_mod):
                                 C.byref(hp.maps_of(*[torch.zeros(1, device="cuda")] * 3)))
     assert st == 6  # HP_ERR_UNSUPPORTED
     assert hp.STATIC_MAX_PIXELS == 1280 * 1024
+
+    # A depth range hp_solve refuses is refused here too: a non-finite far plane.
+    inf_job = hp.make_job(0, [0], hp.make_camera(*cam_of(s, r)), [hp.make_camera(*cam_of(s, srcs[0]))], 1.0,
+                          float("inf"))
+    st = hp.lib.hp_solve_static(0, None, C.byref(inf_job), ref.data_ptr(), W, W, H, tex, C.byref(params),
+                                C.byref(hp.maps_of(*[torch.zeros(1, device="cuda")] * 3)))
+    assert st == 1  # HP_ERR_INVALID_ARG
+    # The Python wrapper checks the texture count against the job's sources.
+    with pytest.raises(ValueError):
+        hp.solve_static(job, params, ref, [0], hp.maps_of(*[torch.zeros(1, device="cuda")] * 3))
