@@ -19,8 +19,12 @@ independent, each rank solves its own 20-view batch (weak scaling, no
 collective on the data path); the step time is the max over ranks.
 
 --impl reference times the reference's algorithm on the host cores (the CPU
-restatement in oracle/, all threads): one red-black iteration of a band of
-rows of one view of the same workload per step.
+restatement in oracle/, all threads): one red-black iteration of view 0 of the
+same workload per step.  It loads nothing from the engine: the scene is
+rendered by oracle/libpmscene.so (the renderer's source, built apart), and
+where the reference's own kernels were compiled (oracle/_ref/libpmref.so) it
+also times them on the GPU ("reference_gpu") at the parameters they support -
+radius 5, stride 1 - which the engine arm times too ("reference_params").
 """
 from __future__ import annotations
 
@@ -59,8 +63,10 @@ def parse():
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
     ap.add_argument("--precision", choices=["f32", "f16acc"], default="f32",
                     help="headline arithmetic; the other is measured too and reported under 'variants'")
-    ap.add_argument("--e2e-steps", type=int, default=3)
-    ap.add_argument("--cpu-rows", type=int, default=256, help="rows of the CPU-baseline band sample")
+    ap.add_argument("--e2e-steps", type=int, default=None, help="end-to-end steps (default: --steps)")
+    ap.add_argument("--cpu-rows", type=int, default=1080, help="rows of the CPU-baseline sample (1080: all of view 0)")
+    ap.add_argument("--no-reference-params", action="store_true",
+                    help="skip timing the engine at the reference kernels' parameters")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--views", type=int, default=WORKLOAD["views"], help="reduce for profiling captures only")
@@ -140,10 +146,49 @@ def job_throughput(world: int, units_per_rank: float, steps: int, max_ms: float)
     return world * units_per_rank * steps / (max_ms / 1e3)
 
 
-def build_scene(views: int):
-    scene = importlib.import_module(PKG + ".scene")
+def scene_module(standalone: bool = False):
+    """The scene generator.  standalone: loaded from its file with the renderer built under oracle/, without
+    importing the engine package (the reference arm must not load the engine)."""
+    if not standalone:
+        return importlib.import_module(PKG + ".scene")
+    import importlib.util
+    os.environ["HP_SCENE_LIB"] = os.path.join(ROOT, "oracle", "libpmscene.so")
+    spec = importlib.util.spec_from_file_location("hp_scene_standalone", os.path.join(ROOT, PKG, "scene.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[spec.name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def build_scene(views: int, standalone: bool = False):
+    scene = scene_module(standalone)
     # The full 20-view arc is always rendered, so a reduced --views case keeps the workload's geometry.
     return scene.multi_object(n_views=max(views, WORKLOAD["views"]), n_refs=views)
+
+
+def workload_config(world: int, n_views: int) -> dict:
+    """The `config` object of both arms' lines."""
+    H, W = WORKLOAD["height"], WORKLOAD["width"]
+    return {"workload": WORKLOAD["name"], "views_per_gpu": n_views, "width": W, "height": H,
+            "sources": WORKLOAD["sources"], "window": f"{2 * WORKLOAD['radius'] + 1}x{2 * WORKLOAD['radius'] + 1}",
+            "stride": WORKLOAD["stride"], "iterations": WORKLOAD["iterations"], "depth_range": WORKLOAD["depth_range"],
+            "images": "u8", "parallelism": f"views/{world} ranks",
+            "mpix_iter_per_step": round(n_views * H * W * WORKLOAD["iterations"] / 1e6 * world, 3),
+            "l2": "inputs larger than L2 (20 x 2.07 Mpix images + 830 MB state per step), no flush"}
+
+
+# Workloads the reference's own kernels can run (radius <= 5, no stride), timed on the same B200 by both arms:
+# the engine arm through hp_solve ("reference_params"), the reference arm through oracle/_ref ("reference_gpu").
+REF_PARAM_WORKLOADS = [
+    dict(name="plane_sphere_5x640x480_r5_s1_it8", scene="plane_sphere", refs=[0, 1, 2, 3, 4], radius=5, stride=1,
+         iterations=8),
+    dict(name="multi_object_1920x1080_r5_s1_it12_2views", scene="multi_object", refs=[4, 13], radius=5, stride=1,
+         iterations=12),
+]
+
+
+def ref_param_scenes(scene_mod):
+    return {"plane_sphere": scene_mod.plane_sphere(), "multi_object": scene_mod.multi_object()}
 
 
 def cpu_sample(s, rows: int, reps: int = 1):
@@ -169,8 +214,8 @@ def cpu_sample(s, rows: int, reps: int = 1):
         dt = time.perf_counter() - t
         best = dt if best is None else min(best, dt)
     mpix = rows * W / 1e6
-    return mpix / best, best, po.num_threads(), (f"1 red-black iteration of rows [{y0},{y0 + rows}) x {W} of view 0 "
-                                                 f"(r=7, s=2, S=6), {po.num_threads()} threads")
+    return mpix / best, best, po.num_threads(), (f"1 red-black iteration (the first) of rows [{y0},{y0 + rows}) x {W} "
+                                                 f"of view 0 (r=7, s=2, S=6), {po.num_threads()} threads")
 
 
 def measure_peaks():
@@ -188,6 +233,17 @@ def measure_peaks():
         rc = f(*args, C.byref(v))
         out[name] = v.value if rc == 0 else None
     return out
+
+
+def load_executed_taps(kind: str):
+    """Taps actually sampled per pixel visit of the propagate launch, from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        e = json.load(open(p)).get(kind) or {}
+        v = e.get("executed_taps_per_pixel_visit")
+        return None if v is None else round(float(v), 1)
+    except (OSError, ValueError, TypeError):
+        return None
 
 
 def load_ncu_traffic(kind: str):
@@ -215,6 +271,7 @@ def run_engine(args, rank, world, local_rank):
     H, W = WORKLOAD["height"], WORKLOAD["width"]
     n_views = args.views
     units_per_step = n_views * H * W * WORKLOAD["iterations"] / 1e6  # Mpix*iter per rank
+    e2e_steps = args.e2e_steps or args.steps
 
     ctx = hp.Context(local_rank)
     stream = torch.cuda.ExternalStream(ctx.stream_handle, device=local_rank)
@@ -307,7 +364,7 @@ def run_engine(args, rank, world, local_rank):
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(args.e2e_steps):
+    for _ in range(e2e_steps):
         e2e_step()
     e1.record(stream)
     e1.synchronize()
@@ -343,6 +400,9 @@ def run_engine(args, rank, world, local_rank):
     fma_peak = onchip.get("fma_per_s")
 
     value = job_throughput(world, units_per_step, args.steps, ms)
+    smem_peak = onchip.get("smem_bytes_per_s")
+    l1_bytes_per_tap = 5 * b_img  # 4 bilinear source texels + 1 reference value, stored element width
+    executed = load_executed_taps(head)
     line = {
         "metric": METRIC,
         "value": round(value, 2),
@@ -356,36 +416,39 @@ def run_engine(args, rank, world, local_rank):
         "vs_baseline": None,
         "dtype": "f16acc" if head == "f16acc" else "f32",
         "data": "synthetic: seeded planes+spheres scene, renderer ground truth (no dataset)",
-        "config": {"workload": WORKLOAD["name"], "views_per_gpu": n_views, "width": W, "height": H,
-                   "sources": S, "window": f"{2 * WORKLOAD['radius'] + 1}x{2 * WORKLOAD['radius'] + 1}",
-                   "stride": WORKLOAD["stride"], "iterations": WORKLOAD["iterations"],
-                   "depth_range": WORKLOAD["depth_range"], "images": "u8", "parallelism": f"views/{world} ranks",
-                   "mpix_iter_per_step": round(units_per_step * world, 3),
-                   "l2": "inputs larger than L2 (20 x 2.07 Mpix images + 830 MB state per step), no flush"},
-        "e2e": {"value": round(job_throughput(world, units_per_step, args.e2e_steps, e2e_ms), 2), "unit": "Mpix*iter/s",
-                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": args.e2e_steps},
-        "roofline": {"bound": "hbm", "achieved": round(achieved_hbm, 2), "peak": hbm_peak, "unit": "GB/s",
-                     "frac": round(achieved_hbm / hbm_peak, 5), "peak_source": hbm_src,
+        "config": workload_config(world, n_views),
+        "e2e": {"value": round(job_throughput(world, units_per_step, e2e_steps, e2e_ms), 2), "unit": "Mpix*iter/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": e2e_steps},
+        # The survey's reported figure for the dominant kernel: algorithmic on-chip gather bytes (4 bilinear
+        # texels of the source + 1 reference value per tap, at the stored element width; taps counted as
+        # 6 candidates x S sources x N_w window taps per pixel visit, with no skips) per CUDA-event launch
+        # duration, against the shared-memory/L1 read bandwidth measured live on the same GPU.
+        "roofline": {"bound": "l1", "achieved": round(fetch_rate * l1_bytes_per_tap / 1e9, 1),
+                     "peak": None if not smem_peak else round(smem_peak / 1e9, 1), "unit": "GB/s",
+                     "frac": None if not smem_peak else round(fetch_rate * l1_bytes_per_tap / smem_peak, 4),
+                     "peak_source": "measured live (shared-memory streaming microbenchmark, lib/libhppeaks.so)",
                      "traffic": None if traffic_per_visit is None else round(traffic_per_visit * visits),
-                     "kernel": "propagate half-pass", "ms_per_launch": round(prop_ms, 4),
-                     "algorithmic_bytes_per_launch": int(visits * hbm_bytes_per_visit),
-                     "note": "compulsory DRAM bytes; HBM does not bind this kernel - see roofline_tex"},
+                     "traffic_note": "DRAM bytes per launch (ncu dram__bytes_read+write, scaled per pixel visit)",
+                     "kernel": ("propagate16_kernel<7,2>" if head == "f16acc" else "propagate_kernel<7,2>")
+                               + " (red-black half-pass)",
+                     "ms_per_launch": round(prop_ms, 4), "launches_timed": prop_launches,
+                     "algorithmic_bytes_per_launch": int(visits * taps_per_visit * l1_bytes_per_tap),
+                     "algorithmic_taps_per_visit": taps_per_visit,
+                     "executed_taps_per_visit": executed,
+                     "executed_note": "taps actually sampled per pixel visit (ncu thread-level sampling "
+                                      "instructions; duplicate neighbour planes and wholly-outside sources skip "
+                                      "theirs), from profiles/ncu_traffic.json"},
+        "roofline_hbm": {"bound": "hbm", "achieved": round(achieved_hbm, 2), "peak": hbm_peak, "unit": "GB/s",
+                         "frac": round(achieved_hbm / hbm_peak, 5), "peak_source": hbm_src + " (MEASURED_PEAKS.json)",
+                         "traffic": None if traffic_per_visit is None else round(traffic_per_visit * visits),
+                         "algorithmic_bytes_per_launch": int(visits * hbm_bytes_per_visit),
+                         "note": "compulsory DRAM bytes per launch; HBM does not bind this kernel"},
         "roofline_tex": {"bound": "texture-filter fetches" if head == "f32" else
                          "bilinear taps (software sampler; the texture rate is the reference ceiling)", "achieved": round(fetch_rate / 1e9, 2),
                          "peak": None if tex_peak is None else round(tex_peak / 1e9, 2), "unit": "Gfetch/s",
                          "frac": None if not tex_peak else round(fetch_rate / tex_peak, 4),
                          "peak_source": "measured live (L1-resident bilinear fetch microbenchmark)",
                          "algorithmic_fetches_per_launch": int(visits * taps_per_visit)},
-        # On-chip gather bytes (4 bilinear texels of the source + 1 reference value per tap, at the stored
-        # element width) against the measured shared-memory/L1 read bandwidth.
-        "roofline_l1": {"bound": "L1/shared gather bytes",
-                        "achieved": round(fetch_rate * (4 * b_img + b_img) / 1e9, 1),
-                        "peak": None if not onchip.get("smem_bytes_per_s") else round(onchip["smem_bytes_per_s"] / 1e9, 1),
-                        "unit": "GB/s",
-                        "frac": None if not onchip.get("smem_bytes_per_s")
-                        else round(fetch_rate * 5 * b_img / onchip["smem_bytes_per_s"], 4),
-                        "bytes_per_tap": 5 * b_img,
-                        "peak_source": "measured live (shared-memory streaming microbenchmark)"},
         "roofline_fp32": {"achieved_fma_equiv": None if fma_peak is None else round(fetch_rate * 14 / 1e12, 3),
                           "peak_fma": None if fma_peak is None else round(fma_peak / 1e12, 3), "unit": "TFMA/s",
                           "note": "~14 FMA-equivalent issue slots per tap on the FP32 path (28 ops)"},
@@ -400,9 +463,18 @@ def run_engine(args, rank, world, local_rank):
         rate_v = visits * taps_per_visit / (var["propagate_ms_per_launch"] * 1e-3)
         var["taps_per_s"] = rate_v
         if onchip.get("smem_bytes_per_s"):
-            var["roofline_l1"] = {"achieved": round(rate_v * 5 * b_v / 1e9, 1), "unit": "GB/s",
-                                  "frac": round(rate_v * 5 * b_v / onchip["smem_bytes_per_s"], 4)}
+            var["roofline"] = {"bound": "l1", "achieved": round(rate_v * 5 * b_v / 1e9, 1), "unit": "GB/s",
+                               "frac": round(rate_v * 5 * b_v / onchip["smem_bytes_per_s"], 4),
+                               "kernel": ("propagate16_kernel<7,2>" if name == "f16acc" else "propagate_kernel<7,2>"),
+                               "ms_per_launch": round(var["propagate_ms_per_launch"], 4),
+                               "executed_taps_per_visit": load_executed_taps(name)}
+    if "f16acc" in variants or head == "f16acc":
+        f16v = value if head == "f16acc" else variants["f16acc"]["value"]
+        f32v = value if head == "f32" else variants["f32"]["value"]
+        line["f16acc_over_f32"] = round(f16v / f32v, 3)
     line["fusion"] = run_fusion(hp, ctx, s, dev_maps, n_views, stream)
+    if world == 1 and not args.no_reference_params:
+        line["reference_params"] = run_reference_params(hp, ctx, stream)
     if world == 1 and not args.no_serving:
         line["serving"] = run_serving(args, hp, local_rank)
     if world == 1 and not args.no_batched:
@@ -623,11 +695,90 @@ def run_serving(args, hp, device: int):
     }
 
 
+def run_reference_params(hp, ctx, stream):
+    """The engine at the parameters the reference's own kernels support (REF_PARAM_WORKLOADS: radius 5, stride 1),
+    per view as the reference solves (one hp_solve per view), FP32 and FP16-acc, device-resident maps, CUDA
+    events on the engine's stream.  The reference arm times the reference's kernels on the same workloads."""
+    import torch
+    scenes = ref_param_scenes(importlib.import_module(PKG + ".scene"))
+    out = {}
+    for wl in REF_PARAM_WORKLOADS:
+        sc = scenes[wl["scene"]]
+        ids = [ctx.upload(v.image) for v in sc.views]
+        cam = lambda i: hp.make_camera(sc.views[i].cam.K, sc.views[i].cam.R, sc.views[i].cam.t)
+        H, W = sc.height, sc.width
+        maps = hp.maps_of(torch.empty(H, W, device="cuda"), torch.empty(H, W, 3, device="cuda"),
+                          torch.empty(H, W, device="cuda"))
+        res = {"views": len(wl["refs"]), "width": W, "height": H, "sources": len(sc.sources[wl["refs"][0]]),
+               "radius": wl["radius"], "stride": wl["stride"], "iterations": wl["iterations"]}
+        for prec, pk in (("f32", hp.PRECISION_F32), ("f16acc", hp.PRECISION_F16ACC)):
+            params = hp.default_params(radius=wl["radius"], stride=wl["stride"], precision=pk)
+            total = 0.0
+            for r in wl["refs"]:
+                job = hp.make_job(ids[r], [ids[i] for i in sc.sources[r]], cam(r), [cam(i) for i in sc.sources[r]],
+                                  *sc.depth_range, seed=42 + 1_000_000 * r, view_id=r, iterations=wl["iterations"])
+                ctx.solve([job], params, [maps])  # warm-up
+                best = None
+                for _ in range(3):
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    ctx.solve([job], params, [maps])
+                    e1.record(stream)
+                    e1.synchronize()
+                    t = e0.elapsed_time(e1)
+                    best = t if best is None else min(best, t)
+                total += best
+            res[prec] = {"ms": round(total, 3),
+                         "mpix_iter_per_s": round(len(wl["refs"]) * H * W * wl["iterations"] / 1e6 / (total / 1e3), 1)}
+        for i in ids:
+            ctx.release(i)
+        out[wl["name"]] = res
+    return out
+
+
+def run_reference_gpu(scene_mod):
+    """The reference's own kernels (oracle/_ref/libpmref.so: patchmatch_mvs.cu compiled unmodified) on
+    REF_PARAM_WORKLOADS, on this box's GPU: pmref.solve_view = init, initial cost and the red-black passes
+    of runPatchMatchMVS (:1094-1107, :1189-1232) with its per-launch device synchronisations, timed by CUDA
+    events from the init launch to the last pass; best of 3 per view."""
+    import pmref
+    if not pmref.available():
+        return {"unavailable": "oracle/_ref/libpmref.so not built (needs the reference tree at build time)"}
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return {"unavailable": "no GPU"}
+    except ImportError:
+        return {"unavailable": "torch missing"}
+    scenes = ref_param_scenes(scene_mod)
+    out = {}
+    for wl in REF_PARAM_WORKLOADS:
+        sc = scenes[wl["scene"]]
+        cam = lambda i: (sc.views[i].cam.K, sc.views[i].cam.R, sc.views[i].cam.t)
+        total = 0.0
+        for r in wl["refs"]:
+            srcs = sc.sources[r]
+            kinv, ab = pmref.setup_views(cam(r), [cam(i) for i in srcs])
+            args = (sc.views[r].image_f32, [sc.views[i].image_f32 for i in srcs], kinv, ab, *sc.depth_range,
+                    wl["radius"], wl["iterations"], r)
+            pmref.solve_view(*args)  # warm-up
+            total += min(pmref.solve_view(*args)[3] for _ in range(3))
+        out[wl["name"]] = {"views": len(wl["refs"]), "width": sc.width, "height": sc.height,
+                           "sources": len(sc.sources[wl["refs"][0]]), "radius": wl["radius"], "stride": wl["stride"],
+                           "iterations": wl["iterations"], "ms": round(total, 3),
+                           "mpix_iter_per_s": round(len(wl["refs"]) * sc.width * sc.height * wl["iterations"] / 1e6
+                                                    / (total / 1e3), 1)}
+    return out
+
+
 def run_reference(args, rank, world):
-    """The reference's algorithm on the host cores (CPU restatement, all threads)."""
+    """The reference's algorithm on the host cores (CPU restatement, all threads), and - where the reference's
+    kernels were compiled - those kernels on the GPU at the parameters they support.  Nothing of the engine is
+    loaded: the scene comes from the renderer built under oracle/."""
     if rank != 0:
         return None
-    s = build_scene(1)
+    scene_mod = scene_module(standalone=True)
+    s = scene_mod.multi_object(n_views=WORKLOAD["views"], n_refs=1)
     rates = []
     desc = thr = None
     for i in range(args.warmup + args.steps):
@@ -635,15 +786,17 @@ def run_reference(args, rank, world):
         if i >= args.warmup:
             rates.append(rate)
     v = float(np.median(rates))
-    return {
+    line = {
         "impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": "Mpix*iter/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "data": "synthetic: seeded planes+spheres scene",
-        "config": {"workload": WORKLOAD["name"], "sources": WORKLOAD["sources"], "window": "15x15", "stride": 2,
-                   "images": "u8"},
+        "dtype": "f32", "data": "synthetic: seeded planes+spheres scene, renderer ground truth (no dataset)",
+        "config": workload_config(world, WORKLOAD["views"]),
         "cpu_baseline": {"value": round(v, 4), "unit": "Mpix*iter/s", "cores": thr, "kind": "port", "sample": desc},
         "e2e": {"value": round(v, 4), "unit": "Mpix*iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if not args.no_reference_params:
+        line["reference_gpu"] = run_reference_gpu(scene_mod)
+    return line
 
 
 def main():

@@ -30,6 +30,11 @@ STATUS_NAMES = {
 }
 DTYPE_U8, DTYPE_F16, DTYPE_F32 = 0, 1, 2
 PRECISION_F32, PRECISION_F16ACC = 0, 1
+# runPatchMatchMVS's geometric-filter constants (patchmatch_mvs.cu:1273-1276):
+# 12% relative depth, normal check off (cos 180 deg), 2 agreeing sources.
+GEOM_DEPTH_TOL = 0.12
+GEOM_NORMAL_COS = -1.0
+GEOM_MIN_CONSISTENT = 2
 MEMORY_HOST, MEMORY_DEVICE = 0, 1
 
 
@@ -50,6 +55,7 @@ class Params(C.Structure):
         ("radius", C.c_int), ("stride", C.c_int), ("top_k", C.c_int), ("precision", C.c_int),
         ("refine_steps", C.c_int), ("iter_decay", C.c_float), ("step_decay", C.c_float),
         ("tile_w", C.c_int), ("tile_h", C.c_int), ("soft_sources", C.c_int),
+        ("filter_min_consistent", C.c_int), ("filter_depth_tol", C.c_float), ("filter_normal_cos", C.c_float),
     ]
 
 
@@ -65,7 +71,8 @@ class Job(C.Structure):
 
 
 class Maps(C.Structure):
-    _fields_ = [("memory", C.c_int), ("depth", C.c_void_p), ("normal", C.c_void_p), ("cost", C.c_void_p)]
+    _fields_ = [("memory", C.c_int), ("depth", C.c_void_p), ("normal", C.c_void_p), ("cost", C.c_void_p),
+                ("confidence", C.c_void_p)]
 
 
 KERNEL_KINDS = ("init", "cost", "propagate", "other", "persistent")
@@ -744,22 +751,28 @@ def make_job(ref_image: int, src_images: Sequence[int], ref_cam: Camera, src_cam
     return j
 
 
-def host_maps(h: int, w: int):
-    """(Maps, depth, normal, cost) with fresh host arrays."""
+def host_maps(h: int, w: int, confidence: bool = False):
+    """(Maps, depth, normal, cost) with fresh host arrays; with ``confidence`` a
+    fifth array, the confidence map, is bound and returned too."""
     depth = np.zeros((h, w), np.float32)
     normal = np.zeros((h, w, 3), np.float32)
     cost = np.zeros((h, w), np.float32)
+    if confidence:
+        conf = np.zeros((h, w), np.float32)
+        return maps_of(depth, normal, cost, conf), depth, normal, cost, conf
     return maps_of(depth, normal, cost), depth, normal, cost
 
 
-def maps_of(depth, normal, cost) -> Maps:
+def maps_of(depth, normal, cost, confidence=None) -> Maps:
     """Maps over existing arrays (host numpy or device tensors, not mixed).
 
-    The returned struct keeps the arrays alive (``.arrays``): the engine writes
+    ``confidence`` (optional) receives 1 - cost / 2, formed on the device.  The
+    returned struct keeps the arrays alive (``.arrays``): the engine writes
     through its raw pointers, so the arrays must outlive every call using it.
     """
-    m = Maps(_mem(depth), _ptr(depth), _ptr(normal), _ptr(cost))
-    m.arrays = (depth, normal, cost)
+    m = Maps(_mem(depth), _ptr(depth), _ptr(normal), _ptr(cost),
+             _ptr(confidence) if confidence is not None else None)
+    m.arrays = (depth, normal, cost, confidence)
     return m
 
 
@@ -850,6 +863,15 @@ def run_patchmatch_mvs(images: Sequence[np.ndarray], cameras: Sequence[Camera],
     try:
         radius = min(MAX_RADIUS, max(1, (config.mvs_patch_size - 1) // 2))
         params = default_params(radius=radius, stride=config.window_stride, precision=config.precision)
+        # The reference writes each view's depth before filtering (:1254-1257); with
+        # intermediates wanted the filter therefore runs after the write, on the host
+        # maps, through hp_geometric_filter (the same check, bit for bit).
+        fused = config.geometric_filter and not (config.save_intermediate and config.output_dir)
+        if fused:
+            # The reference's constants (:1273-1276): 12% depth, normal check off, 2 sources.
+            params.filter_min_consistent = GEOM_MIN_CONSISTENT
+            params.filter_depth_tol = GEOM_DEPTH_TOL
+            params.filter_normal_cos = GEOM_NORMAL_COS
         if views is None:
             if sfm is None:
                 raise ValueError("run_patchmatch_mvs needs views or sfm points")
@@ -866,7 +888,7 @@ def run_patchmatch_mvs(images: Sequence[np.ndarray], cameras: Sequence[Camera],
         jobs, outs, maps = [], [], []
         for v in views:
             h, w = images[v.ref_image_id].shape[:2]
-            m, d, n, c = host_maps(h, w)
+            m, d, n, c, cf = host_maps(h, w, confidence=True)
             job = make_job(ids[v.ref_image_id], [ids[s] for s in v.source_ids], cameras[v.ref_image_id],
                            [cameras[s] for s in v.source_ids], v.depth_min, v.depth_max,
                            seed=42 + 1_000_000 * v.ref_image_id, view_id=v.ref_image_id,
@@ -876,24 +898,26 @@ def run_patchmatch_mvs(images: Sequence[np.ndarray], cameras: Sequence[Camera],
                                               sfm), config.seed_radius)
             jobs.append(job)
             outs.append(m)
-            maps.append((d, n, c))
+            maps.append((d, n, c, cf))
         if jobs:
+            # The geometric filter is the solve's last stage (params.filter_*):
+            # in place and in view order on the device, as the reference's loop.
             ctx.solve(jobs, params, outs)
-        result = [DepthMap(v.ref_image_id, d, n, (1.0 - c * 0.5).astype(np.float32), c)
-                  for v, (d, n, c) in zip(views, maps)]
-        if config.geometric_filter and config.mvs_iterations > 0 and len(result) >= 2:
-            # In place and in view order, as the reference does: a later view
-            # checks against sources already filtered earlier in the loop.
-            by_id = {dm.image_id: dm for dm in result}
-            for v, dm in zip(views, result):
-                srcs = [s for s in v.source_ids if s in by_id and by_id[s].depth.shape == dm.depth.shape]
-                if len(srcs) >= 2:
-                    ctx.geometric_filter(cameras[v.ref_image_id], dm.depth, dm.normal, dm.confidence,
-                                         [cameras[s] for s in srcs], [by_id[s].depth for s in srcs],
-                                         [by_id[s].normal for s in srcs])
+        result = [DepthMap(v.ref_image_id, d, n, cf, c) for v, (d, n, c, cf) in zip(views, maps)]
         if config.save_intermediate and config.output_dir:
             for dm in result:
                 pfm_write(os.path.join(config.output_dir, f"depth_{dm.image_id}.pfm"), dm.depth)
+        if config.geometric_filter and not fused and config.mvs_iterations > 0 and len(result) >= 2:
+            # In place and in view order: a later view sees earlier views filtered.
+            by_id = {dm.image_id: dm for dm in result}
+            for v, dm in zip(views, result):
+                srcs = [s for s in v.source_ids
+                        if s in by_id and s != v.ref_image_id and by_id[s].depth.shape == dm.depth.shape]
+                if len(srcs) >= GEOM_MIN_CONSISTENT:
+                    ctx.geometric_filter(cameras[v.ref_image_id], dm.depth, dm.normal, dm.confidence,
+                                         [cameras[s] for s in srcs], [by_id[s].depth for s in srcs],
+                                         [by_id[s].normal for s in srcs])
+                    dm.cost[dm.confidence == 0] = 2.0
         for i in ids.values():
             ctx.release(i)
         return result

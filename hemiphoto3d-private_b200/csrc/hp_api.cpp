@@ -67,6 +67,12 @@ hp_status check_params(hp_ctx* ctx, const hp_params* p) {
         return fail(ctx, HP_ERR_INVALID_ARG, "refine_steps %d outside 0..4", p->refine_steps);
     if (!(p->iter_decay > 0.f && p->iter_decay <= 1.f) || !(p->step_decay > 0.f && p->step_decay <= 1.f))
         return fail(ctx, HP_ERR_INVALID_ARG, "decay factors must lie in (0, 1]");
+    if (p->filter_min_consistent < 0 || p->filter_min_consistent > HP_MAX_SOURCES)
+        return fail(ctx, HP_ERR_INVALID_ARG, "filter_min_consistent %d outside 0..%d", p->filter_min_consistent,
+                    HP_MAX_SOURCES);
+    if (p->filter_min_consistent > 0 &&
+        (!(p->filter_depth_tol >= 0.f) || !std::isfinite(p->filter_depth_tol) || std::isnan(p->filter_normal_cos)))
+        return fail(ctx, HP_ERR_INVALID_ARG, "filter tolerances invalid");
     if ((p->tile_w != 0 && p->tile_w != hp::TILE_W) || (p->tile_h != 0 && p->tile_h != hp::TILE_H))
         return fail(ctx, HP_ERR_UNSUPPORTED, "tile %dx%d: the kernels use %dx%d tiles", p->tile_w, p->tile_h,
                     hp::TILE_W, hp::TILE_H);
@@ -174,6 +180,62 @@ cudaError_t stage_seeds(const hp_job* j, void* area, hp::ViewDesc* d, cudaStream
     return e;
 }
 
+bool filter_source_of(const hp_camera& ref, const hp_camera& src, hp::FilterSource* q) {
+    double kinv[9];
+    if (!mat3_inv(ref.K, kinv)) return false;
+    double RrT[9], Rrel[9], M[9], A[9], trel[3];
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) RrT[3 * r + c] = ref.R[3 * c + r];
+    mat3_mul(src.R, RrT, Rrel);  // reference camera frame -> source camera frame
+    for (int r = 0; r < 3; ++r)
+        trel[r] = src.t[r] - (Rrel[3 * r] * ref.t[0] + Rrel[3 * r + 1] * ref.t[1] + Rrel[3 * r + 2] * ref.t[2]);
+    mat3_mul(Rrel, kinv, M);  // pixel ray -> source camera frame
+    mat3_mul(src.K, M, A);
+    for (int i = 0; i < 9; ++i) {
+        q->A[i] = static_cast<float>(A[i]);
+        q->Rn[i] = static_cast<float>(Rrel[i]);
+    }
+    for (int r = 0; r < 3; ++r)
+        q->b[r] = static_cast<float>(src.K[3 * r] * trel[0] + src.K[3 * r + 1] * trel[1] + src.K[3 * r + 2] * trel[2]);
+    for (int c = 0; c < 3; ++c) q->m[c] = static_cast<float>(M[6 + c]);
+    q->cz = static_cast<float>(trel[2]);
+    q->view = -1;
+    return true;
+}
+
+void filter_stages(const hp_job* jobs, int n, const hp_params* p, const std::vector<hp::ViewDesc>& descs,
+                   std::vector<hp::FilterStage>* stages, std::vector<char>* has, std::vector<int>* order) {
+    stages->assign(n, hp::FilterStage{});
+    has->assign(n, 0);
+    order->clear();
+    if (!p || p->filter_min_consistent <= 0 || n < 2) return;
+    std::map<int, int> solved;  // ref image -> the last job solving it
+    for (int k = 0; k < n; ++k) solved[jobs[k].ref_image] = k;
+    for (int k = 0; k < n; ++k) {
+        if (jobs[k].iterations <= 0) continue;
+        hp::FilterStage& f = (*stages)[k];
+        std::memset(&f, 0, sizeof f);
+        for (int i = 0; i < jobs[k].num_sources; ++i) {
+            auto it = solved.find(jobs[k].src_images[i]);
+            if (it == solved.end() || it->second == k) continue;
+            const int j = it->second;
+            if (descs[j].W != descs[k].W || descs[j].H != descs[k].H) continue;
+            hp::FilterSource& q = f.src[f.n];
+            if (!filter_source_of(jobs[k].ref_cam, jobs[k].src_cams[i], &q)) continue;
+            q.view = j;
+            ++f.n;
+        }
+        if (f.n < p->filter_min_consistent) continue;
+        f.min_consistent = p->filter_min_consistent;
+        f.depth_tol = p->filter_depth_tol;
+        f.normal_cos = p->filter_normal_cos;
+        f.prev = order->empty() ? -1 : order->back();
+        f.tiles_done = nullptr;
+        (*has)[k] = 1;
+        order->push_back(k);
+    }
+}
+
 }  // namespace hpx
 
 namespace {
@@ -187,9 +249,11 @@ struct Prepared {
     std::vector<int> list_tiles;      // per iteration: total tiles
     int* lists = nullptr;
     int max_iter = 0;
+    std::vector<int> filter_order;    // jobs with a filter stage, in the order they run
 };
 
-hp_status prepare(hp_ctx* ctx, const hp_job* jobs, int n, Prepared* P, bool with_seeds = false) {
+hp_status prepare(hp_ctx* ctx, const hp_job* jobs, int n, Prepared* P, bool with_seeds = false,
+                  const hp_params* filter = nullptr) {
     P->host.resize(n);
     size_t state_bytes = 0;
     std::vector<size_t> offs(n);
@@ -220,6 +284,18 @@ hp_status prepare(hp_ctx* ctx, const hp_job* jobs, int n, Prepared* P, bool with
         for (int k = 0; k < n; ++k) {
             HP_CUDA(stage_seeds(&jobs[k], static_cast<char*>(ctx->seedbuf.p) + off, &P->host[k], ctx->stream));
             off += seed_area_bytes(&jobs[k], P->host[k].W, P->host[k].H);
+        }
+    }
+    {  // geometric-consistency stages after the last half-pass (hp_params.filter_*)
+        std::vector<hp::FilterStage> stages;
+        std::vector<char> has;
+        filter_stages(jobs, n, filter, P->host, &stages, &has, &P->filter_order);
+        if (!P->filter_order.empty()) {
+            HP_CUDA(ctx->filters.ensure(n * sizeof(hp::FilterStage)));
+            hp::FilterStage* fd = static_cast<hp::FilterStage*>(ctx->filters.p);
+            HP_CUDA(cudaMemcpyAsync(fd, stages.data(), n * sizeof(hp::FilterStage), cudaMemcpyHostToDevice,
+                                    ctx->stream));
+            for (int k = 0; k < n; ++k) P->host[k].filter = has[k] ? fd + k : nullptr;
         }
     }
     HP_CUDA(ctx->descs.ensure(n * sizeof(hp::ViewDesc)));
@@ -272,21 +348,25 @@ hp_status export_maps(hp_ctx* ctx, const Prepared& P, int k, hp_maps* m, bool wa
     float* d = want_depth_normal ? m->depth : nullptr;
     float* nrm = want_depth_normal ? m->normal : nullptr;
     float* c = want_cost ? m->cost : nullptr;
+    float* cf = want_cost ? m->confidence : nullptr;
     if (m->memory == HP_MEMORY_DEVICE) {
-        HP_CUDA(counted(ctx, HP_KERNEL_OTHER, [&] { return hp::launch_unpack(P.host.data(), k, d, nrm, c, ctx->stream); }));
+        HP_CUDA(counted(ctx, HP_KERNEL_OTHER,
+                        [&] { return hp::launch_unpack(P.host.data(), k, d, nrm, c, cf, ctx->stream); }));
         return HP_OK;
     }
-    HP_CUDA(ctx->staging.ensure(px * 5 * sizeof(float)));
+    HP_CUDA(ctx->staging.ensure(px * 6 * sizeof(float)));
     float* sd = static_cast<float*>(ctx->staging.p);
     float* sn = sd + px;
     float* sc = sn + 3 * px;
+    float* scf = sc + px;
     HP_CUDA(counted(ctx, HP_KERNEL_OTHER, [&] {
         return hp::launch_unpack(P.host.data(), k, d ? sd : nullptr, nrm ? sn : nullptr, c ? sc : nullptr,
-                                 ctx->stream);
+                                 cf ? scf : nullptr, ctx->stream);
     }));
     if (d) HP_CUDA(cudaMemcpyAsync(d, sd, px * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
     if (nrm) HP_CUDA(cudaMemcpyAsync(nrm, sn, 3 * px * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
     if (c) HP_CUDA(cudaMemcpyAsync(c, sc, px * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    if (cf) HP_CUDA(cudaMemcpyAsync(cf, scf, px * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
     HP_CUDA(cudaStreamSynchronize(ctx->stream));
     flush_profile(ctx);
     return HP_OK;
@@ -407,6 +487,9 @@ void hp_params_default(hp_params* p) {
     p->tile_w = 0;
     p->tile_h = 0;
     p->soft_sources = -1;
+    p->filter_min_consistent = 0;
+    p->filter_depth_tol = 0.12f;
+    p->filter_normal_cos = -1.0f;
 }
 
 hp_status hp_ctx_create(int device, hp_ctx** out) {
@@ -439,6 +522,7 @@ hp_status hp_ctx_destroy(hp_ctx* ctx) {
         ctx->lists.release();
         ctx->staging.release();
         ctx->seedbuf.release();
+        ctx->filters.release();
         for (cudaEvent_t e : ctx->events) cudaEventDestroy(e);
         cudaStreamDestroy(ctx->stream);
     }
@@ -654,7 +738,7 @@ hp_status hp_solve(hp_ctx* ctx, const hp_job* jobs, int num_jobs, const hp_param
     }
     DeviceGuard g(ctx->device);
     Prepared P;
-    if ((st = prepare(ctx, jobs, num_jobs, &P, true)) != HP_OK) return st;
+    if ((st = prepare(ctx, jobs, num_jobs, &P, true, params)) != HP_OK) return st;
     hp::BatchList all = batch_of(P, 0);
     HP_CUDA(counted(ctx, HP_KERNEL_INIT, [&] { return hp::launch_init(all, ctx->stream); }));
     if ((st = launch_cost(ctx, all, params)) != HP_OK) return st;
@@ -662,6 +746,13 @@ hp_status hp_solve(hp_ctx* ctx, const hp_job* jobs, int num_jobs, const hp_param
         hp::BatchList bl = batch_of(P, 1 + it);
         if ((st = launch_pass(ctx, bl, params, it, 0)) != HP_OK) return st;
         if ((st = launch_pass(ctx, bl, params, it, 1)) != HP_OK) return st;
+    }
+    // Geometric-consistency stage, view by view in job order, in place on the
+    // packed state (each launch sees the earlier views already filtered).
+    for (int k : P.filter_order) {
+        const int tiles = P.host[k].tiles_x * P.host[k].tiles_y;
+        HP_CUDA(counted(ctx, HP_KERNEL_OTHER,
+                        [&] { return hp::launch_filter_view(P.dev, k, tiles, false, ctx->stream); }));
     }
     for (int k = 0; k < num_jobs; ++k)
         if ((st = export_maps(ctx, P, k, &out[k], true, true)) != HP_OK) return st;
@@ -731,29 +822,21 @@ hp_status hp_geometric_filter(hp_ctx* ctx, const hp_camera* ref_cam, int width, 
         return fail(ctx, HP_ERR_INVALID_ARG, "geometric_filter: num_sources %d outside 0..%d", num_sources,
                     HP_MAX_SOURCES);
     if (width < 1 || height < 1) return fail(ctx, HP_ERR_INVALID_ARG, "geometric_filter: empty map");
+    if (min_consistent < 0 || !(depth_tol >= 0.f) || std::isnan(normal_tol_cos))
+        return fail(ctx, HP_ERR_INVALID_ARG, "geometric_filter: tolerances invalid");
     DeviceGuard g(ctx->device);
-    hp::FilterArgs a;
+    hp::FilterMaps a;
     std::memset(&a, 0, sizeof a);
-    double kinv[9];
-    if (!mat3_inv(ref_cam->K, kinv)) return fail(ctx, HP_ERR_INVALID_ARG, "geometric_filter: singular K");
-    for (int i = 0; i < 9; ++i) {
-        a.ref_kinv[i] = static_cast<float>(kinv[i]);
-        a.ref_R[i] = static_cast<float>(ref_cam->R[i]);
-    }
-    for (int i = 0; i < 3; ++i) a.ref_t[i] = static_cast<float>(ref_cam->t[i]);
-    for (int s = 0; s < num_sources; ++s) {
-        for (int i = 0; i < 9; ++i) {
-            a.src[s].K[i] = static_cast<float>(src_cams[s].K[i]);
-            a.src[s].R[i] = static_cast<float>(src_cams[s].R[i]);
-        }
-        for (int i = 0; i < 3; ++i) a.src[s].t[i] = static_cast<float>(src_cams[s].t[i]);
-    }
-    a.S = num_sources;
+    for (int s = 0; s < num_sources; ++s)
+        if (!filter_source_of(*ref_cam, src_cams[s], &a.f.src[s]))
+            return fail(ctx, HP_ERR_INVALID_ARG, "geometric_filter: singular reference K");
+    a.f.n = num_sources;
+    a.f.min_consistent = min_consistent;
+    a.f.depth_tol = depth_tol;
+    a.f.normal_cos = normal_tol_cos;
+    a.f.prev = -1;
     a.W = width;
     a.H = height;
-    a.depth_tol = depth_tol;
-    a.normal_tol_cos = normal_tol_cos;
-    a.min_consistent = min_consistent;
     const size_t px = static_cast<size_t>(width) * height;
     if (memory == HP_MEMORY_DEVICE) {
         for (int s = 0; s < num_sources; ++s) {
@@ -761,8 +844,9 @@ hp_status hp_geometric_filter(hp_ctx* ctx, const hp_camera* ref_cam, int width, 
             a.src_normal[s] = src_normals[s];
         }
         HP_CUDA(counted(ctx, HP_KERNEL_OTHER,
-                        [&] { return hp::launch_geometric_filter(a, depth, normal, confidence, ctx->stream); }));
+                        [&] { return hp::launch_filter_maps(a, depth, normal, confidence, ctx->stream); }));
         HP_CUDA(cudaStreamSynchronize(ctx->stream));
+        flush_profile(ctx);
         return HP_OK;
     }
     // Host maps: stage ref (depth, normal, conf) and every source map once.
@@ -782,7 +866,7 @@ hp_status hp_geometric_filter(hp_ctx* ctx, const hp_camera* ref_cam, int width, 
         a.src_depth[s] = dd;
         a.src_normal[s] = dd + px;
     }
-    HP_CUDA(counted(ctx, HP_KERNEL_OTHER, [&] { return hp::launch_geometric_filter(a, sd, sn, sc, ctx->stream); }));
+    HP_CUDA(counted(ctx, HP_KERNEL_OTHER, [&] { return hp::launch_filter_maps(a, sd, sn, sc, ctx->stream); }));
     HP_CUDA(cudaMemcpyAsync(depth, sd, px * 4, cudaMemcpyDeviceToHost, ctx->stream));
     HP_CUDA(cudaMemcpyAsync(confidence, sc, px * 4, cudaMemcpyDeviceToHost, ctx->stream));
     HP_CUDA(cudaStreamSynchronize(ctx->stream));

@@ -79,6 +79,7 @@ struct hp_ctx {
     hpx::DevBuf staging; // host-memory results pass through here
     hpx::DevBuf seedbuf; // SfM seeds of one job and their W*H index map
     hpx::DevBuf upload;  // host images land here before conversion
+    hpx::DevBuf filters; // FilterStage per filtered job of a solve
     // Released images kept for reuse by the next upload of the same size
     // (their planes, arrays, texture objects and quad plane), oldest first,
     // up to image_cache_limit bytes.
@@ -172,6 +173,15 @@ hp_status fill_desc(hp_ctx* ctx, const hp_job* j, int jobno, hp::ViewDesc* d);
 hp_status check_seeds(hp_ctx* ctx, const hp_job* j, int jobno);
 size_t seed_area_bytes(const hp_job* j, int W, int H);
 cudaError_t stage_seeds(const hp_job* j, void* area, hp::ViewDesc* d, cudaStream_t st);
+// Geometric-consistency stages of a batch (hp_params.filter_*): for each job
+// the FilterStage it runs after its last half-pass, or none (has[k] = 0);
+// order lists the filtered jobs in job order, the order the stages run in.
+// Source views are the jobs that solved the job's source images (the last
+// such job when several did), of the same size, the job itself excluded.
+void filter_stages(const hp_job* jobs, int n, const hp_params* p, const std::vector<hp::ViewDesc>& descs,
+                   std::vector<hp::FilterStage>* stages, std::vector<char>* has, std::vector<int>* order);
+// One source's FP64-composed transforms (hp::FilterSource) from the two cameras.
+bool filter_source_of(const hp_camera& ref, const hp_camera& src, hp::FilterSource* q);
 void free_image(Image& im);
 // Device bytes an image holds (planes, arrays, quad plane).
 size_t image_bytes(const Image& im);

@@ -17,6 +17,8 @@ constexpr int TILE_W = 64;
 constexpr int TILE_H = 8;
 constexpr int CTA_THREADS = 256;
 
+struct FilterStage;
+
 // Per-view descriptor, resident in device memory for the duration of a solve.
 // Hypotheses are packed (depth, nx, ny, nz) so one 16-byte load fetches a
 // pixel's plane; cost is a separate float plane.
@@ -43,6 +45,9 @@ struct ViewDesc {
     float* out_depth;
     float* out_normal;
     float* out_cost;
+    float* out_conf;  // may be null: confidence 1 - cost / 2 per pixel
+    // Geometric-consistency stage after the last half-pass (null: none).
+    const FilterStage* filter;
     // SfM seeding (null when the job has none): per pixel the index of the
     // seed whose plane replaces the random initial one, -1 for none.
     const int* seed_map;
@@ -98,21 +103,51 @@ struct Schedule {
     unsigned long long wait_limit_ns;
     int stall_view, stall_tile;   // this tile never reports completion (bounded-wait test); -1 = none
     SolveConsts sc;
+    // Filter stages (null when the schedule has none): tickets below
+    // main_total are the solve proper; every one of them must have finished
+    // (main_done counts them) before a filter stage starts.
+    unsigned* main_done;
+    int main_total;
 };
 
-// Geometric-filter launch arguments: FP32 cameras (cast from FP64 like the
-// reference's eigenToGPUCamera) and one depth / AoS-normal pointer per source.
-struct FilterCam {
-    float K[9], R[9], t[3];
+// Geometric-consistency check of one reference view against its solved
+// sources (the rule of geometric_consistency_filter_kernel,
+// src/dense_recon/patchmatch_mvs.cu:668-781).  Each source's transform is
+// composed in FP64 on the host from the two cameras and cast once: a
+// reference pixel (x, y) at depth d lands at source pixel p.xy / p.z with
+// p = d A (x, y, 1) + b (A = K_s R_rel K_ref^-1, b = K_s t_rel: the
+// homography setup's coefficients) at source-camera depth
+// z = d m.(x, y, 1) + cz (m = the third row of R_rel K_ref^-1, cz = t_rel.z),
+// and a camera-frame normal n maps to R_rel n in the source's frame, so the
+// world-frame normal test is (R_rel n_ref) . n_src.
+struct FilterSource {
+    float A[9];
+    float b[3];
+    float m[3];
+    float cz;
+    float Rn[9];
+    int view;  // fused stage: index of the source's ViewDesc in the solve
 };
-struct FilterArgs {
-    float ref_kinv[9], ref_R[9], ref_t[3];
-    FilterCam src[HP_MAX_SOURCES];
+struct FilterStage {
+    FilterSource src[HP_MAX_SOURCES];
+    int n;                // sources checked (views of the same size that were solved too)
+    int min_consistent;   // fewer agreeing sources: depth 0 and cost 2 (confidence 0)
+    float depth_tol;      // relative depth tolerance
+    float normal_cos;     // minimum cosine between the two world-frame normals
+    // Persistent schedule only: the filtered view before this one in the
+    // sequential order (-1 for the first) and a count of this view's tiles
+    // that finished the stage; a view's filter starts after its predecessor's
+    // has finished everywhere, so each view sees the earlier views filtered
+    // and the later ones not, as the reference's view-by-view loop does.
+    int prev;
+    int* tiles_done;
+};
+// External maps (hp_geometric_filter): the same check on caller maps.
+struct FilterMaps {
+    FilterStage f;
     const float* src_depth[HP_MAX_SOURCES];
-    const float* src_normal[HP_MAX_SOURCES];
-    int S, W, H;
-    float depth_tol, normal_tol_cos;
-    int min_consistent;
+    const float* src_normal[HP_MAX_SOURCES];  // AoS, camera frame
+    int W, H;
 };
 
 // Depth-map fusion (hp_fuse_depth_maps): one view's device maps and its
@@ -159,11 +194,16 @@ cudaError_t launch_quads(const __half* src16, int pitch16, int W, int H, uint2* 
 cudaError_t launch_seed_map(const hp_seed* seeds, int num_seeds, int radius, int W, int H, int* map,
                             cudaStream_t st);
 cudaError_t launch_unpack(const ViewDesc* views_host_copy, int view, float* depth, float* normal, float* cost,
-                          cudaStream_t st);
+                          float* conf, cudaStream_t st);
 cudaError_t launch_pack(const ViewDesc* views_host_copy, int view, const float* depth, const float* normal,
                         const float* cost, cudaStream_t st);
-cudaError_t launch_geometric_filter(const FilterArgs& a, float* depth, const float* normal, float* conf,
-                                    cudaStream_t st);
+// The filter stage of view `view` (views: device descriptors; tiles: its tile
+// count), in place on its packed state; with write_out it also writes the
+// view's out_* maps (the final unpack, fused).
+cudaError_t launch_filter_view(const ViewDesc* views, int view, int tiles, bool write_out, cudaStream_t st);
+// The same check on caller maps: depth and confidence updated in place.
+cudaError_t launch_filter_maps(const FilterMaps& a, float* depth, const float* normal, float* conf,
+                               cudaStream_t st);
 cudaError_t launch_to_f32(const void* src, int dtype, int W, int H, float* dst, int dst_pitch, __half* dst16,
                           int dst16_pitch, cudaStream_t st);
 // Fusion: per-CTA counts of emitted points, their exclusive prefix (and the

@@ -25,6 +25,7 @@
 
 #include "hp_internal.h"
 #include "hp_rng.cuh"
+#include "hp_filter.cuh"
 #include "hp_tile.cuh"
 
 #ifndef HP_F16_MIN_BLOCKS
@@ -706,6 +707,8 @@ __global__ void __launch_bounds__(CTA_THREADS, HP_F16_MIN_BLOCKS) persistent16_k
         } else if (stage <= 2 * v->iterations) {
             const int k = stage - 1;
             tile_propagate16<R, ST>(v, tx, ty, s.sc, k >> 1, k & 1, s_ref, s_win, sm);
+        } else if (is_filter_stage(v, stage)) {
+            tile_filter(s.views, v, tx, ty, true);  // geometric check, then the maps
         } else {
             tile_unpack(v, tx, ty);
         }

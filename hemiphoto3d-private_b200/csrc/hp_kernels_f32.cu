@@ -20,6 +20,7 @@
 // intrinsics so the CPU restatement reproduces it bit for bit.
 #include "hp_internal.h"
 #include "hp_rng.cuh"
+#include "hp_filter.cuh"
 #include "hp_tile.cuh"
 
 // Resident CTAs per SM the cost kernels are register-budgeted for.
@@ -447,6 +448,8 @@ __global__ void __launch_bounds__(CTA_THREADS, HP_F32_MIN_BLOCKS) persistent_ker
         } else if (stage <= 2 * v->iterations) {
             const int k = stage - 1;
             tile_propagate<R, ST>(v, tx, ty, s.sc, k >> 1, k & 1, s_ref, sm);
+        } else if (is_filter_stage(v, stage)) {
+            tile_filter(s.views, v, tx, ty, true);  // geometric check, then the maps
         } else {
             tile_unpack(v, tx, ty);
         }

@@ -66,8 +66,14 @@ struct hp_plan {
     int* d_entry_ticket = nullptr;
     int2* d_entry_info = nullptr;
     int n_entries = 0, total = 0;
-    unsigned* d_counter = nullptr;  // [0] counter, then status[2] at +4 bytes
+    unsigned* d_counter = nullptr;  // [0] counter, then status[2] at +4 bytes, main_done at +16
     int* d_status = nullptr;
+    // Geometric-consistency stages: the filtered views in the order they run,
+    // their per-view finished-tile counts, and the tickets of the solve proper.
+    std::vector<int> filter_order;
+    std::vector<char> filtered;
+    int* d_filter_done = nullptr;
+    int main_total = 0;
     int* h_status = nullptr;        // pinned copy of the status words
     std::vector<float*> staging;    // per view: host-output unpacking area, or nullptr
     cudaGraphExec_t exec = nullptr;
@@ -110,6 +116,8 @@ hp::Schedule schedule_of(const hp_plan* p) {
     s.stall_view = p->opt.debug_stall_view;
     s.stall_tile = p->opt.debug_stall_view >= 0 ? p->opt.debug_stall_tile : -1;
     s.sc = consts_of(&p->params);
+    s.main_done = p->filter_order.empty() ? nullptr : p->d_counter + 4;
+    s.main_total = p->filter_order.empty() ? p->total : p->main_total;
     return s;
 }
 
@@ -130,7 +138,10 @@ cudaError_t enqueue(hp_plan* p) {
     cudaError_t e;
     if (effective_schedule(p) == HP_SCHEDULE_PERSISTENT) {
         if ((e = cudaMemsetAsync(p->d_done, 0xff, p->done_bytes, st)) != cudaSuccess) return e;
-        if ((e = cudaMemsetAsync(p->d_counter, 0, 16, st)) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(p->d_counter, 0, 32, st)) != cudaSuccess) return e;
+        if (!p->filter_order.empty() &&
+            (e = cudaMemsetAsync(p->d_filter_done, 0, p->filter_order.size() * sizeof(int), st)) != cudaSuccess)
+            return e;
         const hp::Schedule s = schedule_of(p);
         const int grid = persistent_grid(p);
         e = f16 ? hp::launch_persistent_f16(s, grid, st) : hp::launch_persistent_f32(s, grid, st);
@@ -148,10 +159,16 @@ cudaError_t enqueue(hp_plan* p) {
             if (e != cudaSuccess) return e;
         }
     }
-    for (size_t k = 0; k < p->host.size(); ++k) {
+    // Filtered views: the geometric check, view by view, writes their maps too.
+    for (int k : p->filter_order) {
         const hp::ViewDesc& v = p->host[k];
-        if ((e = hp::launch_unpack(p->host.data(), static_cast<int>(k), v.out_depth, v.out_normal, v.out_cost, st)) !=
-            cudaSuccess)
+        if ((e = hp::launch_filter_view(p->d_views, k, v.tiles_x * v.tiles_y, true, st)) != cudaSuccess) return e;
+    }
+    for (size_t k = 0; k < p->host.size(); ++k) {
+        if (p->filtered[k]) continue;
+        const hp::ViewDesc& v = p->host[k];
+        if ((e = hp::launch_unpack(p->host.data(), static_cast<int>(k), v.out_depth, v.out_normal, v.out_cost,
+                                   v.out_conf, st)) != cudaSuccess)
             return e;
     }
     return cudaSuccess;
@@ -159,7 +176,7 @@ cudaError_t enqueue(hp_plan* p) {
 
 int launches_per_run(const hp_plan* p) {
     if (effective_schedule(p) == HP_SCHEDULE_PERSISTENT) return 1;
-    return 2 + 2 * p->max_iter + static_cast<int>(p->host.size());
+    return 2 + 2 * p->max_iter + static_cast<int>(p->host.size());  // one filter or unpack per view
 }
 
 void count_launches(hp_plan* p) {
@@ -238,6 +255,9 @@ hp_status finish_run(hp_plan* p, float* ms) {
         HP_CUDA(cudaMemcpyAsync(p->out[k].normal, v.out_normal, 3 * px * sizeof(float), cudaMemcpyDeviceToHost,
                                 ctx->stream));
         HP_CUDA(cudaMemcpyAsync(p->out[k].cost, v.out_cost, px * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+        if (p->out[k].confidence)
+            HP_CUDA(cudaMemcpyAsync(p->out[k].confidence, v.out_conf, px * sizeof(float), cudaMemcpyDeviceToHost,
+                                    ctx->stream));
     }
     HP_CUDA(cudaStreamSynchronize(ctx->stream));
     return HP_OK;
@@ -344,15 +364,33 @@ hp_status hp_plan_create(hp_ctx* ctx, const hp_job* jobs, int num_jobs, const hp
         ints.push_back(acc);
         p->list_tiles.push_back(acc);
     }
+    // Geometric-consistency stages (hp_params.filter_*).
+    std::vector<hp::FilterStage> fstages;
+    filter_stages(jobs, num_jobs, params, p->host, &fstages, &p->filtered, &p->filter_order);
     std::vector<int> tiles(num_jobs), kb(num_jobs, 0), ke(num_jobs);
     for (int k = 0; k < num_jobs; ++k) {
         tiles[k] = p->host[k].tiles_x * p->host[k].tiles_y;
-        ke[k] = 2 * jobs[k].iterations + 2;  // init+cost, half-passes, unpack
+        // init+cost, half-passes, then the unpack - or, for a filtered view,
+        // the filter stage (which writes the maps) after every view's solve.
+        ke[k] = 2 * jobs[k].iterations + (p->filtered[k] ? 1 : 2);
     }
     std::vector<int> eticket;
     std::vector<int2> einfo;
     p->total = build_schedule(num_jobs, tiles.data(), kb.data(), ke.data(), &eticket, &einfo);
     if (p->total < 0) return fail(ctx, HP_ERR_UNSUPPORTED, "plan_create: more than 2^31 tile tickets");
+    p->main_total = p->total;
+    if (!p->filter_order.empty()) {  // filter entries last, in view order
+        eticket.pop_back();
+        long long acc = p->total;
+        for (int k : p->filter_order) {
+            eticket.push_back(static_cast<int>(acc));
+            einfo.push_back(make_int2(k, 2 * jobs[k].iterations + 1));
+            acc += tiles[k];
+            if (acc > 0x7fffffffLL) return fail(ctx, HP_ERR_UNSUPPORTED, "plan_create: more than 2^31 tile tickets");
+        }
+        eticket.push_back(static_cast<int>(acc));
+        p->total = static_cast<int>(acc);
+    }
     p->n_entries = static_cast<int>(einfo.size());
     // One device block: per view state, flags and staging; then descriptors, lists, schedule, counters.
     std::vector<size_t> off_state(num_jobs), off_done(num_jobs), off_stage(num_jobs);
@@ -372,8 +410,12 @@ hp_status hp_plan_create(hp_ctx* ctx, const hp_job* jobs, int num_jobs, const hp
     for (int k = 0; k < num_jobs; ++k) {
         off_stage[k] = bytes;
         if (out[k].memory == HP_MEMORY_HOST)
-            bytes = align256(bytes + static_cast<size_t>(p->host[k].W) * p->host[k].H * 5 * sizeof(float));
+            bytes = align256(bytes + static_cast<size_t>(p->host[k].W) * p->host[k].H * 6 * sizeof(float));
     }
+    const size_t off_filters = bytes;
+    bytes = align256(bytes + num_jobs * sizeof(hp::FilterStage));
+    const size_t off_fdone = bytes;
+    bytes = align256(bytes + std::max<size_t>(1, p->filter_order.size()) * sizeof(int));
     std::vector<size_t> off_seed(num_jobs);  // SfM seed lists and index maps, built once here
     for (int k = 0; k < num_jobs; ++k) {
         off_seed[k] = bytes;
@@ -403,14 +445,24 @@ hp_status hp_plan_create(hp_ctx* ctx, const hp_job* jobs, int num_jobs, const hp
             v.out_depth = out[k].depth;
             v.out_normal = out[k].normal;
             v.out_cost = out[k].cost;
+            v.out_conf = out[k].confidence;
         } else {
             float* sd = reinterpret_cast<float*>(base + off_stage[k]);
             p->staging[k] = sd;
             v.out_depth = sd;
             v.out_normal = sd + px;
             v.out_cost = sd + 4 * px;
+            v.out_conf = out[k].confidence ? sd + 5 * px : nullptr;
         }
     }
+    p->d_filter_done = reinterpret_cast<int*>(base + off_fdone);
+    hp::FilterStage* d_filters = reinterpret_cast<hp::FilterStage*>(base + off_filters);
+    for (size_t i = 0; i < p->filter_order.size(); ++i) {
+        const int k = p->filter_order[i];
+        fstages[k].tiles_done = p->d_filter_done + i;
+        p->host[k].filter = d_filters + k;
+    }
+    HP_CUDA(cudaMemcpy(d_filters, fstages.data(), num_jobs * sizeof(hp::FilterStage), cudaMemcpyHostToDevice));
     for (int k = 0; k < num_jobs; ++k)
         HP_CUDA(stage_seeds(&jobs[k], base + off_seed[k], &p->host[k], ctx->stream));
     HP_CUDA(cudaStreamSynchronize(ctx->stream));

@@ -117,7 +117,7 @@ struct SrvReq {
     hp::ViewDesc desc{};
     hp_maps out{};
     void* mem = nullptr;
-    float* staging = nullptr;  // host outputs: depth, normal, cost on the device
+    float* staging = nullptr;  // host outputs: depth, normal, cost, confidence on the device
     std::vector<hp_seed> seeds;  // the job's SfM seeds, copied at submission
     int seed_radius = 0;
     double pix_iter = 0.0;
@@ -198,7 +198,7 @@ uint64_t request_bytes(const hp::ViewDesc& d, bool host_out, size_t seed_bytes) 
     const size_t px = static_cast<size_t>(d.W) * d.H;
     size_t b = align256(px * (sizeof(float4) + sizeof(float)));
     b = align256(b + static_cast<size_t>(d.tiles_x) * d.tiles_y * sizeof(int));
-    if (host_out) b = align256(b + px * 5 * sizeof(float));
+    if (host_out) b = align256(b + px * 6 * sizeof(float));
     return align256(b + seed_bytes);
 }
 
@@ -244,12 +244,14 @@ cudaError_t materialise(hp_server* s, SrvReq* r) {
         v.out_depth = r->out.depth;
         v.out_normal = r->out.normal;
         v.out_cost = r->out.cost;
+        v.out_conf = r->out.confidence;
     } else {
         r->staging = reinterpret_cast<float*>(base + off);
         v.out_depth = r->staging;
         v.out_normal = r->staging + px;
         v.out_cost = r->staging + 4 * px;
-        off = align256(off + px * 5 * sizeof(float));
+        v.out_conf = r->out.confidence ? r->staging + 5 * px : nullptr;
+        off = align256(off + px * 6 * sizeof(float));
     }
     if (!r->seeds.empty()) {  // SfM seed list and index map, read by the initialisation stage
         hp_job sj{};
@@ -418,6 +420,9 @@ bool enqueue_step(hp_server* s) {
             if (ce == cudaSuccess)
                 ce = cudaMemcpyAsync(r->out.cost, r->staging + 4 * px, px * sizeof(float), cudaMemcpyDeviceToHost,
                                      s->stream);
+            if (ce == cudaSuccess && r->out.confidence)
+                ce = cudaMemcpyAsync(r->out.confidence, r->staging + 5 * px, px * sizeof(float),
+                                     cudaMemcpyDeviceToHost, s->stream);
             if (ce != cudaSuccess) {
                 cudaGetLastError();
                 set_err(s, "server: result copy", ce);

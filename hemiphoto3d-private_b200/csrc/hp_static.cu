@@ -198,7 +198,7 @@ extern "C" hp_status hp_solve_static(int device, void* stream, const hp_job* job
     for (int it = 0; it < job->iterations; ++it)
         for (int color = 0; color < 2; ++color)
             if ((e = hp::launch_propagate_f32(bl, sc, it, color, st)) != cudaSuccess) return bail(e);
-    if ((e = hp::launch_unpack(&d, 0, out->depth, out->normal, out->cost, st)) != cudaSuccess) return bail(e);
+    if ((e = hp::launch_unpack(&d, 0, out->depth, out->normal, out->cost, out->confidence, st)) != cudaSuccess) return bail(e);
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return fail(e);
     return HP_OK;
 }

@@ -46,7 +46,8 @@ __device__ __forceinline__ void tile_init(const ViewDesc* v, int tile_x, int til
 }
 
 // Final stage of a view in a persistent launch: its tile's packed state into
-// the output maps (depth, camera-frame AoS normal, cost).
+// the output maps (depth, camera-frame AoS normal, cost, and confidence
+// 1 - cost / 2 when wanted).
 __device__ __forceinline__ void tile_unpack(const ViewDesc* v, int tile_x, int tile_y) {
     const int ly = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int y = tile_y * TILE_H + ly;
@@ -60,7 +61,9 @@ __device__ __forceinline__ void tile_unpack(const ViewDesc* v, int tile_x, int t
         v->out_normal[3 * i] = h.y;
         v->out_normal[3 * i + 1] = h.z;
         v->out_normal[3 * i + 2] = h.w;
-        v->out_cost[i] = __ldcg(v->cost + i);
+        const float c = __ldcg(v->cost + i);
+        v->out_cost[i] = c;
+        if (v->out_conf) v->out_conf[i] = __fsub_rn(1.0f, __fmul_rn(c, 0.5f));
     }
 }
 
@@ -90,7 +93,20 @@ struct SchedTile {
     const ViewDesc* v;
     int view, stage;
     int tile, tx, ty;
+    int ticket;
 };
+
+// Whether stage `stage` of view v is its geometric-consistency stage (which
+// follows its last half-pass when the view has one).
+__device__ __forceinline__ bool is_filter_stage(const ViewDesc* v, int stage) {
+    return v->filter != nullptr && stage == 2 * v->iterations + 1;
+}
+
+__device__ __forceinline__ unsigned ld_acquire_gpu_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
 
 __device__ __forceinline__ SchedTile decode_ticket(const Schedule& s, int t) {
     int lo = 0, hi = s.n_entries - 1;
@@ -106,6 +122,7 @@ __device__ __forceinline__ SchedTile decode_ticket(const Schedule& s, int t) {
     r.tile = t - s.entry_ticket[lo];
     r.tx = r.tile % r.v->tiles_x;
     r.ty = r.tile / r.v->tiles_x;
+    r.ticket = t;
     return r;
 }
 
@@ -115,10 +132,37 @@ __device__ __forceinline__ void sched_abort(const Schedule& s, int code) {
     atomicExch(s.status + 1, 1);
 }
 
+// Bounded poll of thread 0: spins while ready() is false.  Bounded by the
+// schedule's time limit and by a poll count (in case the global timer stands
+// still); false when this or another CTA gave up.
+struct WaitBudget {
+    unsigned long long start = 0;
+    unsigned polls = 0;
+};
+
+template <class Ready>
+__device__ __forceinline__ bool sched_poll(const Schedule& s, WaitBudget& b, Ready ready) {
+    constexpr unsigned kMaxPolls = 1u << 26;
+    while (!ready()) {
+        if (ld_relaxed_gpu(s.status + 1)) return false;
+        if (++b.polls > 16) {
+            const unsigned long long now = global_ns();
+            if (b.start == 0) b.start = now;
+            if (now - b.start > s.wait_limit_ns || b.polls > kMaxPolls) {
+                sched_abort(s, SCHED_TIMEOUT);
+                return false;
+            }
+            __nanosleep(256);
+        }
+    }
+    return true;
+}
+
 // Thread 0 of a CTA: wait until the tile and its 4-neighbour tiles have
-// finished stage - 1.  Bounded by the schedule's time limit and by a poll
-// count (in case the global timer stands still); false when this or another
-// CTA gave up.
+// finished stage - 1.  A filter stage also waits until every ticket of the
+// solve proper has finished and the previous filtered view's stage has
+// finished on all its tiles (both counts only grow, and every ticket they
+// count precedes this one, so each is held by a running CTA).
 __device__ __forceinline__ bool sched_wait(const Schedule& s, const SchedTile& t) {
     if (t.stage == 0) return true;
     const int need = t.stage - 1;
@@ -131,21 +175,20 @@ __device__ __forceinline__ bool sched_wait(const Schedule& s, const SchedTile& t
     if (t.tx + 1 < tx) deps[n++] = t.tile + 1;
     if (t.ty > 0) deps[n++] = t.tile - tx;
     if (t.ty + 1 < t.v->tiles_y) deps[n++] = t.tile + tx;
-    unsigned long long start = 0;
-    unsigned polls = 0;
-    constexpr unsigned kMaxPolls = 1u << 26;
+    WaitBudget b;
     for (int i = 0; i < n; ++i) {
-        while (ld_acquire_gpu(done + deps[i]) < need) {
-            if (ld_relaxed_gpu(s.status + 1)) return false;
-            if (++polls > 16) {
-                const unsigned long long now = global_ns();
-                if (start == 0) start = now;
-                if (now - start > s.wait_limit_ns || polls > kMaxPolls) {
-                    sched_abort(s, SCHED_TIMEOUT);
-                    return false;
-                }
-                __nanosleep(256);
-            }
+        const int* flag = done + deps[i];
+        if (!sched_poll(s, b, [&] { return ld_acquire_gpu(flag) >= need; })) return false;
+    }
+    if (s.main_done && is_filter_stage(t.v, t.stage)) {
+        const unsigned main_total = static_cast<unsigned>(s.main_total);
+        if (!sched_poll(s, b, [&] { return ld_acquire_gpu_u32(s.main_done) >= main_total; })) return false;
+        const int prev = t.v->filter->prev;
+        if (prev >= 0) {
+            const ViewDesc* pv = &s.views[prev];
+            const int* cnt = pv->filter->tiles_done;
+            const int want = pv->tiles_x * pv->tiles_y;
+            if (!sched_poll(s, b, [&] { return ld_acquire_gpu(cnt) >= want; })) return false;
         }
     }
     return true;
@@ -156,6 +199,12 @@ __device__ __forceinline__ void sched_publish(const Schedule& s, const SchedTile
     if (t.view == s.stall_view && t.tile == s.stall_tile) return;
     __threadfence();
     st_release_gpu(t.v->done + t.tile, t.stage);
+    if (s.main_done) {
+        if (t.ticket < s.main_total)
+            atomicAdd(s.main_done, 1u);
+        else if (is_filter_stage(t.v, t.stage))
+            atomicAdd(t.v->filter->tiles_done, 1);
+    }
 }
 
 // Thread 0: claims the CTA's next ticket and decodes it into *out; false when

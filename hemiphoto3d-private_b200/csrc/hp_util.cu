@@ -90,8 +90,11 @@ __global__ void seed_map_kernel(const hp_seed* __restrict__ seeds, int radius, i
 }
 
 
+// Packed state -> caller maps; confidence is 1 - cost / 2, the reference's
+// host-side conversion (patchmatch_mvs.cu:1246-1252), formed on the device.
 __global__ void unpack_kernel(const float4* __restrict__ hyp, const float* __restrict__ cost_in, size_t n,
-                              float* __restrict__ depth, float* __restrict__ normal, float* __restrict__ cost) {
+                              float* __restrict__ depth, float* __restrict__ normal, float* __restrict__ cost,
+                              float* __restrict__ conf) {
     for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
          i += static_cast<size_t>(gridDim.x) * blockDim.x) {
         const float4 h = hyp[i];
@@ -101,7 +104,11 @@ __global__ void unpack_kernel(const float4* __restrict__ hyp, const float* __res
             normal[3 * i + 1] = h.z;
             normal[3 * i + 2] = h.w;
         }
-        if (cost) cost[i] = cost_in[i];
+        if (cost || conf) {
+            const float c = cost_in[i];
+            if (cost) cost[i] = c;
+            if (conf) conf[i] = __fsub_rn(1.0f, __fmul_rn(c, 0.5f));
+        }
     }
 }
 
@@ -137,11 +144,11 @@ cudaError_t launch_seed_map(const hp_seed* seeds, int num_seeds, int radius, int
     return cudaGetLastError();
 }
 
-cudaError_t launch_unpack(const ViewDesc* vh, int view, float* depth, float* normal, float* cost,
+cudaError_t launch_unpack(const ViewDesc* vh, int view, float* depth, float* normal, float* cost, float* conf,
                           cudaStream_t st) {
     const ViewDesc& v = vh[view];
     unpack_kernel<<<stream_grid(), 256, 0, st>>>(v.hyp, v.cost, static_cast<size_t>(v.W) * v.H, depth, normal,
-                                                 cost);
+                                                 cost, conf);
     return cudaGetLastError();
 }
 

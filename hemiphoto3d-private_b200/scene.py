@@ -31,7 +31,9 @@ from typing import List, Optional, Sequence
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-SCENE_LIB_PATH = os.path.join(_HERE, "lib", "libhpscene.so")
+# The renderer library; HP_SCENE_LIB names another build of the same source
+# (the bench's reference arm renders with one outside the engine's lib/).
+SCENE_LIB_PATH = os.environ.get("HP_SCENE_LIB") or os.path.join(_HERE, "lib", "libhpscene.so")
 
 PLANE, SPHERE = 0, 1
 

@@ -97,6 +97,22 @@ typedef struct hp_params {
      * 20 x 1920x1080, r 7, s 2, 6 sources).
      * -1 = engine default (every source), 0 = texture unit only. */
     int soft_sources;
+    /* Geometric-consistency filter as the final stage of hp_solve and of
+     * plans (geometric_consistency_filter_kernel with runPatchMatchMVS's view
+     * loop, patchmatch_mvs.cu:668-781, :1267-1384).  0 = off (the default
+     * here); the reference stage uses 2.  When on and a solve has at least
+     * two jobs, each job with iterations > 0 is checked, in job order and in
+     * place, against the jobs that solved its source images (a job whose
+     * ref_image is one of its src_images, the last such job when several are,
+     * of the same size, itself excluded): a pixel with fewer than
+     * filter_min_consistent agreeing sources gets depth 0 and cost 2
+     * (confidence 0).  A job with fewer such sources than that is left as
+     * solved.  Later jobs see earlier jobs' filtered depths, as in the
+     * reference's loop.  The check uses the jobs' cameras (also when
+     * use_coeffs is set). */
+    int filter_min_consistent;
+    float filter_depth_tol;     /* relative depth tolerance (reference 0.12) */
+    float filter_normal_cos;    /* min cosine of the two world normals (reference cos(180 deg) = -1: off) */
 } hp_params;
 
 /* One SfM seed in a reference view: pixel, depth and camera-frame normal. */
@@ -139,10 +155,13 @@ typedef struct hp_job {
 
 /* Per-view maps, caller-owned. */
 typedef struct hp_maps {
-    int memory;       /* hp_memory of the three pointers */
+    int memory;       /* hp_memory of the pointers */
     float* depth;     /* H*W */
     float* normal;    /* H*W*3, camera frame */
     float* cost;      /* H*W, mean of the top_k lowest 1-NCC, 2 = invalid */
+    float* confidence; /* H*W or NULL: 1 - cost/2, DepthMap.confidence (patchmatch_mvs.cu:1246-1252),
+                        * written on the device by the solve's unpack; hp_solve, plans and the
+                        * server fill it when given */
 } hp_maps;
 
 const char* hp_status_string(hp_status s);
@@ -232,10 +251,19 @@ hp_status hp_propagate_pass(hp_ctx* ctx, const hp_job* job, const hp_params* par
                             hp_maps* maps, int iteration, int color);
 
 /* Replaces geometric_consistency_filter_kernel + its host packing
- * (patchmatch_mvs.cu:668-781, :1267-1384).  depth and confidence are updated
- * in place: a pixel with fewer than min_consistent agreeing sources gets 0 in
- * both.  Reference defaults: depth_tol 0.12, normal_tol_cos cos(180 deg),
- * min_consistent 2.  All map pointers are in `memory`. */
+ * (patchmatch_mvs.cu:668-781, :1267-1384) for maps the caller holds; a solve
+ * runs the same check itself with hp_params.filter_min_consistent.  depth
+ * and confidence are updated in place: a pixel with fewer than
+ * min_consistent agreeing sources gets 0 in both, and a pixel without a
+ * positive depth gets confidence 0.  All maps are width x height (the
+ * reference's rule: sources of another size are not passed).  A source
+ * agrees when the pixel's point lies in front of it, inside it at the
+ * nearest pixel, that pixel's depth is positive and within depth_tol of the
+ * point's depth in the source camera (relative), and the world-frame normals
+ * have a cosine of at least normal_tol_cos.  Reference defaults: depth_tol
+ * 0.12, normal_tol_cos cos(180 deg), min_consistent 2.  The transforms are
+ * composed in FP64 from the cameras; a source map must not be the depth map
+ * being filtered.  All map pointers are in `memory`. */
 hp_status hp_geometric_filter(hp_ctx* ctx, const hp_camera* ref_cam, int width, int height,
                               float* depth, const float* normal, float* confidence,
                               int num_sources, const hp_camera* src_cams,

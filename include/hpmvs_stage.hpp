@@ -10,9 +10,12 @@
 // Behaviour follows runPatchMatchMVS (:1028-1388): sources and depth range from
 // selectSourceViews, radius (mvs_patch_size - 1) / 2 (clamped to the engine's
 // 1..7 instead of the reference's 1..5), per-view seed 42 + 1e6 * ref_id,
-// confidence 1 - cost / 2, then the in-place geometric filter (tolerance 0.12,
-// normal check off, 2 agreeing views) when iterations > 0 and >= 2 maps, PFM
-// depth per view when save_intermediate.  The initial hypotheses are seeded
+// confidence 1 - cost / 2 (formed on the device), then the in-place geometric
+// filter (tolerance 0.12, normal check off, 2 agreeing views) when iterations
+// > 0 and >= 2 maps, as the solve's last stage on the device.  With
+// save_intermediate the PFM depth of each view is written before the filter,
+// as the reference does, so the filter then runs on the host maps through
+// hp_geometric_filter (the same check, the same bits).  The initial hypotheses are seeded
 // from the SfM points each view sees (:1111-1177, radius 50) through
 // hp_project_seeds.  Errors are reported by return value (an empty vector and
 // `*status`), never by exit().
@@ -62,6 +65,12 @@ inline std::vector<DepthMap> runPatchMatchMVS(const std::vector<ImageData>& imag
     hp_params params;
     hp_params_default(&params);
     params.radius = std::min(HP_MAX_RADIUS, std::max(1, (config.mvs_patch_size - 1) / 2));
+    const bool want_pfm = config.save_intermediate && !config.output_path.empty();
+    if (!want_pfm) {  // the geometric filter as the solve's last stage (:1273-1276 constants)
+        params.filter_min_consistent = 2;
+        params.filter_depth_tol = 0.12f;
+        params.filter_normal_cos = -1.0f;  // cos(180 deg): normal check off
+    }
 
     // The sparse points and their tracks, flattened once for hp_project_seeds.
     std::vector<double> pos;
@@ -118,6 +127,7 @@ inline std::vector<DepthMap> runPatchMatchMVS(const std::vector<ImageData>& imag
         solved.push_back(&vp);
     }
     std::vector<hp_maps> out(jobs.size());
+    std::vector<std::vector<float>> costs(jobs.size());
     for (size_t k = 0; st == HP_OK && k < jobs.size(); ++k) {
         const ImageData& img = images[solved[k]->ref_image_id];
         DepthMap dm;
@@ -128,30 +138,34 @@ inline std::vector<DepthMap> runPatchMatchMVS(const std::vector<ImageData>& imag
         dm.normal = cv::Mat(img.height, img.width, CV_32FC3);
         dm.confidence = cv::Mat(img.height, img.width, CV_32F);
         maps.push_back(dm);
+        costs[k].resize(static_cast<size_t>(img.width) * img.height);
         out[k].memory = HP_MEMORY_HOST;
         out[k].depth = reinterpret_cast<float*>(maps.back().depth.data);
         out[k].normal = reinterpret_cast<float*>(maps.back().normal.data);
-        out[k].cost = reinterpret_cast<float*>(maps.back().confidence.data);  // converted below
+        out[k].cost = costs[k].data();
+        out[k].confidence = reinterpret_cast<float*>(maps.back().confidence.data);  // 1 - cost / 2 (:1246-1252)
     }
     if (st == HP_OK && !jobs.empty())
         st = hp_solve(ctx, jobs.data(), static_cast<int>(jobs.size()), &params, out.data());
-    if (st == HP_OK) {
-        for (DepthMap& dm : maps) {  // confidence = 1 - cost / 2 (:1246-1252)
-            float* c = reinterpret_cast<float*>(dm.confidence.data);
-            for (int p = 0; p < dm.width * dm.height; ++p) c[p] = 1.0f - c[p] * 0.5f;
-        }
+    if (st == HP_OK && want_pfm) {
+        const std::string dir = config.output_path.substr(0, config.output_path.find_last_of('/'));
+        for (const DepthMap& dm : maps)
+            hp_pfm_write((dir + "/depth_" + std::to_string(dm.image_id) + ".pfm").c_str(),
+                         reinterpret_cast<const float*>(dm.depth.data), dm.width, dm.height, 1);
         if (config.mvs_iterations > 0 && maps.size() >= 2) {  // :1267-1384, in place, in view order
             for (size_t k = 0; st == HP_OK && k < maps.size(); ++k) {
                 std::vector<hp_camera> cams;
                 std::vector<const float*> sd, sn;
                 for (const SourceViewInfo& sv : solved[k]->source_views) {
+                    int m_last = -1;  // the last map of that image, as the reference's id lookup
                     for (size_t m = 0; m < maps.size(); ++m)
-                        if (maps[m].image_id == sv.image_id && maps[m].width == maps[k].width &&
-                            maps[m].height == maps[k].height && cams.size() < HP_MAX_SOURCES) {
-                            cams.push_back(to_hp_camera(cameras[sv.image_id]));
-                            sd.push_back(reinterpret_cast<const float*>(maps[m].depth.data));
-                            sn.push_back(reinterpret_cast<const float*>(maps[m].normal.data));
-                        }
+                        if (maps[m].image_id == sv.image_id) m_last = static_cast<int>(m);
+                    if (m_last < 0 || m_last == static_cast<int>(k) || maps[m_last].width != maps[k].width ||
+                        maps[m_last].height != maps[k].height || cams.size() >= HP_MAX_SOURCES)
+                        continue;
+                    cams.push_back(to_hp_camera(cameras[sv.image_id]));
+                    sd.push_back(reinterpret_cast<const float*>(maps[m_last].depth.data));
+                    sn.push_back(reinterpret_cast<const float*>(maps[m_last].normal.data));
                 }
                 if (cams.size() < 2) continue;
                 hp_camera ref = to_hp_camera(cameras[maps[k].image_id]);
@@ -162,12 +176,6 @@ inline std::vector<DepthMap> runPatchMatchMVS(const std::vector<ImageData>& imag
                                          static_cast<int>(cams.size()), cams.data(), sd.data(), sn.data(),
                                          HP_MEMORY_HOST, 0.12f, -1.0f /* cos(180 deg): normal check off */, 2);
             }
-        }
-        if (config.save_intermediate && !config.output_path.empty()) {
-            const std::string dir = config.output_path.substr(0, config.output_path.find_last_of('/'));
-            for (const DepthMap& dm : maps)
-                hp_pfm_write((dir + "/depth_" + std::to_string(dm.image_id) + ".pfm").c_str(),
-                             reinterpret_cast<const float*>(dm.depth.data), dm.width, dm.height, 1);
         }
     }
     hp_ctx_destroy(ctx);

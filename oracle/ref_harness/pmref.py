@@ -165,3 +165,41 @@ def run_stage(grays: Sequence[np.ndarray], cams, positions, tracks, patch_size=1
                                _p(ids), _p(depth), _p(normal), _p(n_out))
     assert rc == 0
     return {int(ids[i]): (depth[i], normal[i]) for i in range(int(n_out[0]))}
+
+
+# ------------------------------------------------------------------------------------------------
+# The engine's C++ stage adapter (include/hpmvs_stage.hpp) run inside the reference's translation
+# unit: oracle/_ref/libpmstage.so (stage_harness.cu).
+STAGE_LIB_PATH = os.path.join(HERE, "..", "_ref", "libpmstage.so")
+_stage = None
+
+
+def stage_available() -> bool:
+    return os.path.exists(STAGE_LIB_PATH)
+
+
+def stage_run(grays: Sequence[np.ndarray], cams, positions, tracks, patch_size=11, iterations=3, output_dir=None):
+    """hpmvs_stage::runPatchMatchMVS: (status, {image id: (depth, normal, confidence)})."""
+    global _stage
+    if _stage is None:
+        L = C.CDLL(STAGE_LIB_PATH)
+        L.pmstage_run.restype = C.c_int
+        _stage = L
+    H, W = grays[0].shape
+    g = [np.ascontiguousarray(x, np.float32) for x in grays]
+    ptrs = (C.c_void_p * len(g))(*[x.ctypes.data for x in g])
+    krt, _, pos, toff, timg = _sfm_arrays(cams, [1] * len(cams), positions, tracks)
+    n = len(cams)
+    ids = np.zeros(n, np.int32)
+    depth = np.zeros((n, H, W), np.float32)
+    normal = np.zeros((n, H, W, 3), np.float32)
+    conf = np.zeros((n, H, W), np.float32)
+    n_out = np.zeros(1, np.int32)
+    status = np.zeros(1, np.int32)
+    rc = _stage.pmstage_run(ptrs, C.c_int(W), C.c_int(H), C.c_void_p(_p(krt)), C.c_int(n), C.c_void_p(_p(pos)),
+                            C.c_void_p(_p(toff)), C.c_void_p(_p(timg)), C.c_int(len(tracks)), C.c_int(patch_size),
+                            C.c_int(iterations), output_dir.encode() if output_dir else None, C.c_void_p(_p(ids)),
+                            C.c_void_p(_p(depth)), C.c_void_p(_p(normal)), C.c_void_p(_p(conf)),
+                            C.c_void_p(_p(n_out)), C.c_void_p(_p(status)))
+    assert rc == 0
+    return int(status[0]), {int(ids[i]): (depth[i], normal[i], conf[i]) for i in range(int(n_out[0]))}

@@ -122,22 +122,30 @@ def test_uneven_iterations_in_one_batch(hp, ctx, ids_full, full_scene):
 def test_stage_api_end_to_end(hp, full_scene, tmp_path):
     """run_patchmatch_mvs mirrors runPatchMatchMVS: 5 views, geometric filter, PFM output.
     EndToEndFilterAndAccuracy (tests/test_patchmatch.cpp:446-539) bounds on this scene:
-    mean relative error of retained pixels < 0.15 (here < 0.02), retention >= 0.5."""
+    mean relative error of retained pixels < 0.15 (here < 0.02), retention >= 0.5.  As in the
+    reference, the PFM files hold each view's depth before the filter (:1254-1257); the filtered maps
+    are the same whether the filter ran fused into the solve or after the write."""
     s = full_scene
     cams = [hp.make_camera(*cam_of(s, i)) for i in range(len(s.views))]
     views = [hp.ViewParams(r, s.sources[r], *s.depth_range) for r in s.refs]
+    imgs = [v.image for v in s.views]
     cfg = hp.MVSConfig(mvs_iterations=8, mvs_patch_size=11, window_stride=2, save_intermediate=True,
                        output_dir=str(tmp_path))
-    maps = hp.run_patchmatch_mvs([v.image for v in s.views], cams, views, cfg)
+    maps = hp.run_patchmatch_mvs(imgs, cams, views, cfg)
+    fused = hp.run_patchmatch_mvs(imgs, cams, views, hp.MVSConfig(mvs_iterations=8, mvs_patch_size=11,
+                                                                   window_stride=2))
+    raw = hp.run_patchmatch_mvs(imgs, cams, views, hp.MVSConfig(mvs_iterations=8, mvs_patch_size=11,
+                                                                 window_stride=2, geometric_filter=False))
     assert [m.image_id for m in maps] == s.refs
     kept, err = [], []
-    for m in maps:
+    for m, f, r in zip(maps, fused, raw):
         gt = s.views[m.image_id].depth_gt
         k = m.depth > 0
         kept.append(k.mean())
         err.append((np.abs(m.depth[k] - gt[k]) / gt[k]).mean())
         assert ((m.confidence >= 0) & (m.confidence <= 1)).all()
-        assert np.array_equal(hp.pfm_read(str(tmp_path / f"depth_{m.image_id}.pfm")), m.depth)
+        assert np.array_equal(m.depth, f.depth) and np.array_equal(m.confidence, f.confidence)
+        assert np.array_equal(hp.pfm_read(str(tmp_path / f"depth_{m.image_id}.pfm")), r.depth)
     assert np.mean(kept) >= 0.5 and np.mean(err) < 0.02, (kept, err)
 
 
