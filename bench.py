@@ -30,6 +30,7 @@ from __future__ import annotations
 
 import argparse
 import importlib
+import importlib.util
 import json
 import os
 import subprocess
@@ -151,7 +152,6 @@ def scene_module(standalone: bool = False):
     importing the engine package (the reference arm must not load the engine)."""
     if not standalone:
         return importlib.import_module(PKG + ".scene")
-    import importlib.util
     os.environ["HP_SCENE_LIB"] = os.path.join(ROOT, "oracle", "libpmscene.so")
     spec = importlib.util.spec_from_file_location("hp_scene_standalone", os.path.join(ROOT, PKG, "scene.py"))
     mod = importlib.util.module_from_spec(spec)
@@ -786,9 +786,11 @@ def run_reference(args, rank, world):
         if i >= args.warmup:
             rates.append(rate)
     v = float(np.median(rates))
+    sample_mpix = args.cpu_rows * WORKLOAD["width"] / 1e6
     line = {
         "impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": "Mpix*iter/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(sample_mpix / v * 1e3, 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic: seeded planes+spheres scene, renderer ground truth (no dataset)",
         "config": workload_config(world, WORKLOAD["views"]),
         "cpu_baseline": {"value": round(v, 4), "unit": "Mpix*iter/s", "cores": thr, "kind": "port", "sample": desc},
