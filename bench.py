@@ -66,6 +66,8 @@ def parse():
                     help="headline arithmetic; the other is measured too and reported under 'variants'")
     ap.add_argument("--e2e-steps", type=int, default=None, help="end-to-end steps (default: --steps)")
     ap.add_argument("--cpu-rows", type=int, default=1080, help="rows of the CPU-baseline sample (1080: all of view 0)")
+    ap.add_argument("--lanes", type=int, default=0, choices=[0, 1, 2],
+                    help="FP16-acc lanes per (pixel, candidate) item (0: engine default)")
     ap.add_argument("--no-reference-params", action="store_true",
                     help="skip timing the engine at the reference kernels' parameters")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -302,7 +304,8 @@ def run_engine(args, rank, world, local_rank):
 
     def timed(precision, steps, warmup):
         params = hp.default_params(radius=WORKLOAD["radius"], stride=WORKLOAD["stride"],
-                                   precision=hp.PRECISION_F16ACC if precision == "f16acc" else hp.PRECISION_F32)
+                                   precision=hp.PRECISION_F16ACC if precision == "f16acc" else hp.PRECISION_F32,
+                                   lanes_per_pixel=args.lanes)
         for _ in range(warmup):
             ctx.solve(jobs, params, dev_maps)
         ctx.profile_reset()

@@ -483,7 +483,7 @@ hp_status hp_plan_create(hp_ctx* ctx, const hp_job* jobs, int num_jobs, const hp
     HP_CUDA(cudaEventCreate(&p->ev1));
     HP_CUDA(cudaDeviceGetAttribute(&p->sms, cudaDevAttrMultiProcessorCount, ctx->device));
     HP_CUDA(params->precision == HP_PRECISION_F16ACC
-                ? hp::persistent_occupancy_f16(params->radius, params->stride, &p->occ)
+                ? hp::persistent_occupancy_f16(params->radius, params->stride, consts_of(params).lanes, &p->occ)
                 : hp::persistent_occupancy_f32(params->radius, params->stride, &p->occ));
     if (p->occ < 1) return fail(ctx, HP_ERR_UNSUPPORTED, "plan_create: persistent kernel does not fit on an SM");
     release.p = nullptr;

@@ -113,6 +113,11 @@ typedef struct hp_params {
     int filter_min_consistent;
     float filter_depth_tol;     /* relative depth tolerance (reference 0.12) */
     float filter_normal_cos;    /* min cosine of the two world normals (reference cos(180 deg) = -1: off) */
+    /* FP16-acc path only: lanes that score one (pixel, candidate) item
+     * together.  1: a lane alone; 2: a lane pair, even and odd window taps
+     * apart, so a warp's source reads span half the width (fewer L1 lines per
+     * load).  Both give the same bits; 0 = engine default. */
+    int lanes_per_pixel;
 } hp_params;
 
 /* One SfM seed in a reference view: pixel, depth and camera-frame normal. */
