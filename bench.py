@@ -471,10 +471,9 @@ def run_engine(args, rank, world, local_rank):
                                "kernel": ("propagate16_kernel<7,2>" if name == "f16acc" else "propagate_kernel<7,2>"),
                                "ms_per_launch": round(var["propagate_ms_per_launch"], 4),
                                "executed_taps_per_visit": load_executed_taps(name)}
-    if "f16acc" in variants or head == "f16acc":
-        f16v = value if head == "f16acc" else variants["f16acc"]["value"]
-        f32v = value if head == "f32" else variants["f32"]["value"]
-        line["f16acc_over_f32"] = round(f16v / f32v, 3)
+    rates = {head: value, **{k: v["value"] for k, v in variants.items()}}
+    if "f16acc" in rates and "f32" in rates:
+        line["f16acc_over_f32"] = round(rates["f16acc"] / rates["f32"], 3)
     line["fusion"] = run_fusion(hp, ctx, s, dev_maps, n_views, stream)
     if world == 1 and not args.no_reference_params:
         line["reference_params"] = run_reference_params(hp, ctx, stream)
