@@ -551,7 +551,8 @@ def run_batched(args, hp, ctx):
             res[prec] = {"mpix_iter_per_s": round(info["pixel_iterations"] / 1e6 / (ms / 1e3), 1),
                          "ms_per_run": round(ms, 2), "mpix_iter_per_run": round(info["pixel_iterations"] / 1e6, 1),
                          "schedule": {1: "per_pass", 2: "persistent"}[info["schedule"]],
-                         "ctas_per_sm": info["ctas_per_sm"], "launches_per_run": info["launches_per_run"],
+                         "ctas_per_sm": info["ctas_per_sm"], "lanes_per_item": info["lanes"],
+                         "launches_per_run": info["launches_per_run"],
                          "tuned_ms": round(info["tuned_ms"], 2), "graph": bool(info["use_graph"]),
                          "state_gb": round(info["state_bytes"] / 1e9, 2)}
     res["f16acc_over_f32"] = round(res["f16acc"]["mpix_iter_per_s"] / res["f32"]["mpix_iter_per_s"], 3)
