@@ -66,8 +66,6 @@ def parse():
                     help="headline arithmetic; the other is measured too and reported under 'variants'")
     ap.add_argument("--e2e-steps", type=int, default=None, help="end-to-end steps (default: --steps)")
     ap.add_argument("--cpu-rows", type=int, default=1080, help="rows of the CPU-baseline sample (1080: all of view 0)")
-    ap.add_argument("--lanes", type=int, default=0, choices=[0, 1, 2],
-                    help="FP16-acc lanes per (pixel, candidate) item (0: engine default)")
     ap.add_argument("--no-reference-params", action="store_true",
                     help="skip timing the engine at the reference kernels' parameters")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -304,8 +302,7 @@ def run_engine(args, rank, world, local_rank):
 
     def timed(precision, steps, warmup):
         params = hp.default_params(radius=WORKLOAD["radius"], stride=WORKLOAD["stride"],
-                                   precision=hp.PRECISION_F16ACC if precision == "f16acc" else hp.PRECISION_F32,
-                                   lanes_per_pixel=args.lanes)
+                                   precision=hp.PRECISION_F16ACC if precision == "f16acc" else hp.PRECISION_F32)
         for _ in range(warmup):
             ctx.solve(jobs, params, dev_maps)
         ctx.profile_reset()
@@ -551,8 +548,7 @@ def run_batched(args, hp, ctx):
             res[prec] = {"mpix_iter_per_s": round(info["pixel_iterations"] / 1e6 / (ms / 1e3), 1),
                          "ms_per_run": round(ms, 2), "mpix_iter_per_run": round(info["pixel_iterations"] / 1e6, 1),
                          "schedule": {1: "per_pass", 2: "persistent"}[info["schedule"]],
-                         "ctas_per_sm": info["ctas_per_sm"], "lanes_per_item": info["lanes"],
-                         "launches_per_run": info["launches_per_run"],
+                         "ctas_per_sm": info["ctas_per_sm"], "launches_per_run": info["launches_per_run"],
                          "tuned_ms": round(info["tuned_ms"], 2), "graph": bool(info["use_graph"]),
                          "state_gb": round(info["state_bytes"] / 1e9, 2)}
     res["f16acc_over_f32"] = round(res["f16acc"]["mpix_iter_per_s"] / res["f32"]["mpix_iter_per_s"], 3)

@@ -54,10 +54,6 @@ bool mat3_inv(const double* m, double* inv) {
 
 namespace hpx {
 
-// Lanes per (pixel, candidate) item of the FP16 kernels when the caller leaves
-// it to the engine (hp_params.lanes_per_pixel = 0).
-constexpr int kDefaultLanes = 1;
-
 hp_status check_params(hp_ctx* ctx, const hp_params* p) {
     if (!p) return fail(ctx, HP_ERR_INVALID_ARG, "params is null");
     if (p->radius < 1 || p->radius > HP_MAX_RADIUS)
@@ -71,8 +67,6 @@ hp_status check_params(hp_ctx* ctx, const hp_params* p) {
         return fail(ctx, HP_ERR_INVALID_ARG, "refine_steps %d outside 0..4", p->refine_steps);
     if (!(p->iter_decay > 0.f && p->iter_decay <= 1.f) || !(p->step_decay > 0.f && p->step_decay <= 1.f))
         return fail(ctx, HP_ERR_INVALID_ARG, "decay factors must lie in (0, 1]");
-    if (p->lanes_per_pixel < 0 || p->lanes_per_pixel > 2)
-        return fail(ctx, HP_ERR_INVALID_ARG, "lanes_per_pixel %d not 0, 1 or 2", p->lanes_per_pixel);
     if (p->filter_min_consistent < 0 || p->filter_min_consistent > HP_MAX_SOURCES)
         return fail(ctx, HP_ERR_INVALID_ARG, "filter_min_consistent %d outside 0..%d", p->filter_min_consistent,
                     HP_MAX_SOURCES);
@@ -97,7 +91,6 @@ hp::SolveConsts consts_of(const hp_params* p) {
     sc.soft_mask = p->precision == HP_PRECISION_F16ACC
                        ? (p->soft_sources < 0 ? 0xFFu : static_cast<unsigned>(p->soft_sources) & 0xFFu)
                        : 0u;
-    sc.lanes = p->lanes_per_pixel > 0 ? p->lanes_per_pixel : kDefaultLanes;
     return sc;
 }
 
@@ -497,7 +490,6 @@ void hp_params_default(hp_params* p) {
     p->filter_min_consistent = 0;
     p->filter_depth_tol = 0.12f;
     p->filter_normal_cos = -1.0f;
-    p->lanes_per_pixel = 0;
 }
 
 hp_status hp_ctx_create(int device, hp_ctx** out) {

@@ -59,7 +59,6 @@ struct SolveConsts {
     int radius, stride, top_k, refine_steps;
     float iter_decay, step_decay;
     unsigned soft_mask;  // FP16 path: sources sampled in software (bit per source)
-    int lanes;           // FP16 path: lanes per (pixel, candidate) item, 1 or 2 (same results)
 };
 
 // A batch launch covers the tiles of several views: view k owns flattened
@@ -185,7 +184,7 @@ cudaError_t launch_persistent_f32(const Schedule& s, int grid, cudaStream_t st);
 cudaError_t launch_persistent_f16(const Schedule& s, int grid, cudaStream_t st);
 // Resident CTAs per SM of the persistent kernel for (radius, stride).
 cudaError_t persistent_occupancy_f32(int radius, int stride, int* blocks_per_sm);
-cudaError_t persistent_occupancy_f16(int radius, int stride, int lanes, int* blocks_per_sm);
+cudaError_t persistent_occupancy_f16(int radius, int stride, int* blocks_per_sm);
 cudaError_t launch_propagate_f16(const BatchList& bl, const SolveConsts& sc, int iteration, int color,
                                  cudaStream_t st);
 // FP16 plane -> block-tiled software-sampler quad plane (see hpx::QuadPlane).

@@ -77,12 +77,8 @@ struct hp_plan {
     int* h_status = nullptr;        // pinned copy of the status words
     std::vector<float*> staging;    // per view: host-output unpacking area, or nullptr
     cudaGraphExec_t exec = nullptr;
-    int exec_schedule = -1, exec_cpsm = -1, exec_lanes = -1;
+    int exec_schedule = -1, exec_cpsm = -1;
     int sms = 0, occ = 0;
-    // FP16 path: lanes per (pixel, candidate) item in use (hp_params.lanes_per_pixel,
-    // or the tuner's pick when that is 0), and the persistent kernel's occupancy per layout.
-    int lanes = 1;
-    int occ_by_lanes[3] = {0, 0, 0};
     float tuned_ms = 0.f;
     double pix_iter = 0.0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -120,7 +116,6 @@ hp::Schedule schedule_of(const hp_plan* p) {
     s.stall_view = p->opt.debug_stall_view;
     s.stall_tile = p->opt.debug_stall_view >= 0 ? p->opt.debug_stall_tile : -1;
     s.sc = consts_of(&p->params);
-    s.sc.lanes = p->lanes;
     s.main_done = p->filter_order.empty() ? nullptr : p->d_counter + 4;
     s.main_total = p->filter_order.empty() ? p->total : p->main_total;
     return s;
@@ -153,8 +148,7 @@ cudaError_t enqueue(hp_plan* p) {
         if (e != cudaSuccess) return e;
         return cudaMemcpyAsync(p->h_status, p->d_status, 2 * sizeof(int), cudaMemcpyDeviceToHost, st);
     }
-    hp::SolveConsts sc = consts_of(&p->params);
-    sc.lanes = p->lanes;
+    const hp::SolveConsts sc = consts_of(&p->params);
     const hp::BatchList all = list_of(p, 0);
     if ((e = hp::launch_init(all, st)) != cudaSuccess) return e;
     if ((e = f16 ? hp::launch_cost_f16(all, sc, st) : hp::launch_cost_f32(all, sc, st)) != cudaSuccess) return e;
@@ -200,13 +194,13 @@ void count_launches(hp_plan* p) {
 void drop_graph(hp_plan* p) {
     if (p->exec) cudaGraphExecDestroy(p->exec);
     p->exec = nullptr;
-    p->exec_schedule = p->exec_cpsm = p->exec_lanes = -1;
+    p->exec_schedule = p->exec_cpsm = -1;
 }
 
 hp_status ensure_graph(hp_plan* p) {
     hp_ctx* ctx = p->ctx;
     const int sched = effective_schedule(p), cpsm = effective_cpsm(p);
-    if (p->exec && p->exec_schedule == sched && p->exec_cpsm == cpsm && p->exec_lanes == p->lanes) return HP_OK;
+    if (p->exec && p->exec_schedule == sched && p->exec_cpsm == cpsm) return HP_OK;
     drop_graph(p);
     HP_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
     cudaError_t e = enqueue(p);
@@ -218,7 +212,6 @@ hp_status ensure_graph(hp_plan* p) {
     HP_CUDA(e);
     p->exec_schedule = sched;
     p->exec_cpsm = cpsm;
-    p->exec_lanes = p->lanes;
     return HP_OK;
 }
 
@@ -489,14 +482,9 @@ hp_status hp_plan_create(hp_ctx* ctx, const hp_job* jobs, int num_jobs, const hp
     HP_CUDA(cudaEventCreate(&p->ev0));
     HP_CUDA(cudaEventCreate(&p->ev1));
     HP_CUDA(cudaDeviceGetAttribute(&p->sms, cudaDevAttrMultiProcessorCount, ctx->device));
-    p->lanes = params->precision == HP_PRECISION_F16ACC ? consts_of(params).lanes : 1;
-    if (params->precision == HP_PRECISION_F16ACC) {
-        for (int l = 1; l <= 2; ++l)
-            HP_CUDA(hp::persistent_occupancy_f16(params->radius, params->stride, l, &p->occ_by_lanes[l]));
-    } else {
-        HP_CUDA(hp::persistent_occupancy_f32(params->radius, params->stride, &p->occ_by_lanes[1]));
-    }
-    p->occ = p->occ_by_lanes[p->lanes];
+    HP_CUDA(params->precision == HP_PRECISION_F16ACC
+                ? hp::persistent_occupancy_f16(params->radius, params->stride, &p->occ)
+                : hp::persistent_occupancy_f32(params->radius, params->stride, &p->occ));
     if (p->occ < 1) return fail(ctx, HP_ERR_UNSUPPORTED, "plan_create: persistent kernel does not fit on an SM");
     release.p = nullptr;
     *plan = p.release();
@@ -540,7 +528,6 @@ hp_status hp_plan_get_info(const hp_plan* p, hp_plan_info* info) {
     info->state_bytes = p->block_bytes;
     info->pixel_iterations = p->pix_iter;
     info->tuned_ms = p->tuned_ms;
-    info->lanes = p->lanes;
     return HP_OK;
 }
 
@@ -548,31 +535,14 @@ hp_status hp_plan_tune(hp_plan* p, int repeats, hp_plan_info* best) {
     if (!p) return HP_ERR_INVALID_ARG;
     if (repeats < 1 || repeats > 100) return fail(p->ctx, HP_ERR_INVALID_ARG, "plan_tune: repeats %d", repeats);
     DeviceGuard g(p->ctx->device);
-    // Candidates: (lanes per item, schedule, resident CTAs per SM).  Lane
-    // layouts are tried for the FP16 path when the caller left them to the
-    // engine; every candidate gives the same bits.
-    struct Cand {
-        int lanes, schedule, cpsm;
-    };
-    std::vector<int> lane_opts;
-    if (p->params.precision == HP_PRECISION_F16ACC && p->params.lanes_per_pixel == 0)
-        lane_opts = {1, 2};
-    else
-        lane_opts = {p->lanes};
-    std::vector<Cand> cands;
-    for (int l : lane_opts) {
-        cands.push_back({l, HP_SCHEDULE_PER_PASS, 0});
-        for (int c = 1; c <= p->occ_by_lanes[l]; ++c) cands.push_back({l, HP_SCHEDULE_PERSISTENT, c});
-    }
+    std::vector<std::pair<int, int>> cands = {{HP_SCHEDULE_PER_PASS, 0}};
+    for (int c = 1; c <= p->occ; ++c) cands.emplace_back(HP_SCHEDULE_PERSISTENT, c);
     const hp_plan_options keep = p->opt;
-    const int keep_lanes = p->lanes;
     float best_ms = -1.f;
-    Cand best_c = cands[0];
-    for (const Cand& c : cands) {
-        p->lanes = c.lanes;
-        p->occ = p->occ_by_lanes[c.lanes];
-        p->opt.schedule = c.schedule;
-        p->opt.ctas_per_sm = c.cpsm;
+    std::pair<int, int> best_c = cands[0];
+    for (const auto& c : cands) {
+        p->opt.schedule = c.first;
+        p->opt.ctas_per_sm = c.second;
         std::vector<float> t;
         for (int r = 0; r < repeats; ++r) {
             float ms = 0.f;
@@ -580,8 +550,6 @@ hp_status hp_plan_tune(hp_plan* p, int repeats, hp_plan_info* best) {
             if (st == HP_OK) st = finish_run(p, &ms);
             if (st != HP_OK) {
                 p->opt = keep;
-                p->lanes = keep_lanes;
-                p->occ = p->occ_by_lanes[keep_lanes];
                 return st;
             }
             t.push_back(ms);
@@ -593,10 +561,8 @@ hp_status hp_plan_tune(hp_plan* p, int repeats, hp_plan_info* best) {
             best_c = c;
         }
     }
-    p->lanes = best_c.lanes;
-    p->occ = p->occ_by_lanes[best_c.lanes];
-    p->opt.schedule = best_c.schedule;
-    p->opt.ctas_per_sm = best_c.cpsm;
+    p->opt.schedule = best_c.first;
+    p->opt.ctas_per_sm = best_c.second;
     p->tuned_ms = best_ms;
     // Leave the maps holding a solve of the chosen candidate.
     hp_status st = hp_plan_run(p);

@@ -113,11 +113,6 @@ typedef struct hp_params {
     int filter_min_consistent;
     float filter_depth_tol;     /* relative depth tolerance (reference 0.12) */
     float filter_normal_cos;    /* min cosine of the two world normals (reference cos(180 deg) = -1: off) */
-    /* FP16-acc path only: lanes that score one (pixel, candidate) item
-     * together.  1: a lane alone; 2: a lane pair, even and odd window taps
-     * apart, so a warp's source reads span half the width (fewer L1 lines per
-     * load).  Both give the same bits; 0 = engine default. */
-    int lanes_per_pixel;
 } hp_params;
 
 /* One SfM seed in a reference view: pixel, depth and camera-frame normal. */
@@ -348,7 +343,6 @@ typedef struct hp_plan_info {
     uint64_t state_bytes;    /* device memory the plan holds */
     double pixel_iterations; /* sum over views of W * H * iterations */
     float tuned_ms;          /* hp_plan_tune: the chosen candidate's median solve time (0 before) */
-    int lanes;               /* FP16 path: lanes per (pixel, candidate) item in use (1 for FP32) */
 } hp_plan_info;
 
 typedef struct hp_plan hp_plan;
@@ -366,11 +360,9 @@ hp_status hp_plan_run(hp_plan* plan);
  * only); hp_plan_wait completes it and reports its status. */
 hp_status hp_plan_launch(hp_plan* plan);
 hp_status hp_plan_wait(hp_plan* plan);
-/* Autotuner: times every candidate `repeats` times on the plan's own jobs,
- * keeps the fastest by median, and reports it in `best`.  Candidates: the
- * per-pass graph and the persistent kernel at each resident-CTA count up to
- * its occupancy maximum, for each lane layout of the FP16 path (one or two
- * lanes per item) when params.lanes_per_pixel is 0.  All give the same bits.
+/* Autotuner: times every schedule candidate (per-pass graph; persistent at
+ * each resident-CTA count up to the occupancy maximum) `repeats` times on the
+ * plan's own jobs, keeps the fastest by median, and reports it in `best`.
  * The bound maps hold a valid solve afterwards. */
 hp_status hp_plan_tune(hp_plan* plan, int repeats, hp_plan_info* best);
 hp_status hp_plan_get_info(const hp_plan* plan, hp_plan_info* info);

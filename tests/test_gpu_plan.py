@@ -96,7 +96,6 @@ def test_autotuner_picks_a_candidate_and_keeps_results(hp, batch):
     with hp.Plan(ctx, jobs, params, [o[0] for o in outs]) as plan:
         best = plan.tune(repeats=2)
         assert best["schedule"] in (hp.SCHEDULE_PER_PASS, hp.SCHEDULE_PERSISTENT)
-        assert best["lanes"] in (1, 2)  # both FP16 lane layouts are candidates, with the same bits
         assert best["tuned_ms"] > 0
         if best["schedule"] == hp.SCHEDULE_PERSISTENT:
             assert 1 <= best["ctas_per_sm"] <= best["max_ctas_per_sm"]
