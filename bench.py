@@ -66,6 +66,10 @@ def parse():
                     help="headline arithmetic; the other is measured too and reported under 'variants'")
     ap.add_argument("--e2e-steps", type=int, default=None, help="end-to-end steps (default: --steps)")
     ap.add_argument("--cpu-rows", type=int, default=1080, help="rows of the CPU-baseline sample (1080: all of view 0)")
+    ap.add_argument("--tile-h", type=int, default=0, choices=[0, 4, 8],
+                    help="FP16-acc tile height of the headline solve (0: engine default)")
+    ap.add_argument("--staging", type=int, default=0, choices=[0, 4, 8],
+                    help="FP16-acc quad loads in flight per window row (0: engine default)")
     ap.add_argument("--no-reference-params", action="store_true",
                     help="skip timing the engine at the reference kernels' parameters")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -301,8 +305,10 @@ def run_engine(args, rank, world, local_rank):
             dist.barrier()
 
     def timed(precision, steps, warmup):
+        f16 = precision == "f16acc"
         params = hp.default_params(radius=WORKLOAD["radius"], stride=WORKLOAD["stride"],
-                                   precision=hp.PRECISION_F16ACC if precision == "f16acc" else hp.PRECISION_F32)
+                                   precision=hp.PRECISION_F16ACC if f16 else hp.PRECISION_F32,
+                                   tile_h=args.tile_h if f16 else 0, staging=args.staging if f16 else 0)
         for _ in range(warmup):
             ctx.solve(jobs, params, dev_maps)
         ctx.profile_reset()
@@ -548,7 +554,9 @@ def run_batched(args, hp, ctx):
             res[prec] = {"mpix_iter_per_s": round(info["pixel_iterations"] / 1e6 / (ms / 1e3), 1),
                          "ms_per_run": round(ms, 2), "mpix_iter_per_run": round(info["pixel_iterations"] / 1e6, 1),
                          "schedule": {1: "per_pass", 2: "persistent"}[info["schedule"]],
-                         "ctas_per_sm": info["ctas_per_sm"], "launches_per_run": info["launches_per_run"],
+                         "ctas_per_sm": info["ctas_per_sm"], "tile": f"{64}x{info['tile_h']}",
+                         "staging": info["staging"] if prec == "f16acc" else None,
+                         "launches_per_run": info["launches_per_run"],
                          "tuned_ms": round(info["tuned_ms"], 2), "graph": bool(info["use_graph"]),
                          "state_gb": round(info["state_bytes"] / 1e9, 2)}
     res["f16acc_over_f32"] = round(res["f16acc"]["mpix_iter_per_s"] / res["f32"]["mpix_iter_per_s"], 3)

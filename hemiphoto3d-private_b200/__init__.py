@@ -56,6 +56,7 @@ class Params(C.Structure):
         ("refine_steps", C.c_int), ("iter_decay", C.c_float), ("step_decay", C.c_float),
         ("tile_w", C.c_int), ("tile_h", C.c_int), ("soft_sources", C.c_int),
         ("filter_min_consistent", C.c_int), ("filter_depth_tol", C.c_float), ("filter_normal_cos", C.c_float),
+        ("staging", C.c_int),
     ]
 
 
@@ -97,7 +98,8 @@ class PlanOptions(C.Structure):
 class PlanInfo(C.Structure):
     _fields_ = [("schedule", C.c_int), ("ctas_per_sm", C.c_int), ("grid", C.c_int), ("max_ctas_per_sm", C.c_int),
                 ("tickets", C.c_int), ("launches_per_run", C.c_int), ("views", C.c_int), ("use_graph", C.c_int),
-                ("state_bytes", C.c_uint64), ("pixel_iterations", C.c_double), ("tuned_ms", C.c_float)]
+                ("state_bytes", C.c_uint64), ("pixel_iterations", C.c_double), ("tuned_ms", C.c_float),
+                ("tile_h", C.c_int), ("staging", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

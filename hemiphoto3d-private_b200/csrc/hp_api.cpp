@@ -73,9 +73,12 @@ hp_status check_params(hp_ctx* ctx, const hp_params* p) {
     if (p->filter_min_consistent > 0 &&
         (!(p->filter_depth_tol >= 0.f) || !std::isfinite(p->filter_depth_tol) || std::isnan(p->filter_normal_cos)))
         return fail(ctx, HP_ERR_INVALID_ARG, "filter tolerances invalid");
-    if ((p->tile_w != 0 && p->tile_w != hp::TILE_W) || (p->tile_h != 0 && p->tile_h != hp::TILE_H))
-        return fail(ctx, HP_ERR_UNSUPPORTED, "tile %dx%d: the kernels use %dx%d tiles", p->tile_w, p->tile_h,
-                    hp::TILE_W, hp::TILE_H);
+    if (p->tile_w != 0 && p->tile_w != hp::TILE_W)
+        return fail(ctx, HP_ERR_UNSUPPORTED, "tile width %d: the kernels use %d", p->tile_w, hp::TILE_W);
+    if (p->tile_h != 0 && p->tile_h != 8 && !(p->tile_h == 4 && p->precision == HP_PRECISION_F16ACC))
+        return fail(ctx, HP_ERR_UNSUPPORTED, "tile height %d: 8, or 4 on the FP16-acc path", p->tile_h);
+    if (p->staging != 0 && p->staging != 4 && p->staging != 8)
+        return fail(ctx, HP_ERR_INVALID_ARG, "staging %d not 0, 4 or 8", p->staging);
     return HP_OK;
 }
 
@@ -91,11 +94,13 @@ hp::SolveConsts consts_of(const hp_params* p) {
     sc.soft_mask = p->precision == HP_PRECISION_F16ACC
                        ? (p->soft_sources < 0 ? 0xFFu : static_cast<unsigned>(p->soft_sources) & 0xFFu)
                        : 0u;
+    sc.tile_h = p->tile_h > 0 ? p->tile_h : hp::TILE_H;
+    sc.staging = p->staging > 0 ? p->staging : 4;
     return sc;
 }
 
 // Validate a job and fill the image/camera part of its descriptor.
-hp_status fill_desc(hp_ctx* ctx, const hp_job* j, int jobno, hp::ViewDesc* d) {
+hp_status fill_desc(hp_ctx* ctx, const hp_job* j, int jobno, hp::ViewDesc* d, int tile_h) {
     std::memset(d, 0, sizeof *d);
     auto it = ctx->images.find(j->ref_image);
     if (it == ctx->images.end()) return fail(ctx, HP_ERR_NOT_FOUND, "job %d: unknown ref image %d", jobno, j->ref_image);
@@ -137,8 +142,9 @@ hp_status fill_desc(hp_ctx* ctx, const hp_job* j, int jobno, hp::ViewDesc* d) {
         for (int s = 0; s < j->num_sources; ++s)
             for (int i = 0; i < 12; ++i) d->ab[s][i] = static_cast<float>(ab[12 * s + i]);
     }
+    d->tile_h = tile_h;
     d->tiles_x = (ref.W + hp::TILE_W - 1) / hp::TILE_W;
-    d->tiles_y = (ref.H + hp::TILE_H - 1) / hp::TILE_H;
+    d->tiles_y = (ref.H + tile_h - 1) / tile_h;
     d->dmin = j->depth_min;
     d->dmax = j->depth_max;
     d->seed_lo = static_cast<uint32_t>(j->seed);
@@ -250,15 +256,18 @@ struct Prepared {
     int* lists = nullptr;
     int max_iter = 0;
     std::vector<int> filter_order;    // jobs with a filter stage, in the order they run
+    int tile_h = hp::TILE_H;          // rows per tile of this solve's kernels
 };
 
-hp_status prepare(hp_ctx* ctx, const hp_job* jobs, int n, Prepared* P, bool with_seeds = false,
-                  const hp_params* filter = nullptr) {
+hp_status prepare(hp_ctx* ctx, const hp_job* jobs, int n, const hp_params* params, Prepared* P,
+                  bool with_seeds = false, bool with_filter = false) {
     P->host.resize(n);
+    P->tile_h = consts_of(params).tile_h;
+    const hp_params* filter = with_filter ? params : nullptr;
     size_t state_bytes = 0;
     std::vector<size_t> offs(n);
     for (int k = 0; k < n; ++k) {
-        hp_status st = fill_desc(ctx, &jobs[k], k, &P->host[k]);
+        hp_status st = fill_desc(ctx, &jobs[k], k, &P->host[k], P->tile_h);
         if (st != HP_OK) return st;
         offs[k] = state_bytes;
         size_t px = static_cast<size_t>(P->host[k].W) * P->host[k].H;
@@ -490,6 +499,7 @@ void hp_params_default(hp_params* p) {
     p->filter_min_consistent = 0;
     p->filter_depth_tol = 0.12f;
     p->filter_normal_cos = -1.0f;
+    p->staging = 0;
 }
 
 hp_status hp_ctx_create(int device, hp_ctx** out) {
@@ -738,9 +748,9 @@ hp_status hp_solve(hp_ctx* ctx, const hp_job* jobs, int num_jobs, const hp_param
     }
     DeviceGuard g(ctx->device);
     Prepared P;
-    if ((st = prepare(ctx, jobs, num_jobs, &P, true, params)) != HP_OK) return st;
+    if ((st = prepare(ctx, jobs, num_jobs, params, &P, true, true)) != HP_OK) return st;
     hp::BatchList all = batch_of(P, 0);
-    HP_CUDA(counted(ctx, HP_KERNEL_INIT, [&] { return hp::launch_init(all, ctx->stream); }));
+    HP_CUDA(counted(ctx, HP_KERNEL_INIT, [&] { return hp::launch_init(all, P.tile_h, ctx->stream); }));
     if ((st = launch_cost(ctx, all, params)) != HP_OK) return st;
     for (int it = 0; it < P.max_iter; ++it) {
         hp::BatchList bl = batch_of(P, 1 + it);
@@ -752,7 +762,7 @@ hp_status hp_solve(hp_ctx* ctx, const hp_job* jobs, int num_jobs, const hp_param
     for (int k : P.filter_order) {
         const int tiles = P.host[k].tiles_x * P.host[k].tiles_y;
         HP_CUDA(counted(ctx, HP_KERNEL_OTHER,
-                        [&] { return hp::launch_filter_view(P.dev, k, tiles, false, ctx->stream); }));
+                        [&] { return hp::launch_filter_view(P.dev, k, tiles, P.tile_h, false, ctx->stream); }));
     }
     for (int k = 0; k < num_jobs; ++k)
         if ((st = export_maps(ctx, P, k, &out[k], true, true)) != HP_OK) return st;
@@ -768,8 +778,8 @@ hp_status hp_init_hypotheses(hp_ctx* ctx, const hp_job* job, const hp_params* pa
     if (st != HP_OK) return st;
     DeviceGuard g(ctx->device);
     Prepared P;
-    if ((st = prepare(ctx, job, 1, &P, true)) != HP_OK) return st;
-    HP_CUDA(counted(ctx, HP_KERNEL_INIT, [&] { return hp::launch_init(batch_of(P, 0), ctx->stream); }));
+    if ((st = prepare(ctx, job, 1, params, &P, true)) != HP_OK) return st;
+    HP_CUDA(counted(ctx, HP_KERNEL_INIT, [&] { return hp::launch_init(batch_of(P, 0), P.tile_h, ctx->stream); }));
     if ((st = export_maps(ctx, P, 0, out, true, false)) != HP_OK) return st;
     HP_CUDA(cudaStreamSynchronize(ctx->stream));
     flush_profile(ctx);
@@ -783,7 +793,7 @@ hp_status hp_ncc_cost(hp_ctx* ctx, const hp_job* job, const hp_params* params, h
     if (st != HP_OK) return st;
     DeviceGuard g(ctx->device);
     Prepared P;
-    if ((st = prepare(ctx, job, 1, &P)) != HP_OK) return st;
+    if ((st = prepare(ctx, job, 1, params, &P)) != HP_OK) return st;
     if ((st = import_maps(ctx, P, 0, maps, false)) != HP_OK) return st;
     if ((st = launch_cost(ctx, batch_of(P, 0), params)) != HP_OK) return st;
     if ((st = export_maps(ctx, P, 0, maps, false, true)) != HP_OK) return st;
@@ -802,7 +812,7 @@ hp_status hp_propagate_pass(hp_ctx* ctx, const hp_job* job, const hp_params* par
     if (st != HP_OK) return st;
     DeviceGuard g(ctx->device);
     Prepared P;
-    if ((st = prepare(ctx, job, 1, &P)) != HP_OK) return st;
+    if ((st = prepare(ctx, job, 1, params, &P)) != HP_OK) return st;
     if ((st = import_maps(ctx, P, 0, maps, true)) != HP_OK) return st;
     if ((st = launch_pass(ctx, batch_of(P, 0), params, iteration, color)) != HP_OK) return st;
     if ((st = export_maps(ctx, P, 0, maps, true, true)) != HP_OK) return st;

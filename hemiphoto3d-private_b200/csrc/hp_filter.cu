@@ -13,7 +13,7 @@ namespace hp {
 
 namespace {
 
-__global__ void __launch_bounds__(CTA_THREADS) filter_view_kernel(const ViewDesc* __restrict__ views, int view,
+__global__ void __launch_bounds__(256) filter_view_kernel(const ViewDesc* __restrict__ views, int view,
                                                                   bool write_out) {
     const ViewDesc* v = &views[view];
     const int tx = blockIdx.x % v->tiles_x, ty = blockIdx.x / v->tiles_x;
@@ -49,9 +49,10 @@ __global__ void __launch_bounds__(256) filter_maps_kernel(FilterMaps a, float* _
 
 }  // namespace
 
-cudaError_t launch_filter_view(const ViewDesc* views, int view, int tiles, bool write_out, cudaStream_t st) {
+cudaError_t launch_filter_view(const ViewDesc* views, int view, int tiles, int tile_h, bool write_out,
+                               cudaStream_t st) {
     if (tiles <= 0) return cudaSuccess;
-    filter_view_kernel<<<tiles, CTA_THREADS, 0, st>>>(views, view, write_out);
+    filter_view_kernel<<<tiles, 32 * tile_h, 0, st>>>(views, view, write_out);
     return cudaGetLastError();
 }
 

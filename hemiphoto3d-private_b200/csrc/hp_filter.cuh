@@ -48,14 +48,15 @@ __device__ __forceinline__ int filter_agreeing(const FilterStage* __restrict__ f
     return agree;
 }
 
-// The filter stage of one tile of view v, in place on its packed state.  The
+// The filter stage of one tile of view v (a CTA of v->tile_h warps, one per
+// tile row, two pixels a thread), in place on its packed state.  The
 // sources' state is read through L2 (ld.global.cg): in a persistent launch it
 // may have been written by other CTAs since this SM last cached it.  With
 // write_out the tile's final maps go to v's out_* pointers too (the unpack).
 __device__ __forceinline__ void tile_filter(const ViewDesc* __restrict__ views, const ViewDesc* __restrict__ v,
                                             int tile_x, int tile_y, bool write_out) {
     const int ly = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int y = tile_y * TILE_H + ly;
+    const int y = tile_y * v->tile_h + ly;
     if (y >= v->H) return;
     const FilterStage* f = v->filter;
     const int W = v->W, H = v->H;

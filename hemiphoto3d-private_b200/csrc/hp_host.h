@@ -165,8 +165,9 @@ struct DeviceGuard {
 
 hp_status check_params(hp_ctx* ctx, const hp_params* p);
 hp::SolveConsts consts_of(const hp_params* p);
-// Validate a job and fill the image/camera part of its descriptor.
-hp_status fill_desc(hp_ctx* ctx, const hp_job* j, int jobno, hp::ViewDesc* d);
+// Validate a job and fill the image/camera part of its descriptor (tiles of
+// TILE_W x tile_h pixels).
+hp_status fill_desc(hp_ctx* ctx, const hp_job* j, int jobno, hp::ViewDesc* d, int tile_h);
 // SfM seeds of a job: validation, the device bytes its seed list and W x H
 // index map take, and staging them (upload + map build on `st`) into `area`,
 // which sets d->seeds / d->seed_map (left null for a job without seeds).

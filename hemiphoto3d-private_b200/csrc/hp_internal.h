@@ -9,7 +9,8 @@
 
 namespace hp {
 
-// Pixel tile one CTA covers: TILE_W x TILE_H pixels, 256 threads.  In a
+// Pixel tile one CTA covers: TILE_W x TILE_H pixels, 256 threads (the FP16
+// kernels also run TILE_W x 4 tiles with 128 threads).  In a
 // red-black half-pass each thread owns one pixel of the active color (a warp
 // covers one 64-pixel row segment); the full-map kernels give each thread the
 // two horizontally adjacent pixels of its pair.
@@ -35,6 +36,7 @@ struct ViewDesc {
     int ref_pitch, ref16_pitch;
     int W, H, S;
     int tiles_x, tiles_y;
+    int tile_h;                       // rows of a tile (a CTA has tile_h warps, one per row)
     float dmin, dmax;
     uint32_t seed_lo, seed_hi, view_id;
     int iterations;
@@ -59,6 +61,8 @@ struct SolveConsts {
     int radius, stride, top_k, refine_steps;
     float iter_decay, step_decay;
     unsigned soft_mask;  // FP16 path: sources sampled in software (bit per source)
+    int tile_h;          // rows of a CTA's tile (TILE_W x tile_h pixels, tile_h warps): 8, or 4 (FP16 path)
+    int staging;         // FP16 path: quad loads in flight per window row, 4 or 8
 };
 
 // A batch launch covers the tiles of several views: view k owns flattened
@@ -175,7 +179,8 @@ constexpr int FUSE_THREADS = 256;  // pixels per CTA of the fusion kernels
 
 // Kernel launchers (defined in the .cu files), all on the given stream.
 namespace hp {
-cudaError_t launch_init(const BatchList& bl, cudaStream_t st);
+// Initialisation of a batch whose views have tiles of tile_h rows.
+cudaError_t launch_init(const BatchList& bl, int tile_h, cudaStream_t st);
 cudaError_t launch_cost_f32(const BatchList& bl, const SolveConsts& sc, cudaStream_t st);
 cudaError_t launch_propagate_f32(const BatchList& bl, const SolveConsts& sc, int iteration, int color,
                                  cudaStream_t st);
@@ -184,7 +189,7 @@ cudaError_t launch_persistent_f32(const Schedule& s, int grid, cudaStream_t st);
 cudaError_t launch_persistent_f16(const Schedule& s, int grid, cudaStream_t st);
 // Resident CTAs per SM of the persistent kernel for (radius, stride).
 cudaError_t persistent_occupancy_f32(int radius, int stride, int* blocks_per_sm);
-cudaError_t persistent_occupancy_f16(int radius, int stride, int* blocks_per_sm);
+cudaError_t persistent_occupancy_f16(const SolveConsts& sc, int* blocks_per_sm);
 cudaError_t launch_propagate_f16(const BatchList& bl, const SolveConsts& sc, int iteration, int color,
                                  cudaStream_t st);
 // FP16 plane -> block-tiled software-sampler quad plane (see hpx::QuadPlane).
@@ -200,7 +205,8 @@ cudaError_t launch_pack(const ViewDesc* views_host_copy, int view, const float* 
 // The filter stage of view `view` (views: device descriptors; tiles: its tile
 // count), in place on its packed state; with write_out it also writes the
 // view's out_* maps (the final unpack, fused).
-cudaError_t launch_filter_view(const ViewDesc* views, int view, int tiles, bool write_out, cudaStream_t st);
+cudaError_t launch_filter_view(const ViewDesc* views, int view, int tiles, int tile_h, bool write_out,
+                               cudaStream_t st);
 // The same check on caller maps: depth and confidence updated in place.
 cudaError_t launch_filter_maps(const FilterMaps& a, float* depth, const float* normal, float* conf,
                                cudaStream_t st);

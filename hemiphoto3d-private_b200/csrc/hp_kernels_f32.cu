@@ -227,7 +227,7 @@ __device__ __forceinline__ bool same_plane(float4 a, float4 b) {
            __float_as_uint(a.z) == __float_as_uint(b.z) && __float_as_uint(a.w) == __float_as_uint(b.w);
 }
 
-__global__ void __launch_bounds__(CTA_THREADS) init_kernel(BatchList bl) {
+__global__ void __launch_bounds__(256) init_kernel(BatchList bl) {
     int tile_x, tile_y;
     const ViewDesc* v = locate_tile(bl, blockIdx.x, &tile_x, &tile_y);
     tile_init(v, tile_x, tile_y);
@@ -526,9 +526,9 @@ cudaError_t persistent_occupancy_f32(int radius, int stride, int* blocks_per_sm)
     return persistent_dispatch(radius, stride, &dummy, 0, nullptr, blocks_per_sm);
 }
 
-cudaError_t launch_init(const BatchList& bl, cudaStream_t st) {
+cudaError_t launch_init(const BatchList& bl, int tile_h, cudaStream_t st) {
     if (bl.total_tiles <= 0) return cudaSuccess;
-    init_kernel<<<bl.total_tiles, CTA_THREADS, 0, st>>>(bl);
+    init_kernel<<<bl.total_tiles, 32 * tile_h, 0, st>>>(bl);
     return cudaGetLastError();
 }
 

@@ -74,10 +74,16 @@ struct hp_plan {
     std::vector<char> filtered;
     int* d_filter_done = nullptr;
     int main_total = 0;
+    // The jobs (and their seed lists), kept so the device side can be rebuilt
+    // for another tile height; the tile height and staging depth in use.
+    std::vector<hp_job> jobs;
+    std::vector<std::vector<hp_seed>> seeds;
+    int tile_h = hp::TILE_H;
+    int depth = 4;  // FP16 staging depth
     int* h_status = nullptr;        // pinned copy of the status words
     std::vector<float*> staging;    // per view: host-output unpacking area, or nullptr
     cudaGraphExec_t exec = nullptr;
-    int exec_schedule = -1, exec_cpsm = -1;
+    int exec_schedule = -1, exec_cpsm = -1, exec_tile_h = -1, exec_staging = -1;
     int sms = 0, occ = 0;
     float tuned_ms = 0.f;
     double pix_iter = 0.0;
@@ -102,6 +108,13 @@ int persistent_grid(const hp_plan* p) {
     return std::max(1, std::min(p->total, p->sms * effective_cpsm(p)));
 }
 
+hp::SolveConsts plan_consts(const hp_plan* p) {
+    hp::SolveConsts sc = consts_of(&p->params);
+    sc.tile_h = p->tile_h;
+    sc.staging = p->depth;
+    return sc;
+}
+
 hp::Schedule schedule_of(const hp_plan* p) {
     hp::Schedule s{};
     s.views = p->d_views;
@@ -115,7 +128,7 @@ hp::Schedule schedule_of(const hp_plan* p) {
     s.wait_limit_ns = static_cast<unsigned long long>(ms) * 1000000ull;
     s.stall_view = p->opt.debug_stall_view;
     s.stall_tile = p->opt.debug_stall_view >= 0 ? p->opt.debug_stall_tile : -1;
-    s.sc = consts_of(&p->params);
+    s.sc = plan_consts(p);
     s.main_done = p->filter_order.empty() ? nullptr : p->d_counter + 4;
     s.main_total = p->filter_order.empty() ? p->total : p->main_total;
     return s;
@@ -148,9 +161,9 @@ cudaError_t enqueue(hp_plan* p) {
         if (e != cudaSuccess) return e;
         return cudaMemcpyAsync(p->h_status, p->d_status, 2 * sizeof(int), cudaMemcpyDeviceToHost, st);
     }
-    const hp::SolveConsts sc = consts_of(&p->params);
+    const hp::SolveConsts sc = plan_consts(p);
     const hp::BatchList all = list_of(p, 0);
-    if ((e = hp::launch_init(all, st)) != cudaSuccess) return e;
+    if ((e = hp::launch_init(all, p->tile_h, st)) != cudaSuccess) return e;
     if ((e = f16 ? hp::launch_cost_f16(all, sc, st) : hp::launch_cost_f32(all, sc, st)) != cudaSuccess) return e;
     for (int it = 0; it < p->max_iter; ++it) {
         const hp::BatchList bl = list_of(p, 1 + it);
@@ -162,7 +175,8 @@ cudaError_t enqueue(hp_plan* p) {
     // Filtered views: the geometric check, view by view, writes their maps too.
     for (int k : p->filter_order) {
         const hp::ViewDesc& v = p->host[k];
-        if ((e = hp::launch_filter_view(p->d_views, k, v.tiles_x * v.tiles_y, true, st)) != cudaSuccess) return e;
+        if ((e = hp::launch_filter_view(p->d_views, k, v.tiles_x * v.tiles_y, p->tile_h, true, st)) != cudaSuccess)
+            return e;
     }
     for (size_t k = 0; k < p->host.size(); ++k) {
         if (p->filtered[k]) continue;
@@ -194,13 +208,15 @@ void count_launches(hp_plan* p) {
 void drop_graph(hp_plan* p) {
     if (p->exec) cudaGraphExecDestroy(p->exec);
     p->exec = nullptr;
-    p->exec_schedule = p->exec_cpsm = -1;
+    p->exec_schedule = p->exec_cpsm = p->exec_tile_h = p->exec_staging = -1;
 }
 
 hp_status ensure_graph(hp_plan* p) {
     hp_ctx* ctx = p->ctx;
     const int sched = effective_schedule(p), cpsm = effective_cpsm(p);
-    if (p->exec && p->exec_schedule == sched && p->exec_cpsm == cpsm) return HP_OK;
+    if (p->exec && p->exec_schedule == sched && p->exec_cpsm == cpsm && p->exec_tile_h == p->tile_h &&
+        p->exec_staging == p->depth)
+        return HP_OK;
     drop_graph(p);
     HP_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
     cudaError_t e = enqueue(p);
@@ -212,6 +228,8 @@ hp_status ensure_graph(hp_plan* p) {
     HP_CUDA(e);
     p->exec_schedule = sched;
     p->exec_cpsm = cpsm;
+    p->exec_tile_h = p->tile_h;
+    p->exec_staging = p->depth;
     return HP_OK;
 }
 
@@ -269,80 +287,44 @@ void free_plan(hp_plan* p) {
     if (p->ev1) cudaEventDestroy(p->ev1);
     if (p->h_status) cudaFreeHost(p->h_status);
     if (p->block) cudaFree(p->block);
+    p->ev0 = p->ev1 = nullptr;
+    p->h_status = nullptr;
     p->block = nullptr;
 }
 
-}  // namespace
-
-extern "C" {
-
-void hp_plan_options_default(hp_plan_options* o) {
-    if (!o) return;
-    o->schedule = HP_SCHEDULE_AUTO;
-    o->ctas_per_sm = 0;
-    o->use_graph = 1;
-    o->wait_limit_ms = 2000;
-    o->debug_stall_view = -1;
-    o->debug_stall_tile = -1;
-}
-
-hp_status hp_schedule_build(int num_views, const int* tiles, const int* stage_begin, const int* stage_end,
-                            int capacity, int* entry_ticket, int* entry_view, int* entry_stage, int* num_entries) {
-    if (num_views < 0 || !tiles || !stage_begin || !stage_end || !entry_ticket || !entry_view || !entry_stage ||
-        !num_entries || capacity < 0)
-        return HP_ERR_INVALID_ARG;
-    for (int v = 0; v < num_views; ++v)
-        if (tiles[v] < 0 || stage_begin[v] < 0 || stage_end[v] < stage_begin[v]) return HP_ERR_INVALID_ARG;
-    std::vector<int> t;
-    std::vector<int2> info;
-    if (build_schedule(num_views, tiles, stage_begin, stage_end, &t, &info) < 0) return HP_ERR_UNSUPPORTED;
-    *num_entries = static_cast<int>(info.size());
-    if (static_cast<int>(info.size()) > capacity) return HP_ERR_INVALID_ARG;
-    for (size_t e = 0; e < info.size(); ++e) {
-        entry_ticket[e] = t[e];
-        entry_view[e] = info[e].x;
-        entry_stage[e] = info[e].y;
-    }
-    entry_ticket[info.size()] = t.back();
+// Persistent-kernel occupancy of the plan's current kernel variant.
+hp_status plan_occupancy(hp_plan* p) {
+    hp_ctx* ctx = p->ctx;
+    const hp::SolveConsts sc = plan_consts(p);
+    HP_CUDA(p->params.precision == HP_PRECISION_F16ACC
+                ? hp::persistent_occupancy_f16(sc, &p->occ)
+                : hp::persistent_occupancy_f32(p->params.radius, p->params.stride, &p->occ));
+    if (p->occ < 1) return fail(ctx, HP_ERR_UNSUPPORTED, "plan: persistent kernel does not fit on an SM");
     return HP_OK;
 }
 
-hp_status hp_plan_create(hp_ctx* ctx, const hp_job* jobs, int num_jobs, const hp_params* params,
-                         const hp_plan_options* options, const hp_maps* out, hp_plan** plan) {
-    if (!ctx) return HP_ERR_INVALID_ARG;
-    if (!plan) return fail(ctx, HP_ERR_INVALID_ARG, "plan_create: null plan pointer");
-    *plan = nullptr;
-    if (!jobs || !out || num_jobs < 1) return fail(ctx, HP_ERR_INVALID_ARG, "plan_create: no jobs or outputs");
-    hp_status st = check_params(ctx, params);
-    if (st != HP_OK) return st;
-    std::unique_ptr<hp_plan> p(new hp_plan);
-    struct Release {  // frees the device side of a plan that fails half-built
-        hp_plan* p;
-        ~Release() {
-            if (p) free_plan(p);
-        }
-    } release{p.get()};
-    p->ctx = ctx;
-    p->params = *params;
-    if (options)
-        p->opt = *options;
-    else
-        hp_plan_options_default(&p->opt);
-    if (p->opt.schedule < HP_SCHEDULE_AUTO || p->opt.schedule > HP_SCHEDULE_PERSISTENT)
-        return fail(ctx, HP_ERR_INVALID_ARG, "plan_create: unknown schedule %d", p->opt.schedule);
+hp_status build_device(hp_plan* p, int tile_h);
+
+// (Re)builds the plan's device side - descriptors, launch lists, ticket
+// schedule, filter stages and the one device block - for tiles of tile_h rows.
+hp_status build_device(hp_plan* p, int tile_h) {
+    hp_ctx* ctx = p->ctx;
+    const hp_job* jobs = p->jobs.data();
+    const int num_jobs = static_cast<int>(p->jobs.size());
+    const hp_params* params = &p->params;
+    const hp_maps* out = p->out.data();
+    hp_status st;
+    free_plan(p);
+    p->tile_h = tile_h;
+    p->host.assign(num_jobs, hp::ViewDesc{});
+    p->iters.clear();
+    p->max_iter = 0;
+    p->pix_iter = 0.0;
+    p->list_off.clear();
+    p->list_count.clear();
+    p->list_tiles.clear();
     for (int k = 0; k < num_jobs; ++k) {
-        const hp_maps& m = out[k];
-        if (!m.depth || !m.normal || !m.cost)
-            return fail(ctx, HP_ERR_INVALID_ARG, "plan_create: output maps of job %d incomplete", k);
-        if (m.memory != HP_MEMORY_HOST && m.memory != HP_MEMORY_DEVICE)
-            return fail(ctx, HP_ERR_INVALID_ARG, "plan_create: job %d: unknown memory kind %d", k, m.memory);
-    }
-    DeviceGuard g(ctx->device);
-    p->host.resize(num_jobs);
-    p->out.assign(out, out + num_jobs);
-    for (int k = 0; k < num_jobs; ++k) {
-        if ((st = check_seeds(ctx, &jobs[k], k)) != HP_OK) return st;
-        if ((st = fill_desc(ctx, &jobs[k], k, &p->host[k])) != HP_OK) return st;
+        if ((st = fill_desc(ctx, &jobs[k], k, &p->host[k], tile_h)) != HP_OK) return st;
         p->iters.push_back(jobs[k].iterations);
         p->max_iter = std::max(p->max_iter, jobs[k].iterations);
         p->pix_iter += static_cast<double>(p->host[k].W) * p->host[k].H * jobs[k].iterations;
@@ -481,11 +463,89 @@ hp_status hp_plan_create(hp_ctx* ctx, const hp_job* jobs, int num_jobs, const hp
     p->h_status[0] = p->h_status[1] = 0;
     HP_CUDA(cudaEventCreate(&p->ev0));
     HP_CUDA(cudaEventCreate(&p->ev1));
+    return plan_occupancy(p);
+}
+
+}  // namespace
+
+extern "C" {
+
+void hp_plan_options_default(hp_plan_options* o) {
+    if (!o) return;
+    o->schedule = HP_SCHEDULE_AUTO;
+    o->ctas_per_sm = 0;
+    o->use_graph = 1;
+    o->wait_limit_ms = 2000;
+    o->debug_stall_view = -1;
+    o->debug_stall_tile = -1;
+}
+
+hp_status hp_schedule_build(int num_views, const int* tiles, const int* stage_begin, const int* stage_end,
+                            int capacity, int* entry_ticket, int* entry_view, int* entry_stage, int* num_entries) {
+    if (num_views < 0 || !tiles || !stage_begin || !stage_end || !entry_ticket || !entry_view || !entry_stage ||
+        !num_entries || capacity < 0)
+        return HP_ERR_INVALID_ARG;
+    for (int v = 0; v < num_views; ++v)
+        if (tiles[v] < 0 || stage_begin[v] < 0 || stage_end[v] < stage_begin[v]) return HP_ERR_INVALID_ARG;
+    std::vector<int> t;
+    std::vector<int2> info;
+    if (build_schedule(num_views, tiles, stage_begin, stage_end, &t, &info) < 0) return HP_ERR_UNSUPPORTED;
+    *num_entries = static_cast<int>(info.size());
+    if (static_cast<int>(info.size()) > capacity) return HP_ERR_INVALID_ARG;
+    for (size_t e = 0; e < info.size(); ++e) {
+        entry_ticket[e] = t[e];
+        entry_view[e] = info[e].x;
+        entry_stage[e] = info[e].y;
+    }
+    entry_ticket[info.size()] = t.back();
+    return HP_OK;
+}
+
+hp_status hp_plan_create(hp_ctx* ctx, const hp_job* jobs, int num_jobs, const hp_params* params,
+                         const hp_plan_options* options, const hp_maps* out, hp_plan** plan) {
+    if (!ctx) return HP_ERR_INVALID_ARG;
+    if (!plan) return fail(ctx, HP_ERR_INVALID_ARG, "plan_create: null plan pointer");
+    *plan = nullptr;
+    if (!jobs || !out || num_jobs < 1) return fail(ctx, HP_ERR_INVALID_ARG, "plan_create: no jobs or outputs");
+    hp_status st = check_params(ctx, params);
+    if (st != HP_OK) return st;
+    std::unique_ptr<hp_plan> p(new hp_plan);
+    struct Release {  // frees the device side of a plan that fails half-built
+        hp_plan* p;
+        ~Release() {
+            if (p) free_plan(p);
+        }
+    } release{p.get()};
+    p->ctx = ctx;
+    p->params = *params;
+    if (options)
+        p->opt = *options;
+    else
+        hp_plan_options_default(&p->opt);
+    if (p->opt.schedule < HP_SCHEDULE_AUTO || p->opt.schedule > HP_SCHEDULE_PERSISTENT)
+        return fail(ctx, HP_ERR_INVALID_ARG, "plan_create: unknown schedule %d", p->opt.schedule);
+    for (int k = 0; k < num_jobs; ++k) {
+        const hp_maps& m = out[k];
+        if (!m.depth || !m.normal || !m.cost)
+            return fail(ctx, HP_ERR_INVALID_ARG, "plan_create: output maps of job %d incomplete", k);
+        if (m.memory != HP_MEMORY_HOST && m.memory != HP_MEMORY_DEVICE)
+            return fail(ctx, HP_ERR_INVALID_ARG, "plan_create: job %d: unknown memory kind %d", k, m.memory);
+    }
+    DeviceGuard g(ctx->device);
+    p->out.assign(out, out + num_jobs);
+    p->jobs.assign(jobs, jobs + num_jobs);
+    p->seeds.resize(num_jobs);
+    for (int k = 0; k < num_jobs; ++k) {
+        if ((st = check_seeds(ctx, &jobs[k], k)) != HP_OK) return st;
+        if (jobs[k].num_seeds > 0) {
+            p->seeds[k].assign(jobs[k].seeds, jobs[k].seeds + jobs[k].num_seeds);
+            p->jobs[k].seeds = p->seeds[k].data();
+        }
+    }
+    const hp::SolveConsts sc0 = consts_of(params);
+    p->depth = sc0.staging;
     HP_CUDA(cudaDeviceGetAttribute(&p->sms, cudaDevAttrMultiProcessorCount, ctx->device));
-    HP_CUDA(params->precision == HP_PRECISION_F16ACC
-                ? hp::persistent_occupancy_f16(params->radius, params->stride, &p->occ)
-                : hp::persistent_occupancy_f32(params->radius, params->stride, &p->occ));
-    if (p->occ < 1) return fail(ctx, HP_ERR_UNSUPPORTED, "plan_create: persistent kernel does not fit on an SM");
+    if ((st = build_device(p.get(), sc0.tile_h)) != HP_OK) return st;
     release.p = nullptr;
     *plan = p.release();
     return HP_OK;
@@ -528,6 +588,8 @@ hp_status hp_plan_get_info(const hp_plan* p, hp_plan_info* info) {
     info->state_bytes = p->block_bytes;
     info->pixel_iterations = p->pix_iter;
     info->tuned_ms = p->tuned_ms;
+    info->tile_h = p->tile_h;
+    info->staging = p->depth;
     return HP_OK;
 }
 
@@ -535,29 +597,68 @@ hp_status hp_plan_tune(hp_plan* p, int repeats, hp_plan_info* best) {
     if (!p) return HP_ERR_INVALID_ARG;
     if (repeats < 1 || repeats > 100) return fail(p->ctx, HP_ERR_INVALID_ARG, "plan_tune: repeats %d", repeats);
     DeviceGuard g(p->ctx->device);
-    std::vector<std::pair<int, int>> cands = {{HP_SCHEDULE_PER_PASS, 0}};
-    for (int c = 1; c <= p->occ; ++c) cands.emplace_back(HP_SCHEDULE_PERSISTENT, c);
     const hp_plan_options keep = p->opt;
-    float best_ms = -1.f;
-    std::pair<int, int> best_c = cands[0];
-    for (const auto& c : cands) {
-        p->opt.schedule = c.first;
-        p->opt.ctas_per_sm = c.second;
+    // Median time of `repeats` runs of the current configuration.
+    auto timed = [&](float* med) -> hp_status {
         std::vector<float> t;
         for (int r = 0; r < repeats; ++r) {
             float ms = 0.f;
             hp_status st = launch_run(p);
             if (st == HP_OK) st = finish_run(p, &ms);
-            if (st != HP_OK) {
-                p->opt = keep;
-                return st;
-            }
+            if (st != HP_OK) return st;
             t.push_back(ms);
         }
         std::sort(t.begin(), t.end());
-        const float med = t[t.size() / 2];
-        if (best_ms < 0.f || med < best_ms) {
-            best_ms = med;
+        *med = t[t.size() / 2];
+        return HP_OK;
+    };
+    hp_status st;
+    // Stage 1 (FP16-acc path, where the caller left them to the engine): tile
+    // height x staging depth, each timed with the per-pass graph.
+    const bool f16 = p->params.precision == HP_PRECISION_F16ACC;
+    std::vector<int> th_opts = {p->tile_h}, d_opts = {p->depth};
+    if (f16 && p->params.tile_h == 0) th_opts = {8, 4};
+    if (f16 && p->params.staging == 0) d_opts = {4, 8};
+    if (th_opts.size() * d_opts.size() > 1) {
+        float best_ms = -1.f;
+        int best_th = p->tile_h, best_d = p->depth;
+        for (int th : th_opts) {
+            if (th != p->tile_h && (st = build_device(p, th)) != HP_OK) return st;
+            for (int d : d_opts) {
+                p->depth = d;
+                p->opt.schedule = HP_SCHEDULE_PER_PASS;
+                float ms = 0.f;
+                if ((st = timed(&ms)) != HP_OK) {
+                    p->opt = keep;
+                    return st;
+                }
+                if (best_ms < 0.f || ms < best_ms) {
+                    best_ms = ms;
+                    best_th = th;
+                    best_d = d;
+                }
+            }
+        }
+        if (best_th != p->tile_h && (st = build_device(p, best_th)) != HP_OK) return st;
+        p->depth = best_d;
+        if ((st = plan_occupancy(p)) != HP_OK) return st;
+    }
+    // Stage 2: the schedule - the per-pass graph, or the persistent kernel at
+    // each resident-CTA count up to its occupancy maximum.
+    std::vector<std::pair<int, int>> cands = {{HP_SCHEDULE_PER_PASS, 0}};
+    for (int c = 1; c <= p->occ; ++c) cands.emplace_back(HP_SCHEDULE_PERSISTENT, c);
+    float best_ms = -1.f;
+    std::pair<int, int> best_c = cands[0];
+    for (const auto& c : cands) {
+        p->opt.schedule = c.first;
+        p->opt.ctas_per_sm = c.second;
+        float ms = 0.f;
+        if ((st = timed(&ms)) != HP_OK) {
+            p->opt = keep;
+            return st;
+        }
+        if (best_ms < 0.f || ms < best_ms) {
+            best_ms = ms;
             best_c = c;
         }
     }
@@ -565,7 +666,7 @@ hp_status hp_plan_tune(hp_plan* p, int repeats, hp_plan_info* best) {
     p->opt.ctas_per_sm = best_c.second;
     p->tuned_ms = best_ms;
     // Leave the maps holding a solve of the chosen candidate.
-    hp_status st = hp_plan_run(p);
+    st = hp_plan_run(p);
     if (st != HP_OK) return st;
     if (best) hp_plan_get_info(p, best);
     return HP_OK;

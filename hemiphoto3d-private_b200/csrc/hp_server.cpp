@@ -604,7 +604,7 @@ hp_status hp_server_create(hp_ctx* ctx, const hp_params* params, const hp_server
     uint64_t keep = ~0ull;  // keep freed state cached for the next requests
     HP_CUDA(cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep));
     HP_CUDA(cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, ctx->device));
-    HP_CUDA(params->precision == HP_PRECISION_F16ACC ? hp::persistent_occupancy_f16(params->radius, params->stride, &s->occ)
+    HP_CUDA(params->precision == HP_PRECISION_F16ACC ? hp::persistent_occupancy_f16(s->sc, &s->occ)
                                                      : hp::persistent_occupancy_f32(params->radius, params->stride, &s->occ));
     if (s->occ < 1) return fail(ctx, HP_ERR_UNSUPPORTED, "server_create: persistent kernel does not fit on an SM");
     s->cpsm = (o.ctas_per_sm > 0 && o.ctas_per_sm < s->occ) ? o.ctas_per_sm : s->occ;
@@ -653,7 +653,7 @@ hp_status hp_submit(hp_server* s, const hp_job* job, const hp_maps* out, uint64_
     }
     // The context's images are read under the server lock (fill_desc reports through the context).
     hp_status st = check_seeds(s->ctx, job, 0);
-    if (st == HP_OK) st = fill_desc(s->ctx, job, 0, &r->desc);
+    if (st == HP_OK) st = fill_desc(s->ctx, job, 0, &r->desc, s->sc.tile_h);
     if (st != HP_OK) {
         s->err = std::string("submit: ") + s->ctx->err;
         return st;

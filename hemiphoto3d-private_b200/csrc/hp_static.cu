@@ -153,6 +153,7 @@ extern "C" hp_status hp_solve_static(int device, void* stream, const hp_job* job
         for (int s = 0; s < job->num_sources; ++s)
             for (int i = 0; i < 12; ++i) d.ab[s][i] = static_cast<float>(ab[12 * s + i]);
     }
+    d.tile_h = hp::TILE_H;
     d.tiles_x = (width + hp::TILE_W - 1) / hp::TILE_W;
     d.tiles_y = (height + hp::TILE_H - 1) / hp::TILE_H;
     d.dmin = job->depth_min;
@@ -192,8 +193,11 @@ extern "C" hp_status hp_solve_static(int device, void* stream, const hp_job* job
     sc.refine_steps = params->refine_steps;
     sc.iter_decay = params->iter_decay;
     sc.step_decay = params->step_decay;
+    sc.soft_mask = 0;
+    sc.tile_h = hp::TILE_H;
+    sc.staging = 4;
 
-    if ((e = hp::launch_init(bl, st)) != cudaSuccess) return bail(e);
+    if ((e = hp::launch_init(bl, hp::TILE_H, st)) != cudaSuccess) return bail(e);
     if ((e = hp::launch_cost_f32(bl, sc, st)) != cudaSuccess) return bail(e);
     for (int it = 0; it < job->iterations; ++it)
         for (int color = 0; color < 2; ++color)

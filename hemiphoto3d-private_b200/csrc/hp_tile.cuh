@@ -17,7 +17,7 @@ namespace hp {
 // depths lie in [dmin, dmax] and normal components are at least ~1e-10).
 __device__ __forceinline__ void tile_init(const ViewDesc* v, int tile_x, int tile_y) {
     const int ly = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int y = tile_y * TILE_H + ly;
+    const int y = tile_y * v->tile_h + ly;
     if (y >= v->H) return;
     for (int j = 0; j < 2; ++j) {
         const int x = tile_x * TILE_W + j * 32 + lane;
@@ -50,7 +50,7 @@ __device__ __forceinline__ void tile_init(const ViewDesc* v, int tile_x, int til
 // 1 - cost / 2 when wanted).
 __device__ __forceinline__ void tile_unpack(const ViewDesc* v, int tile_x, int tile_y) {
     const int ly = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int y = tile_y * TILE_H + ly;
+    const int y = tile_y * v->tile_h + ly;
     if (y >= v->H) return;
     for (int j = 0; j < 2; ++j) {
         const int x = tile_x * TILE_W + j * 32 + lane;

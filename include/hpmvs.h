@@ -87,8 +87,10 @@ typedef struct hp_params {
     int refine_steps;    /* random perturbations per pixel visit, 0..4 */
     float iter_decay;    /* perturbation range factor per iteration */
     float step_decay;    /* perturbation range factor per refinement step */
-    int tile_w;          /* pixels per CTA row: 0 or 64 (the kernels' one tile shape: a warp per */
-    int tile_h;          /* row of 32 same-colour pixels, 8 rows); 0 or 8.  Others: HP_ERR_UNSUPPORTED */
+    int tile_w;          /* pixels per CTA row: 0 or 64 (a warp per row of 32 same-colour pixels) */
+    int tile_h;          /* rows per CTA tile: 8, or 4 (FP16-acc path only: 128-thread CTAs); 0 = 8,
+                          * or for plans the autotuner's pick.  Others: HP_ERR_UNSUPPORTED.
+                          * Every tile shape gives the same bits */
     /* FP16-acc path only: bit s set = source s is sampled by the software
      * bilinear sampler (quad-packed FP16 texels, fixed-point weights, FP16
      * interpolation) instead of the texture unit.  The software sampler
@@ -113,6 +115,9 @@ typedef struct hp_params {
     int filter_min_consistent;
     float filter_depth_tol;     /* relative depth tolerance (reference 0.12) */
     float filter_normal_cos;    /* min cosine of the two world normals (reference cos(180 deg) = -1: off) */
+    /* FP16-acc path: quad loads in flight per window row (the staging depth):
+     * 4 or 8; 0 = 4, or for plans the autotuner's pick.  Same bits either way. */
+    int staging;
 } hp_params;
 
 /* One SfM seed in a reference view: pixel, depth and camera-frame normal. */
@@ -343,6 +348,8 @@ typedef struct hp_plan_info {
     uint64_t state_bytes;    /* device memory the plan holds */
     double pixel_iterations; /* sum over views of W * H * iterations */
     float tuned_ms;          /* hp_plan_tune: the chosen candidate's median solve time (0 before) */
+    int tile_h;              /* rows per CTA tile in use (8, or 4 on the FP16-acc path) */
+    int staging;             /* FP16-acc: quad loads in flight per window row in use (4 or 8) */
 } hp_plan_info;
 
 typedef struct hp_plan hp_plan;
@@ -360,10 +367,14 @@ hp_status hp_plan_run(hp_plan* plan);
  * only); hp_plan_wait completes it and reports its status. */
 hp_status hp_plan_launch(hp_plan* plan);
 hp_status hp_plan_wait(hp_plan* plan);
-/* Autotuner: times every schedule candidate (per-pass graph; persistent at
- * each resident-CTA count up to the occupancy maximum) `repeats` times on the
- * plan's own jobs, keeps the fastest by median, and reports it in `best`.
- * The bound maps hold a valid solve afterwards. */
+/* Autotuner: times candidates `repeats` times each on the plan's own jobs and
+ * keeps the fastest by median, reporting it in `best`.  On the FP16-acc path
+ * it first picks the tile height (64x8 or 64x4 pixels per CTA) and the
+ * staging depth (4 or 8 quad loads in flight per window row) with the
+ * per-pass graph, where params left them at 0; then the schedule: the
+ * per-pass graph, or the persistent kernel at each resident-CTA count up to
+ * its occupancy maximum.  Every candidate gives the same bits.  The bound maps
+ * hold a valid solve afterwards. */
 hp_status hp_plan_tune(hp_plan* plan, int repeats, hp_plan_info* best);
 hp_status hp_plan_get_info(const hp_plan* plan, hp_plan_info* info);
 hp_status hp_plan_destroy(hp_plan* plan);

@@ -196,11 +196,16 @@ def test_error_paths(hp, ctx, ids_full, full_scene):
         with pytest.raises(hp.HpError) as e:
             ctx.solve([job], hp.default_params(**bad), [m])
         assert e.value.status == 1
-    for tile in (dict(tile_w=32), dict(tile_h=16)):  # one tile shape exists: 64 x 8
+    # Tile shapes: 64 x 8, and 64 x 4 on the FP16-acc path only.
+    for tile in (dict(tile_w=32), dict(tile_h=16), dict(tile_h=4), dict(tile_h=4, precision=0)):
         with pytest.raises(hp.HpError) as e:
             ctx.solve([job], hp.default_params(**tile), [m])
         assert e.value.status == 6
     ctx.solve([job], hp.default_params(tile_w=64, tile_h=8), [m])
+    ctx.solve([job], hp.default_params(tile_h=4, precision=1), [m])
+    with pytest.raises(hp.HpError) as e:
+        ctx.solve([job], hp.default_params(staging=6, precision=1), [m])
+    assert e.value.status == 1
     bad_job = job_for(hp, s, ids_full, 0)
     bad_job.ref_image = 999999
     with pytest.raises(hp.HpError) as e:
