@@ -53,7 +53,7 @@ BATCHED = dict(name="batched_uneven_64", views=64, sizes=[[640, 480], [1280, 720
                sources=[2, 8], iterations=[6, 12], radius=7, stride=2, views_per_size=9, runs=2, tune_repeats=1)
 SERVING = dict(name="serving_poisson", sizes=[[640, 480], [1920, 1080], [4000, 3000]], sources=[2, 8],
                iterations=[4, 12], radius=7, stride=2, requests=480, rate_per_s=10.0, views_per_size=9,
-               mem_fraction=0.8, passes_per_step=8)
+               mem_fraction=0.8, passes_per_step=8, policy=0, step_budget_mpix=1200.0)
 
 
 def parse():
@@ -82,6 +82,11 @@ def parse():
     ap.add_argument("--serve-passes", type=int, default=SERVING["passes_per_step"], help="server stages per step")
     ap.add_argument("--serve-only", action="store_true", help="run only the serving leg (N = 1)")
     ap.add_argument("--serve-split", type=int, default=0, help="server: one launch per stage offset")
+    ap.add_argument("--serve-policy", type=int, default=SERVING["policy"], choices=[0, 1],
+                    help="server step policy: 0 round robin, 1 oldest first within a work budget")
+    ap.add_argument("--serve-budget", type=float, default=SERVING["step_budget_mpix"],
+                    help="budget policy: work per step, 1e6 pixel x source stage units")
+    ap.add_argument("--serve-seed", type=int, default=2024, help="arrival and request draw seed")
     return ap.parse_args()
 
 
@@ -615,7 +620,7 @@ def run_serving(args, hp, device: int):
     submission to the last completion."""
     import torch
     scene = importlib.import_module(PKG + ".scene")
-    rng = np.random.default_rng(2024)
+    rng = np.random.default_rng(args.serve_seed)
     ctx = hp.Context(device)
     pools = []
     for k, (w, h) in enumerate(SERVING["sizes"]):
@@ -638,7 +643,8 @@ def run_serving(args, hp, device: int):
         reqs.append((t, job, w, h, w * h * it))
     params = hp.default_params(radius=SERVING["radius"], stride=SERVING["stride"], precision=hp.PRECISION_F16ACC)
     srv = hp.Server(ctx, params, mem_fraction=SERVING["mem_fraction"], passes_per_step=args.serve_passes,
-                    split_launches=args.serve_split)
+                    split_launches=args.serve_split, policy=args.serve_policy,
+                    step_budget_mpix=args.serve_budget)
     # Warm-up: one request of each size, not counted.
     for sc, ids, cams, w, h in pools:
         m = hp.maps_of(torch.empty(h, w, device="cuda"), torch.empty(h, w, 3, device="cuda"),
@@ -694,6 +700,9 @@ def run_serving(args, hp, device: int):
         "device_busy_frac": round(st["device_ms"] / 1e3 / wall, 3), "wall_s": round(wall, 1),
         "peak_active": st["peak_active"], "steps": st["steps"], "launches": st["launches"],
         "passes_per_step": args.serve_passes,
+        "policy": {0: "round_robin", 1: "budget"}[args.serve_policy],
+        "step_budget_mpix": args.serve_budget if args.serve_policy == 1 else None,
+        "seed": args.serve_seed,
         "peak_state_gb": round(st["peak_state_bytes"] / 1e9, 2),
         "config": {"sizes": SERVING["sizes"], "sources": SERVING["sources"], "iterations": SERVING["iterations"],
                    "window": "15x15", "stride": SERVING["stride"], "precision": "f16acc",

@@ -123,7 +123,8 @@ class ViewSelection(C.Structure):
 class ServerOptions(C.Structure):
     _fields_ = [("max_active", C.c_int), ("mem_fraction", C.c_float), ("mem_limit", C.c_uint64),
                 ("passes_per_step", C.c_int), ("split_launches", C.c_int), ("ctas_per_sm", C.c_int),
-                ("inflight_steps", C.c_int), ("wait_limit_ms", C.c_int)]
+                ("inflight_steps", C.c_int), ("wait_limit_ms", C.c_int), ("policy", C.c_int),
+                ("step_budget_mpix", C.c_double)]
 
 
 class Completion(C.Structure):
@@ -218,6 +219,9 @@ def _load() -> C.CDLL:
         "hp_server_destroy": (C.c_int, [C.c_void_p]),
         "hp_server_simulate": (C.c_int, [C.c_int, P(C.c_int), P(C.c_uint64), P(C.c_int), C.c_int, C.c_uint64,
                                          C.c_int, P(C.c_int), P(C.c_int), P(C.c_int)]),
+        "hp_server_simulate_policy": (C.c_int, [C.c_int, P(C.c_int), P(C.c_uint64), P(C.c_int), P(C.c_double),
+                                                C.c_int, C.c_uint64, C.c_int, C.c_int, C.c_double, P(C.c_int),
+                                                P(C.c_int), P(C.c_int)]),
         "hp_fuse_params_default": (None, [P(FuseParams)]),
         "hp_fuse_depth_maps": (C.c_int, [C.c_void_p, P(FuseView), C.c_int, P(FuseParams), P(PointCloudC)]),
         "hp_pfm_write": (C.c_int, [C.c_char_p, C.c_void_p, C.c_int, C.c_int, C.c_int]),
@@ -242,7 +246,8 @@ EXPORTS = (
     "hp_plan_options_default", "hp_plan_create", "hp_plan_run", "hp_plan_launch", "hp_plan_wait", "hp_plan_tune",
     "hp_plan_get_info", "hp_plan_destroy", "hp_schedule_build", "hp_server_options_default", "hp_server_create",
     "hp_submit", "hp_poll", "hp_server_drain", "hp_server_stats_get", "hp_server_stats_reset",
-    "hp_server_last_error", "hp_server_destroy", "hp_server_simulate", "hp_select_sources", "hp_project_seeds",
+    "hp_server_last_error", "hp_server_destroy", "hp_server_simulate", "hp_server_simulate_policy",
+    "hp_select_sources", "hp_project_seeds",
     "hp_ctx_set_image_cache", "hp_fuse_params_default", "hp_fuse_depth_maps",
 )
 STATIC_MAX_PIXELS = 1280 * 1024  # HP_STATIC_MAX_PIXELS
@@ -654,19 +659,26 @@ class Server:
             pass
 
 
+SERVER_POLICY_ROUND_ROBIN, SERVER_POLICY_BUDGET = 0, 1
+
+
 def server_simulate(arrive_step: Sequence[int], state_bytes: Sequence[int], stages: Sequence[int], max_active: int,
-                    budget: int, passes_per_step: int):
-    """The server's admission and step policy without a device (hp_server_simulate):
-    (admit_step[n], finish_step[n], steps)."""
+                    budget: int, passes_per_step: int, policy: int = 0, work: Optional[Sequence[float]] = None,
+                    step_work: float = 0.0):
+    """The server's admission and step policy without a device (hp_server_simulate_policy):
+    (admit_step[n], finish_step[n], steps).  ``work`` is each request's work per stage (W * H * sources),
+    ``step_work`` the budget policy's work per step in the same units."""
     n = len(arrive_step)
     m = max(1, n)
     a = (C.c_int * m)(*arrive_step)
     b = (C.c_uint64 * m)(*state_bytes)
     k = (C.c_int * m)(*stages)
+    w = (C.c_double * m)(*(work if work is not None else [0.0] * n))
     adm, fin, steps = (C.c_int * m)(), (C.c_int * m)(), C.c_int()
-    st = lib.hp_server_simulate(n, a, b, k, max_active, budget, passes_per_step, adm, fin, C.byref(steps))
+    st = lib.hp_server_simulate_policy(n, a, b, k, w, max_active, budget, passes_per_step, policy, float(step_work),
+                                       adm, fin, C.byref(steps))
     if st != OK:
-        raise HpError(st, "hp_server_simulate")
+        raise HpError(st, "hp_server_simulate_policy")
     return np.array(adm[:n]), np.array(fin[:n]), steps.value
 
 

@@ -5,7 +5,9 @@
 // while a request slot is free and its state fits the byte budget.  The
 // queue is strict FIFO - a request that does not fit holds back those behind
 // it - so large requests are never starved by a stream of small ones.  A step
-// runs, for each admitted request, its next passes_per_step stages; a request
+// runs, for each admitted request, its next passes_per_step stages (round
+// robin), or, with the budget policy, as many as a per-step work budget
+// covers for the oldest requests first (at least one each); a request
 // whose last stage (the unpack into its maps) is in the step leaves the
 // active set as the step is composed, so its slot and bytes serve the next
 // step's admissions.  That reuse is safe before the step has executed: every
@@ -43,6 +45,7 @@ struct CoreReq {
     int tiles = 0;
     int stages = 0;      // 2 * iterations + 2: init + cost, half-passes, unpack
     uint64_t bytes = 0;  // device state the request holds while admitted
+    double work = 0.0;   // work of one stage, in pixel x source units (W * H * S)
     int stage = 0;       // next stage to run
     void* user = nullptr;
 };
@@ -59,7 +62,9 @@ struct ServerCore {
     std::vector<CoreReq*> active;
     uint64_t held = 0;
     int max_active = 64;
-    int passes = 4;
+    int passes = 4;            // stages per request per step (HP_SERVER_POLICY_BUDGET: at most)
+    int policy = HP_SERVER_POLICY_ROUND_ROBIN;
+    double step_work = 0.0;    // HP_SERVER_POLICY_BUDGET: work of a step, pixel x source x stage units
 
     // Head-of-queue admissions that fit `budget` bytes of request state.
     void admit(uint64_t budget, std::vector<CoreReq*>* admitted) {
@@ -79,13 +84,25 @@ struct ServerCore {
         held -= r->bytes;
     }
 
+    // Stage ranges of a step.  Round robin: every admitted request advances
+    // `passes` stages.  Budget: requests in admission order (oldest first)
+    // take as many of their next stages (up to `passes`) as the step's work
+    // budget still covers, and every request at least one, so the oldest
+    // finish first while none stalls.
     void compose(StepPlan* sp) {
         sp->reqs.clear();
         sp->kb.clear();
         sp->ke.clear();
         sp->finishing.clear();
+        double left = step_work;
         for (CoreReq* r : active) {
-            const int kb = r->stage, ke = std::min(r->stage + passes, r->stages);
+            int n = passes;
+            if (policy == HP_SERVER_POLICY_BUDGET) {
+                const double c = std::max(r->work, 1.0);
+                n = std::max(1, std::min(passes, static_cast<int>(std::min(left / c, 1e9))));
+                left = std::max(0.0, left - n * c);
+            }
+            const int kb = r->stage, ke = std::min(r->stage + n, r->stages);
             sp->reqs.push_back(r);
             sp->kb.push_back(kb);
             sp->ke.push_back(ke);
@@ -547,6 +564,8 @@ void hp_server_options_default(hp_server_options* o) {
     o->mem_fraction = 0.8f;
     o->mem_limit = 0;
     o->passes_per_step = 8;
+    o->policy = HP_SERVER_POLICY_ROUND_ROBIN;
+    o->step_budget_mpix = 0.0;
     o->split_launches = 0;
     o->ctas_per_sm = 0;
     o->inflight_steps = 2;
@@ -576,6 +595,11 @@ hp_status hp_server_create(hp_ctx* ctx, const hp_params* params, const hp_server
         return fail(ctx, HP_ERR_INVALID_ARG, "server_create: mem_fraction must lie in (0, 1]");
     if (o.passes_per_step < 1 || o.passes_per_step > 64)
         return fail(ctx, HP_ERR_INVALID_ARG, "server_create: passes_per_step %d outside 1..64", o.passes_per_step);
+    if (o.policy != HP_SERVER_POLICY_ROUND_ROBIN && o.policy != HP_SERVER_POLICY_BUDGET)
+        return fail(ctx, HP_ERR_INVALID_ARG, "server_create: unknown policy %d", o.policy);
+    if (o.step_budget_mpix == 0.0) o.step_budget_mpix = 1200.0;
+    if (!(o.step_budget_mpix > 0.0) || !std::isfinite(o.step_budget_mpix))
+        return fail(ctx, HP_ERR_INVALID_ARG, "server_create: step_budget_mpix invalid");
     if (o.inflight_steps < 1 || o.inflight_steps > kRing)
         return fail(ctx, HP_ERR_INVALID_ARG, "server_create: inflight_steps %d outside 1..%d", o.inflight_steps,
                     kRing);
@@ -588,6 +612,8 @@ hp_status hp_server_create(hp_ctx* ctx, const hp_params* params, const hp_server
     s->sc = consts_of(params);
     s->core.max_active = o.max_active;
     s->core.passes = o.passes_per_step;
+    s->core.policy = o.policy;
+    s->core.step_work = o.step_budget_mpix * 1e6;
     DeviceGuard g(ctx->device);
     struct Release {
         hp_server* p;
@@ -664,6 +690,7 @@ hp_status hp_submit(hp_server* s, const hp_job* job, const hp_maps* out, uint64_
     }
     r->out = *out;
     r->core.tiles = r->desc.tiles_x * r->desc.tiles_y;
+    r->core.work = static_cast<double>(r->desc.W) * r->desc.H * r->desc.S;
     r->core.stages = 2 * job->iterations + 2;
     r->core.bytes = request_bytes(r->desc, out->memory == HP_MEMORY_HOST,
                                   seed_area_bytes(job, r->desc.W, r->desc.H));
@@ -774,11 +801,13 @@ hp_status hp_server_destroy(hp_server* s) {
     return HP_OK;
 }
 
-hp_status hp_server_simulate(int n, const int* arrive_step, const uint64_t* state_bytes, const int* stages,
-                             int max_active, uint64_t budget, int passes_per_step, int* admit_step,
-                             int* finish_step, int* steps) {
+hp_status hp_server_simulate_policy(int n, const int* arrive_step, const uint64_t* state_bytes, const int* stages,
+                                    const double* work, int max_active, uint64_t budget, int passes_per_step,
+                                    int policy, double step_work, int* admit_step, int* finish_step, int* steps) {
     if (n < 0 || (n > 0 && (!arrive_step || !state_bytes || !stages || !admit_step || !finish_step)) || !steps ||
-        max_active < 1 || passes_per_step < 1)
+        max_active < 1 || passes_per_step < 1 ||
+        (policy != HP_SERVER_POLICY_ROUND_ROBIN && policy != HP_SERVER_POLICY_BUDGET) ||
+        (policy == HP_SERVER_POLICY_BUDGET && (n > 0 && !work)) || !(step_work >= 0.0))
         return HP_ERR_INVALID_ARG;
     std::vector<CoreReq> reqs(n);
     std::vector<int> order(n);
@@ -787,6 +816,7 @@ hp_status hp_server_simulate(int n, const int* arrive_step, const uint64_t* stat
         if (state_bytes[k] > budget) return HP_ERR_OUT_OF_MEMORY;
         reqs[k].stages = stages[k];
         reqs[k].bytes = state_bytes[k];
+        reqs[k].work = work ? work[k] : 0.0;
         reqs[k].tiles = 1;
         reqs[k].user = reinterpret_cast<void*>(static_cast<intptr_t>(k));
         order[k] = k;
@@ -796,6 +826,8 @@ hp_status hp_server_simulate(int n, const int* arrive_step, const uint64_t* stat
     ServerCore core;
     core.max_active = max_active;
     core.passes = passes_per_step;
+    core.policy = policy;
+    core.step_work = step_work;
     int next = 0, finished = 0, ran = 0;
     for (int tick = 0; finished < n; ++tick) {
         while (next < n && arrive_step[order[next]] <= tick) core.queue.push_back(&reqs[order[next++]]);
@@ -813,6 +845,14 @@ hp_status hp_server_simulate(int n, const int* arrive_step, const uint64_t* stat
     }
     *steps = ran;
     return HP_OK;
+}
+
+hp_status hp_server_simulate(int n, const int* arrive_step, const uint64_t* state_bytes, const int* stages,
+                             int max_active, uint64_t budget, int passes_per_step, int* admit_step,
+                             int* finish_step, int* steps) {
+    return hp_server_simulate_policy(n, arrive_step, state_bytes, stages, nullptr, max_active, budget,
+                                     passes_per_step, HP_SERVER_POLICY_ROUND_ROBIN, 0.0, admit_step, finish_step,
+                                     steps);
 }
 
 }  // extern "C"

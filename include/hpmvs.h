@@ -408,6 +408,18 @@ hp_status hp_schedule_build(int num_views, const int* tiles, const int* stage_be
  * ------------------------------------------------------------------------- */
 typedef struct hp_server hp_server;
 
+/* How a step divides its stages among the admitted requests. */
+typedef enum hp_server_policy {
+    /* Every admitted request advances passes_per_step stages per step. */
+    HP_SERVER_POLICY_ROUND_ROBIN = 0,
+    /* Oldest first within a work budget: in admission order, each request
+     * takes as many of its next stages (up to passes_per_step) as the step's
+     * budget of step_budget_mpix million pixel x source stage units still
+     * covers, and at least one, so the oldest requests finish first and none
+     * stalls. */
+    HP_SERVER_POLICY_BUDGET = 1
+} hp_server_policy;
+
 typedef struct hp_server_options {
     int max_active;         /* request slots (admitted, not yet completed); 0 = 64 */
     float mem_fraction;     /* admit while device memory in use stays <= this fraction
@@ -420,6 +432,9 @@ typedef struct hp_server_options {
     int ctas_per_sm;        /* resident CTAs per SM (0 = the occupancy maximum) */
     int inflight_steps;     /* steps enqueued ahead of the oldest unfinished one, 1..4 (0 = 2) */
     int wait_limit_ms;      /* bound on one inter-tile dependency wait (0 = 2000) */
+    int policy;             /* hp_server_policy (0 = round robin) */
+    double step_budget_mpix; /* HP_SERVER_POLICY_BUDGET: work per step, in 1e6 pixel x source stage
+                              * units (0 = 1200, ~0.2 s of FP16-acc r 7 s 2 work on a B200) */
 } hp_server_options;
 
 /* One finished request. */
@@ -470,6 +485,12 @@ hp_status hp_server_destroy(hp_server* s);
 hp_status hp_server_simulate(int n, const int* arrive_step, const uint64_t* state_bytes, const int* stages,
                              int max_active, uint64_t budget, int passes_per_step, int* admit_step,
                              int* finish_step, int* steps);
+/* The same with a step policy: work[k] is request k's work per stage (pixel x
+ * source units, W * H * num_sources), step_work the budget policy's work per
+ * step in the same units. */
+hp_status hp_server_simulate_policy(int n, const int* arrive_step, const uint64_t* state_bytes, const int* stages,
+                                    const double* work, int max_active, uint64_t budget, int passes_per_step,
+                                    int policy, double step_work, int* admit_step, int* finish_step, int* steps);
 
 /* ---------------------------------------------------------------------------
  * SfM front of the stage: what runPatchMatchMVS derives from the sparse

@@ -56,6 +56,39 @@ def test_late_arrival_joins_running_work(hp):
     assert adm[1] == fin[0] + 1
 
 
+def test_budget_policy_serves_the_oldest_first_and_stalls_none(hp):
+    """HP_SERVER_POLICY_BUDGET: in admission order each request takes as many stages (up to
+    passes_per_step) as the step's work budget still covers, and at least one - so the oldest request
+    finishes first when the budget covers it, and every admitted request still advances every step."""
+    # Two requests of 26 stages, work 10 a stage, budget 100 a step, cap 16: the first takes 10 stages
+    # a step (finishing in 3 steps), the second 1 a step until the first is done.
+    adm, fin, steps = hp.server_simulate([0, 0], [1, 1], [26, 26], 4, 100, 16, policy=hp.SERVER_POLICY_BUDGET,
+                                         work=[10.0, 10.0], step_work=100.0)
+    assert adm.tolist() == [0, 0]
+    assert fin[0] == 2  # stages 10 + 10 + 6
+    assert fin[1] > fin[0]
+    rng = np.random.default_rng(5)
+    for trial in range(30):
+        n = int(rng.integers(1, 40))
+        arrive = np.sort(rng.integers(0, 30, n))
+        bytes_ = rng.integers(1, 100, n)
+        stages = 2 * rng.integers(0, 13, n) + 2
+        work = rng.uniform(1, 50, n)
+        slots = int(rng.integers(1, 9))
+        budget = int(rng.integers(int(bytes_.max()), 400))
+        passes = int(rng.integers(1, 20))
+        adm, fin, steps = hp.server_simulate(arrive.tolist(), bytes_.tolist(), stages.tolist(), slots, budget, passes,
+                                             policy=hp.SERVER_POLICY_BUDGET, work=work.tolist(),
+                                             step_work=float(rng.uniform(0, 200)))
+        assert (adm >= arrive).all() and (np.diff(adm) >= 0).all()
+        # At least one stage and at most `passes` a step: ceil(stages / passes) - 1 <= fin - adm <= stages - 1.
+        assert (fin - adm >= np.ceil(stages / passes).astype(int) - 1).all() and (fin - adm <= stages - 1).all()
+        active, held = _occupancy(adm, fin, bytes_, int(fin.max()) + 1)
+        assert active.max() <= slots and held.max() <= budget
+    with pytest.raises(hp.HpError):
+        hp.server_simulate([0], [1], [4], 1, 10, 2, policy=7)
+
+
 def test_budget_serialises_and_oversize_is_refused(hp):
     adm, fin, steps = hp.server_simulate([0, 0, 0], [60, 60, 60], [6, 6, 6], 8, 100, 3)
     assert adm.tolist() == [0, 2, 4] and fin.tolist() == [1, 3, 5] and steps == 6
