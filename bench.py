@@ -70,6 +70,9 @@ def parse():
                     help="FP16-acc tile height of the headline solve (0: engine default)")
     ap.add_argument("--staging", type=int, default=0, choices=[0, 4, 8],
                     help="FP16-acc quad loads in flight per window row (0: engine default)")
+    ap.add_argument("--count-taps", action="store_true",
+                    help="with HP_ENGINE_LIB set to the instrumented engine (make -C <pkg> count): taps sampled per "
+                         "pixel visit of the propagate half-passes, views 0 and 10, 12 iterations, both precisions")
     ap.add_argument("--no-reference-params", action="store_true",
                     help="skip timing the engine at the reference kernels' parameters")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -245,8 +248,9 @@ def measure_peaks():
 
 
 def load_executed_taps(kind: str):
-    """Taps actually sampled per pixel visit of the propagate launch, from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    """Taps actually sampled per pixel visit of the propagate launch, from the committed measurement
+    (profiles/executed_taps.json, made by --count-taps on the instrumented engine)."""
+    p = os.path.join(ROOT, "profiles", "executed_taps.json")
     try:
         e = json.load(open(p)).get(kind) or {}
         v = e.get("executed_taps_per_pixel_visit")
@@ -446,9 +450,9 @@ def run_engine(args, rank, world, local_rank):
                      "algorithmic_bytes_per_launch": int(visits * taps_per_visit * l1_bytes_per_tap),
                      "algorithmic_taps_per_visit": taps_per_visit,
                      "executed_taps_per_visit": executed,
-                     "executed_note": "taps actually sampled per pixel visit (ncu thread-level sampling "
-                                      "instructions; duplicate neighbour planes and wholly-outside sources skip "
-                                      "theirs), from profiles/ncu_traffic.json"},
+                     "executed_note": "taps actually sampled per pixel visit, counted by the instrumented engine "
+                                      "(duplicate neighbour planes and wholly-outside sources skip theirs), from "
+                                      "profiles/executed_taps.json"},
         "roofline_hbm": {"bound": "hbm", "achieved": round(achieved_hbm, 2), "peak": hbm_peak, "unit": "GB/s",
                          "frac": round(achieved_hbm / hbm_peak, 5), "peak_source": hbm_src + " (MEASURED_PEAKS.json)",
                          "traffic": None if traffic_per_visit is None else round(traffic_per_visit * visits),
@@ -711,6 +715,44 @@ def run_serving(args, hp, device: int):
     }
 
 
+def run_count_taps(args):
+    """Executed taps: the instrumented engine counts, per sampled (candidate, source), its window's taps
+    (wholly-outside sources and duplicate neighbour planes are skipped, as in the timed kernels).  Views 0 and
+    10 of the headline workload are solved pass by pass (hp_propagate_pass), so only the half-passes count."""
+    import ctypes as C
+    hp = importlib.import_module(PKG)
+    L = C.CDLL(hp.LIB_PATH)
+    if not hasattr(L, "hp_debug_taps"):
+        raise SystemExit("--count-taps needs HP_ENGINE_LIB=<pkg>/lib/libhpmvs_count.so (make -C <pkg> count)")
+    f32c, f16c = C.c_ulonglong(), C.c_ulonglong()
+    s = build_scene(WORKLOAD["views"])
+    out = {}
+    refs = [0, 10]
+    with hp.Context(0) as ctx:
+        ids = [ctx.upload(v.image) for v in s.views]
+        cam = lambda i: hp.make_camera(s.views[i].cam.K, s.views[i].cam.R, s.views[i].cam.t)
+        for name, prec in (("f32", hp.PRECISION_F32), ("f16acc", hp.PRECISION_F16ACC)):
+            per_it = np.zeros(WORKLOAD["iterations"])
+            for r in refs:
+                job = hp.make_job(ids[r], [ids[i] for i in s.sources[r]], cam(r), [cam(i) for i in s.sources[r]],
+                                  *WORKLOAD["depth_range"], seed=42, view_id=r, iterations=WORKLOAD["iterations"])
+                p = hp.default_params(radius=WORKLOAD["radius"], stride=WORKLOAD["stride"], precision=prec)
+                m, _, _, _ = hp.host_maps(s.height, s.width)
+                ctx.init_hypotheses(job, p, m)
+                ctx.ncc_cost(job, p, m)
+                L.hp_debug_taps(C.byref(f32c), C.byref(f16c))
+                for it in range(WORKLOAD["iterations"]):
+                    for color in (0, 1):
+                        ctx.propagate_pass(job, p, m, it, color)
+                    L.hp_debug_taps(C.byref(f32c), C.byref(f16c))
+                    per_it[it] += (f32c if name == "f32" else f16c).value
+            visits_per_it = len(refs) * s.height * s.width  # two half-passes of W * H / 2 visits per view
+            out[name] = {"executed_taps_per_pixel_visit": round(float(per_it.sum() / (visits_per_it * len(per_it))), 1),
+                         "per_iteration": [round(float(x / visits_per_it), 1) for x in per_it],
+                         "algorithmic_taps_per_pixel_visit": 6 * WORKLOAD["sources"] * 64, "views": refs}
+    return out
+
+
 def run_reference_params(hp, ctx, stream):
     """The engine at the parameters the reference's own kernels support (REF_PARAM_WORKLOADS: radius 5, stride 1),
     per view as the reference solves (one hp_solve per view), FP32 and FP16-acc, device-resident maps, CUDA
@@ -824,6 +866,9 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if world != args.gpus:
         print(f"warning: --gpus {args.gpus} but WORLD_SIZE {world}", file=sys.stderr)
+    if args.count_taps:
+        print(json.dumps({"executed_taps": run_count_taps(args)}))
+        return
     if args.serve_only:
         hp = importlib.import_module(PKG)
         print(json.dumps({"serving": run_serving(args, hp, local_rank)}))

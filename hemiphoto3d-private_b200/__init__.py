@@ -18,7 +18,9 @@ from typing import List, Optional, Sequence
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "lib", "libhpmvs.so")
+# HP_ENGINE_LIB loads another build of the engine (the instrumented
+# lib/libhpmvs_count.so of `make count`, for the bench's --count-taps).
+LIB_PATH = os.environ.get("HP_ENGINE_LIB") or os.path.join(_HERE, "lib", "libhpmvs.so")
 
 MAX_SOURCES = 8
 MAX_RADIUS = 7

@@ -43,6 +43,12 @@ namespace hp {
 namespace f16 {
 namespace {
 
+#ifdef HP_COUNT_TAPS
+// Instrumented builds only (make count): taps sampled, window taps per
+// (candidate, source) whose window is not wholly outside the source.
+__device__ unsigned long long g_taps;
+#endif
+
 // Tile shapes: TILE_W x TH pixels per CTA, TH warps (one per tile row).
 template <int TH>
 struct Tile {
@@ -474,12 +480,18 @@ __device__ __forceinline__ float cost_f16(RefStats st, const __half2* s_win, con
         float c = 2.0f;
         if (outside) {
         } else if (soft) {
+#ifdef HP_COUNT_TAPS
+            atomicAdd(&g_taps, static_cast<unsigned long long>(Win<R, ST>::N));
+#endif
             const uint2* qb = soft_base(v->src_quad[s]);
             c = all_inside ? source_cost<R, ST, false, true, NT, D>(P, 0, qb, st, s_win, s_ref, tw, lx, ly, x,
                                                              y, fW, fH)
                            : source_cost<R, ST, true, true, NT, D>(P, 0, qb, st, s_win, s_ref, tw, lx, ly, x,
                                                             y, fW, fH);
         } else {
+#ifdef HP_COUNT_TAPS
+            atomicAdd(&g_taps, static_cast<unsigned long long>(Win<R, ST>::N));
+#endif
             const cudaTextureObject_t tex = v->src_tex16[s];
             c = all_inside ? source_cost<R, ST, false, false, NT, D>(P, tex, nullptr, st, s_win, s_ref, tw, lx, ly, x, y,
                                                               fW, fH)
@@ -778,6 +790,16 @@ struct Dispatch {
     }
 };
 
+#ifdef HP_COUNT_TAPS
+unsigned long long taps_read_reset() {
+    unsigned long long v = 0, z = 0;
+    cudaDeviceSynchronize();
+    cudaMemcpyFromSymbol(&v, g_taps, sizeof v);
+    cudaMemcpyToSymbol(g_taps, &z, sizeof z);
+    return v;
+}
+#endif
+
 }  // namespace
 }  // namespace f16
 
@@ -789,5 +811,10 @@ cudaError_t f16_dispatch_th8(int mode, int radius, int stride, int staging, cons
 cudaError_t f16_dispatch_th4(int mode, int radius, int stride, int staging, const BatchList* bl,
                              const SolveConsts& sc, int iteration, int color, const Schedule* s, int grid,
                              cudaStream_t st, int* occ);
+#ifdef HP_COUNT_TAPS
+unsigned long long f16_taps_th8();
+unsigned long long f16_taps_th4();
+unsigned long long f32_taps();
+#endif
 
 }  // namespace hp

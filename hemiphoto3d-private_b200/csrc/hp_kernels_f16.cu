@@ -5,6 +5,10 @@
 
 namespace hp {
 
+#ifdef HP_COUNT_TAPS
+unsigned long long f16_taps_th8() { return f16::taps_read_reset(); }
+#endif
+
 cudaError_t f16_dispatch_th8(int mode, int radius, int stride, int staging, const BatchList* bl,
                              const SolveConsts& sc, int iteration, int color, const Schedule* s, int grid,
                              cudaStream_t st, int* occ) {
@@ -45,3 +49,13 @@ cudaError_t persistent_occupancy_f16(const SolveConsts& sc, int* blocks_per_sm) 
 }
 
 }  // namespace hp
+
+#ifdef HP_COUNT_TAPS
+// Instrumented builds only: taps sampled by the FP32 and FP16 kernels since
+// the last call (both counters are reset).
+extern "C" int hp_debug_taps(unsigned long long* f32, unsigned long long* f16) {
+    *f32 = hp::f32_taps();
+    *f16 = hp::f16_taps_th8() + hp::f16_taps_th4();
+    return 0;
+}
+#endif

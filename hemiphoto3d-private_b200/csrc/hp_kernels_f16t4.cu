@@ -5,6 +5,10 @@
 
 namespace hp {
 
+#ifdef HP_COUNT_TAPS
+unsigned long long f16_taps_th4() { return f16::taps_read_reset(); }
+#endif
+
 cudaError_t f16_dispatch_th4(int mode, int radius, int stride, int staging, const BatchList* bl,
                              const SolveConsts& sc, int iteration, int color, const Schedule* s, int grid,
                              cudaStream_t st, int* occ) {

@@ -30,6 +30,18 @@
 
 namespace hp {
 
+#ifdef HP_COUNT_TAPS
+// Instrumented builds only (make count): taps sampled.
+__device__ unsigned long long g_taps32;
+unsigned long long f32_taps() {
+    unsigned long long v = 0, z = 0;
+    cudaDeviceSynchronize();
+    cudaMemcpyFromSymbol(&v, g_taps32, sizeof v);
+    cudaMemcpyToSymbol(g_taps32, &z, sizeof z);
+    return v;
+}
+#endif
+
 namespace {
 
 constexpr int MAX_TW = TILE_W + 2 * HP_MAX_RADIUS;
@@ -147,6 +159,9 @@ __device__ __forceinline__ float cost_f32(const float* __restrict__ s_ref, int t
             // Cost 2 would change nothing in the running top-3 (every entry is <= 2).
             if (front && (left || right || top_ || bottom)) continue;
         }
+#ifdef HP_COUNT_TAPS
+        atomicAdd(&g_taps32, static_cast<unsigned long long>(SIDE * SIDE));
+#endif
 #pragma unroll 1
         for (int i = 0; i < SIDE; ++i) {
             const float wpy = fy + static_cast<float>(i * ST - R);
