@@ -434,9 +434,8 @@ __device__ __forceinline__ float cost_f16(RefStats st, const __half2* s_win, con
         // corners inside [lo, W - 1 + lo) x [lo, H - 1 + lo) by a 0.05 px
         // margin (which covers the rounding of the row-stepped taps and of the
         // corners themselves, stepped here from the first along the window's
-        // edges), tested as w_x >= ulo w_z etc. without a division.  The warp
-        // of the window rectangle is then the convex quad of its corners, so
-        // every tap is valid by the per-tap rules too.
+        // edges).  The warp of the window rectangle is then the convex quad of
+        // its corners, so every tap is valid by the per-tap rules too.
         const float ulo = __fadd_rn(lo, 0.05f), uhi = __fsub_rn(__fadd_rn(fW, lo), 1.05f);
         const float vhi = __fsub_rn(__fadd_rn(fH, lo), 1.05f);
         constexpr float SPAN = static_cast<float>((Win<R, ST>::SIDE - 1) * ST);
@@ -460,18 +459,31 @@ __device__ __forceinline__ float cost_f16(RefStats st, const __half2* s_win, con
         // sampling.
         const float olo = __fsub_rn(lo, 0.05f), ohi = __fadd_rn(__fadd_rn(fW, lo), -0.95f);
         const float ovhi = __fadd_rn(__fadd_rn(fH, lo), -0.95f);
-        bool inside = true, front = true, left = true, right = true, top = true, bottom = true;
+        // Each corner is projected (approximate reciprocal, error far below the
+        // margin) and the tests run on the corners' bounding box: ~45
+        // instructions for the four corners instead of ~90 for per-corner
+        // products and compares.  A corner behind the camera fails `front`,
+        // and its garbage coordinates then decide nothing.
+        float umin = 0.f, umax = 0.f, vmin = 0.f, vmax = 0.f, zmin = 0.f;
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
-            const float wz = cz[c], wxc = cx[c], wyc = cy[c];
-            inside = inside && wz > 1e-6f && wxc >= __fmul_rn(ulo, wz) && wxc < __fmul_rn(uhi, wz) &&
-                     wyc >= __fmul_rn(ulo, wz) && wyc < __fmul_rn(vhi, wz);
-            front = front && wz > 1e-6f;
-            left = left && wxc < __fmul_rn(olo, wz);
-            right = right && wxc >= __fmul_rn(ohi, wz);
-            top = top && wyc < __fmul_rn(olo, wz);
-            bottom = bottom && wyc >= __fmul_rn(ovhi, wz);
+            const float iz = rcp_approx(cz[c]);
+            const float2 uv = __fmul2_rn(make_float2(cx[c], cy[c]), make_float2(iz, iz));
+            if (c == 0) {
+                umin = umax = uv.x;
+                vmin = vmax = uv.y;
+                zmin = cz[c];
+            } else {
+                umin = fminf(umin, uv.x);
+                umax = fmaxf(umax, uv.x);
+                vmin = fminf(vmin, uv.y);
+                vmax = fmaxf(vmax, uv.y);
+                zmin = fminf(zmin, cz[c]);
+            }
         }
+        const bool front = zmin > 1e-6f;
+        const bool inside = front && umin >= ulo && umax < uhi && vmin >= ulo && vmax < vhi;
+        const bool left = umax < olo, right = umin >= ohi, top = vmax < olo, bottom = vmin >= ovhi;
         const bool outside = front && (left || right || top || bottom);
         // One form per warp for the lanes that sample: the checked form gives
         // the unchecked form's bits whenever every tap is valid, so lanes that
