@@ -77,8 +77,6 @@ hp_status check_params(hp_ctx* ctx, const hp_params* p) {
         return fail(ctx, HP_ERR_UNSUPPORTED, "tile width %d: the kernels use %d", p->tile_w, hp::TILE_W);
     if (p->tile_h != 0 && p->tile_h != 8 && !(p->tile_h == 4 && p->precision == HP_PRECISION_F16ACC))
         return fail(ctx, HP_ERR_UNSUPPORTED, "tile height %d: 8, or 4 on the FP16-acc path", p->tile_h);
-    if (p->early_reject < -1 || p->early_reject > 1)
-        return fail(ctx, HP_ERR_INVALID_ARG, "early_reject %d not -1, 0 or 1", p->early_reject);
     if (p->staging != 0 && p->staging != 4 && p->staging != 8)
         return fail(ctx, HP_ERR_INVALID_ARG, "staging %d not 0, 4 or 8", p->staging);
     return HP_OK;
@@ -98,7 +96,6 @@ hp::SolveConsts consts_of(const hp_params* p) {
                        : 0u;
     sc.tile_h = p->tile_h > 0 ? p->tile_h : hp::TILE_H;
     sc.staging = p->staging > 0 ? p->staging : 4;
-    sc.prune = p->precision == HP_PRECISION_F16ACC && p->early_reject >= 0 ? 1 : 0;
     return sc;
 }
 
@@ -503,7 +500,6 @@ void hp_params_default(hp_params* p) {
     p->filter_depth_tol = 0.12f;
     p->filter_normal_cos = -1.0f;
     p->staging = 0;
-    p->early_reject = 0;
 }
 
 hp_status hp_ctx_create(int device, hp_ctx** out) {

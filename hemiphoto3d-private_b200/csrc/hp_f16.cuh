@@ -384,54 +384,17 @@ __device__ __forceinline__ float source_cost(const Plane& P, cudaTextureObject_t
     return __fsub_rn(1.0f, ncc);
 }
 
-// The three lowest source costs so far (2 = none / invalid), in order.
-struct TopK {
-    float t0, t1, t2;
-};
-
-// Mean of the top-k lowest source costs (k = min(topk, S)): the view-selection
-// rule of computePixelCost (patchmatch_mvs.cu:309-337).
-__device__ __forceinline__ float topk_mean(const TopK& tk, int topk, int S) {
-    const int kk = min(topk, S);
-    float sum = tk.t0;
-    if (kk > 1) sum = __fadd_rn(sum, tk.t1);
-    if (kk > 2) sum = __fadd_rn(sum, tk.t2);
-    return __fdiv_rn(sum, static_cast<float>(kk));
-}
-
-// Exact early rejection.  With `remaining` sources still unscored (costs >= 0),
-// the final k lowest costs are at least, one by one, the k lowest of the
-// current ones together with `remaining` zeros, and rounded addition and
-// division are monotonic, so the final mean is at least the mean of those.
-// If that bound already reaches the pixel's current cost, the candidate cannot
-// be adopted (adoption needs a strictly lower cost), whatever the remaining
-// sources give.
-__device__ __forceinline__ bool cannot_win(const TopK& tk, int remaining, int topk, int S, float current) {
-    const int kk = min(topk, S);
-    if (remaining <= 0 || remaining >= kk) return false;
-    // Bound sums: (0, .., 0, t0) -> t0; for k = 3 and one left, (0, t0, t1) -> t0 + t1.
-    const float lb = remaining == kk - 1 ? tk.t0 : __fadd_rn(tk.t0, tk.t1);
-    return __fdiv_rn(lb, static_cast<float>(kk)) >= current;
-}
-
-constexpr int SCORED = 1, DEGENERATE = 0, REJECTED = 2;
-
-// Scores sources [s_begin, s_end) of plane (d, n) at pixel (x, y) into tk.
-// DEGENERATE: the plane is edge-on to the viewing ray (cost 2, as the
-// reference's |n.P| < 1e-8 rule).  With check, after each source it stops
-// with REJECTED once cannot_win holds for `current`.
 template <int R, int ST, int NT, int D>
-__device__ __noinline__ int cost_sources(RefStats st, const __half2* s_win, const float* s_ref, int tw, int lx,
-                                            int ly, int x, int y, float d, float cnx, float cny, float cnz,
-                                            const ViewDesc* __restrict__ v, unsigned soft_mask, int s_begin,
-                                            int s_end, TopK& tk, bool check, int topk, float current) {
+__device__ __forceinline__ float cost_f16(RefStats st, const __half2* s_win, const float* s_ref, int tw, int lx,
+                                          int ly, int x, int y, float d, float cnx, float cny, float cnz,
+                                          const ViewDesc* __restrict__ v, int topk, unsigned soft_mask) {
     const float* k = v->kinv;
     const float fx = static_cast<float>(x), fy = static_cast<float>(y);
     const float Px = __fmul_rn(d, __fmaf_rn(k[0], fx, __fmaf_rn(k[1], fy, k[2])));
     const float Py = __fmul_rn(d, __fmaf_rn(k[3], fx, __fmaf_rn(k[4], fy, k[5])));
     const float Pz = __fmul_rn(d, __fmaf_rn(k[6], fx, __fmaf_rn(k[7], fy, k[8])));
     const float ndp = __fmaf_rn(cnx, Px, __fmaf_rn(cny, Py, __fmul_rn(cnz, Pz)));
-    if (fabsf(ndp) < 1e-8f) return DEGENERATE;
+    if (fabsf(ndp) < 1e-8f) return 2.0f;
     const float ind = __frcp_rn(ndp);
     const float m0 = __fmul_rn(__fmaf_rn(k[0], cnx, __fmaf_rn(k[3], cny, __fmul_rn(k[6], cnz))), ind);
     const float m1 = __fmul_rn(__fmaf_rn(k[1], cnx, __fmaf_rn(k[4], cny, __fmul_rn(k[7], cnz))), ind);
@@ -439,9 +402,9 @@ __device__ __noinline__ int cost_sources(RefStats st, const __half2* s_win, cons
     const float fW = static_cast<float>(v->W), fH = static_cast<float>(v->H);
     const float xa = static_cast<float>(x - R);
     const float ya = static_cast<float>(y - R);
-    float top0 = tk.t0, top1 = tk.t1, top2 = tk.t2;
+    float top0 = 2.0f, top1 = 2.0f, top2 = 2.0f;
     const int S = v->S;
-    for (int s = s_begin; s < s_end; ++s) {
+    for (int s = 0; s < S; ++s) {
         // A (9) and b (3) of the source: three 16-byte loads (ViewDesc::ab is 16-byte aligned).
         const float4* A4 = reinterpret_cast<const float4*>(v->ab[s]);
         const float4 q0 = __ldg(A4), q1 = __ldg(A4 + 1), q2 = __ldg(A4 + 2);
@@ -554,50 +517,18 @@ __device__ __noinline__ int cost_sources(RefStats st, const __half2* s_win, cons
                 if (top1 < top0) { t = top0; top0 = top1; top1 = t; }
             }
         }
-        if (check && cannot_win(TopK{top0, top1, top2}, S - 1 - s, topk, S, current)) {
-            tk = TopK{top0, top1, top2};
-            return REJECTED;
-        }
     }
-    tk = TopK{top0, top1, top2};
-    return SCORED;
-}
-
-// Top-k mean NCC cost of plane (d, n) at pixel (x, y) over all the view's sources.
-template <int R, int ST, int NT, int D>
-__device__ __forceinline__ float cost_f16(RefStats st, const __half2* s_win, const float* s_ref, int tw, int lx,
-                                          int ly, int x, int y, float d, float cnx, float cny, float cnz,
-                                          const ViewDesc* __restrict__ v, int topk, unsigned soft_mask) {
-    TopK tk{2.0f, 2.0f, 2.0f};
-    if (cost_sources<R, ST, NT, D>(st, s_win, s_ref, tw, lx, ly, x, y, d, cnx, cny, cnz, v, soft_mask, 0, v->S, tk,
-                                   false, topk, 0.0f) == DEGENERATE)
-        return 2.0f;
-    return topk_mean(tk, topk, v->S);
+    const int kk = min(topk, S);
+    float sum = top0;
+    if (kk > 1) sum = __fadd_rn(sum, top1);
+    if (kk > 2) sum = __fadd_rn(sum, top2);
+    return __fdiv_rn(sum, static_cast<float>(kk));
 }
 
 __device__ __forceinline__ bool same_plane16(float4 a, float4 b) {
     return __float_as_uint(a.x) == __float_as_uint(b.x) && __float_as_uint(a.y) == __float_as_uint(b.y) &&
            __float_as_uint(a.z) == __float_as_uint(b.z) && __float_as_uint(a.w) == __float_as_uint(b.w);
 }
-
-// A neighbour candidate that survived the first sources: its top-k so far and its item.
-struct Surv {
-    float t0, t1, t2;
-    int item;
-};
-
-// Dynamic shared memory of the half-pass and persistent kernels: the
-// reference window (s_win), each warp's queue of surviving candidates (a ring
-// of QCAP), and each pixel's cost before the pass.
-template <int R, int ST, int TH>
-struct Dyn {
-    static constexpr int NT = 32 * TH;
-    static constexpr int QCAP = 64;
-    static constexpr size_t WIN = Win<R, ST>::IN_SMEM ? WIN_PAIRS_MAX * NT * sizeof(__half2) : 16;
-    static constexpr size_t QUEUE = static_cast<size_t>(TH) * QCAP * sizeof(Surv);
-    static constexpr size_t BEST = NT * sizeof(float);
-    static constexpr size_t BYTES = WIN + QUEUE + BEST;
-};
 
 template <int R, int ST, int TH, int D>
 __device__ __forceinline__ void tile_cost16(const ViewDesc* v, int tile_x, int tile_y, const SolveConsts& sc,
@@ -651,7 +582,7 @@ struct PassSmem {
 template <int R, int ST, int TH, int D>
 __device__ __forceinline__ void tile_propagate16(const ViewDesc* v, int tile_x, int tile_y, const SolveConsts& sc,
                                                  int iteration, int color, float* s_ref, __half2* s_win,
-                                                 PassSmem<TH>& sm, Surv* s_queue, float* s_best) {
+                                                 PassSmem<TH>& sm) {
     constexpr int NT = Tile<TH>::NT, WARPS = TH;
     constexpr int tw = TILE_W + 2 * R, th = TH + 2 * R;
     const int x0 = tile_x * TILE_W, y0 = tile_y * TH;
@@ -693,7 +624,6 @@ __device__ __forceinline__ void tile_propagate16(const ViewDesc* v, int tile_x, 
         }
     }
     sm.stat[threadIdx.x] = make_float2(st.mean, st.ssd);
-    s_best[threadIdx.x] = best_cost;
     const int cnt = __popc(need);
     int incl = cnt;
 #pragma unroll
@@ -716,81 +646,20 @@ __device__ __forceinline__ void tile_propagate16(const ViewDesc* v, int tile_x, 
             if (need & (1u << cand)) sm.items[k++] = static_cast<unsigned short>((ly << 7) | (lane << 2) | cand);
     }
     __syncthreads();  // the CTA's item list is complete
-    // Exact early rejection (sc.prune): every item first scores sources
-    // [0, SA), SA = S - k + 1, where k = min(top_k, S); an item whose top-k
-    // bound (cannot_win) already reaches its owner's cost is settled there.
-    // The survivors go to the warp's queue and are scored on the remaining
-    // sources 32 at a time, so the rejected work leaves no lane idle.
-    const int S = v->S, kk = min(sc.top_k, S);
-    const int SA = (sc.prune && kk >= 2) ? S - kk + 1 : S;
-    Surv* q = s_queue + ly * Dyn<R, ST, TH>::QCAP;
-    int qh = 0, qt = 0;  // warp-uniform ring indices
-    // Scores item `item` (from its first unscored source with top-k state tk)
-    // and leaves its cost - or +inf when it cannot win - in its owner's slot.
-    auto score = [&](int item, int s_begin, TopK tk, bool* queued) {
-        const int oly = item >> 7, owner = (item >> 2) & 31, cand = item & 3;
-        const int oy = y0 + oly, olx = 2 * owner + ((oy + color) & 1), ox = x0 + olx;
-        const float2 os = sm.stat[oly * 32 + owner];
-        const float current = s_best[oly * 32 + owner];
-        const int nxp = ox + (cand == 0 ? -1 : (cand == 1 ? 1 : 0));
-        const int nyp = oy + (cand == 2 ? -1 : (cand == 3 ? 1 : 0));
-        const float4 h = v->hyp[static_cast<size_t>(nyp) * W + nxp];
-        const int s_end = s_begin == 0 ? SA : S;
-        const int r = cost_sources<R, ST, NT, D>(RefStats{os.x, os.y}, s_win + (oly * 32 + owner) * Win<R, ST>::VEC,
-                                                 s_ref, tw, olx, oly, ox, oy, h.x, h.y, h.z, h.w, v, sc.soft_mask,
-                                                 s_begin, s_end, tk, s_begin > 0, sc.top_k, current);
-        float c;
-        if (r == DEGENERATE) {
-            c = 2.0f;
-        } else if (r == REJECTED) {
-            c = __int_as_float(0x7f800000);
-        } else if (s_end == S) {
-            c = topk_mean(tk, sc.top_k, S);
-        } else if (cannot_win(tk, S - s_end, sc.top_k, S, current)) {
-            c = __int_as_float(0x7f800000);
-        } else {
-            *queued = true;
-            return tk;
+    for (int base = ly * 32; base < total; base += NT) {
+        const int w = base + lane;
+        if (w < total) {
+            const int item = sm.items[w];
+            const int oly = item >> 7, owner = (item >> 2) & 31, cand = item & 3;
+            const int oy = y0 + oly, olx = 2 * owner + ((oy + color) & 1), ox = x0 + olx;
+            const float2 os = sm.stat[oly * 32 + owner];
+            const int nxp = ox + (cand == 0 ? -1 : (cand == 1 ? 1 : 0));
+            const int nyp = oy + (cand == 2 ? -1 : (cand == 3 ? 1 : 0));
+            const float4 h = v->hyp[static_cast<size_t>(nyp) * W + nxp];
+            sm.cost[oly][item & 127] = cost_f16<R, ST, NT, D>(RefStats{os.x, os.y}, s_win + (oly * 32 + owner) * Win<R, ST>::VEC, s_ref, tw,
+                                                       olx, oly, ox, oy, h.x, h.y, h.z, h.w, v, sc.top_k,
+                                                       sc.soft_mask);
         }
-        sm.cost[oly][item & 127] = c;
-        return tk;
-    };
-    // One scoring site for both kinds of work, so the cost code is inlined
-    // once: each warp step takes the queue's next 32 survivors when it holds
-    // that many, else the next 32 items of the list, else the queue's rest.
-    constexpr int QMASK = Dyn<R, ST, TH>::QCAP - 1;
-    int next = ly * 32;  // the warp's next slice of the item list
-    for (;;) {
-        const int queued_n = qt - qh;
-        const bool from_queue = queued_n >= 32 || (next >= total && queued_n > 0);
-        if (!from_queue && next >= total) break;
-        const int n = from_queue ? min(32, queued_n) : min(32, total - next);
-        bool queued = false;
-        TopK tk{2.0f, 2.0f, 2.0f};
-        int item = 0;
-        if (lane < n) {
-            int s_begin = 0;
-            if (from_queue) {
-                const Surv e = q[(qh + lane) & QMASK];
-                item = e.item;
-                tk = TopK{e.t0, e.t1, e.t2};
-                s_begin = SA;
-            } else {
-                item = sm.items[next + lane];
-            }
-            tk = score(item, s_begin, tk, &queued);
-        }
-        if (from_queue) {
-            qh += n;
-        } else {
-            next += NT;
-            if (SA < S) {
-                const unsigned qb = __ballot_sync(0xffffffffu, queued);
-                if (queued) q[(qt + __popc(qb & ((1u << lane) - 1u))) & QMASK] = Surv{tk.t0, tk.t1, tk.t2, item};
-                qt += __popc(qb);
-            }
-        }
-        __syncwarp();
     }
     __syncthreads();  // every neighbour cost is in its owner's slot
     if (!active) return;
@@ -841,15 +710,11 @@ template <int R, int ST, int TH, int D>
 __global__ void __launch_bounds__(Tile<TH>::NT, Tile<TH>::MIN_BLOCKS) propagate16_kernel(BatchList bl, SolveConsts sc,
                                                                                        int iteration, int color) {
     __shared__ float s_ref[(TILE_W + 2 * R) * (TH + 2 * R)];
+    __shared__ __align__(16) __half2 s_win[Win<R, ST>::IN_SMEM ? WIN_PAIRS_MAX * Tile<TH>::NT : 1];
     __shared__ PassSmem<TH> sm;
-    extern __shared__ __align__(16) unsigned char f16_dyn[];
-    using DL = Dyn<R, ST, TH>;
-    __half2* s_win = reinterpret_cast<__half2*>(f16_dyn);
-    Surv* s_queue = reinterpret_cast<Surv*>(f16_dyn + DL::WIN);
-    float* s_best = reinterpret_cast<float*>(f16_dyn + DL::WIN + DL::QUEUE);
     int tile_x, tile_y;
     const ViewDesc* v = locate_tile16(bl, blockIdx.x, &tile_x, &tile_y);
-    tile_propagate16<R, ST, TH, D>(v, tile_x, tile_y, sc, iteration, color, s_ref, s_win, sm, s_queue, s_best);
+    tile_propagate16<R, ST, TH, D>(v, tile_x, tile_y, sc, iteration, color, s_ref, s_win, sm);
 }
 
 // Persistent form (see Schedule and the FP32 persistent kernel): the stage
@@ -857,12 +722,8 @@ __global__ void __launch_bounds__(Tile<TH>::NT, Tile<TH>::MIN_BLOCKS) propagate1
 template <int R, int ST, int TH, int D>
 __global__ void __launch_bounds__(Tile<TH>::NT, Tile<TH>::MIN_BLOCKS) persistent16_kernel(Schedule s) {
     __shared__ float s_ref[(TILE_W + 2 * R) * (TH + 2 * R)];
+    __shared__ __align__(16) __half2 s_win[Win<R, ST>::IN_SMEM ? WIN_PAIRS_MAX * Tile<TH>::NT : 1];
     __shared__ PassSmem<TH> sm;
-    extern __shared__ __align__(16) unsigned char f16_dyn[];
-    using DL = Dyn<R, ST, TH>;
-    __half2* s_win = reinterpret_cast<__half2*>(f16_dyn);
-    Surv* s_queue = reinterpret_cast<Surv*>(f16_dyn + DL::WIN);
-    float* s_best = reinterpret_cast<float*>(f16_dyn + DL::WIN + DL::QUEUE);
     // The claimed tile lives in shared memory: thread 0 decodes it once and
     // publishes it after the stage, so no thread carries it through the body.
     __shared__ SchedTile s_tile;
@@ -882,7 +743,7 @@ __global__ void __launch_bounds__(Tile<TH>::NT, Tile<TH>::MIN_BLOCKS) persistent
             tile_cost16<R, ST, TH, D>(v, tx, ty, s.sc, s_ref, s_win);
         } else if (stage <= 2 * v->iterations) {
             const int k = stage - 1;
-            tile_propagate16<R, ST, TH, D>(v, tx, ty, s.sc, k >> 1, k & 1, s_ref, s_win, sm, s_queue, s_best);
+            tile_propagate16<R, ST, TH, D>(v, tx, ty, s.sc, k >> 1, k & 1, s_ref, s_win, sm);
         } else if (is_filter_stage(v, stage)) {
             tile_filter(s.views, v, tx, ty, true);  // geometric check, then the maps
         } else {
@@ -903,29 +764,13 @@ struct Dispatch {
     static cudaError_t run(int mode, const BatchList* bl, const SolveConsts& sc, int iteration, int color,
                            const Schedule* s, int grid, cudaStream_t st, int* occ) {
         constexpr int NT = Tile<TH>::NT;
-        constexpr size_t DYN = Dyn<R, ST, TH>::BYTES;
-        // The half-pass and persistent kernels use more than the default 48 KB
-        // of shared memory in all: allow it (a host-side function attribute;
-        // not issued while the stream is being captured - the plan sets it
-        // through its occupancy query before capturing).
-        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
-        if (!occ && st) cudaStreamIsCapturing(st, &cap);
-        if (occ || cap == cudaStreamCaptureStatusNone) {
-            cudaError_t e = cudaFuncSetAttribute(propagate16_kernel<R, ST, TH, D>,
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(DYN));
-            if (e == cudaSuccess)
-                e = cudaFuncSetAttribute(persistent16_kernel<R, ST, TH, D>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(DYN));
-            if (e != cudaSuccess) return e;
-        }
         if (mode == 2) {
-            if (occ)
-                return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, persistent16_kernel<R, ST, TH, D>, NT, DYN);
-            persistent16_kernel<R, ST, TH, D><<<grid, NT, DYN, st>>>(*s);
+            if (occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, persistent16_kernel<R, ST, TH, D>, NT, 0);
+            persistent16_kernel<R, ST, TH, D><<<grid, NT, 0, st>>>(*s);
         } else if (mode == 0) {
             cost16_kernel<R, ST, TH, D><<<bl->total_tiles, NT, 0, st>>>(*bl, sc);
         } else {
-            propagate16_kernel<R, ST, TH, D><<<bl->total_tiles, NT, DYN, st>>>(*bl, sc, iteration, color);
+            propagate16_kernel<R, ST, TH, D><<<bl->total_tiles, NT, 0, st>>>(*bl, sc, iteration, color);
         }
         return cudaGetLastError();
     }

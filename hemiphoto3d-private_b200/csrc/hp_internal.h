@@ -63,7 +63,6 @@ struct SolveConsts {
     unsigned soft_mask;  // FP16 path: sources sampled in software (bit per source)
     int tile_h;          // rows of a CTA's tile (TILE_W x tile_h pixels, tile_h warps): 8, or 4 (FP16 path)
     int staging;         // FP16 path: quad loads in flight per window row, 4 or 8
-    int prune;           // FP16 path: exact early rejection of neighbour candidates (same results)
 };
 
 // A batch launch covers the tiles of several views: view k owns flattened

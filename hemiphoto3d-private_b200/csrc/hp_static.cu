@@ -196,7 +196,6 @@ extern "C" hp_status hp_solve_static(int device, void* stream, const hp_job* job
     sc.soft_mask = 0;
     sc.tile_h = hp::TILE_H;
     sc.staging = 4;
-    sc.prune = 0;
 
     if ((e = hp::launch_init(bl, hp::TILE_H, st)) != cudaSuccess) return bail(e);
     if ((e = hp::launch_cost_f32(bl, sc, st)) != cudaSuccess) return bail(e);

@@ -118,13 +118,6 @@ typedef struct hp_params {
     /* FP16-acc path: quad loads in flight per window row (the staging depth):
      * 4 or 8; 0 = 4, or for plans the autotuner's pick.  Same bits either way. */
     int staging;
-    /* FP16-acc path: exact early rejection of neighbour candidates.  After
-     * S - k + 1 of its S sources (k = min(top_k, S)) a candidate whose lowest
-     * possible top-k mean already reaches the pixel's current cost cannot be
-     * adopted, so its remaining sources are not scored; the surviving
-     * candidates are re-packed so no lane idles.  Same bits either way.
-     * 0 = engine default (on), 1 = on, -1 = off. */
-    int early_reject;
 } hp_params;
 
 /* One SfM seed in a reference view: pixel, depth and camera-frame normal. */

@@ -1,9 +1,8 @@
 """FP16-acc kernel variants the batched form's autotuner chooses between: the tile height (64 x 8
 pixels per CTA with 8 warps, or 64 x 4 with 4) and the staging depth (4 or 8 quad loads in flight per
-window row); and the exact early rejection of neighbour candidates.  They change how work is grouped
-into CTAs, when loads are issued and which sure losers are left unscored, never the arithmetic of a
-pixel, so every variant must give the same bits - initial costs, whole solves (ragged tiles at the
-view edges included), plans under both schedules, with and without the fused filter."""
+window row).  They change how work is grouped into CTAs and when loads are issued, never the
+arithmetic of a pixel, so every variant must give the same bits - initial costs, whole solves (ragged
+tiles at the view edges included), plans under both schedules, with and without the fused filter."""
 from __future__ import annotations
 
 import numpy as np
@@ -67,39 +66,14 @@ def test_variants_give_the_same_solve(hp, setup, filtered):
                 assert np.array_equal(x, y)
 
 
-@pytest.mark.parametrize("top_k,n_src", [(3, 4), (2, 3), (1, 4), (3, 2)])
-def test_early_rejection_gives_the_same_solve(hp, setup, scene_mod, top_k, n_src):
-    """Rejected candidates are exactly those whose best possible top-k mean already reaches the pixel's
-    cost, so switching the rejection off changes no bit (including k = 1, where nothing is rejected, and
-    fewer sources than k)."""
-    s, ctx, ids = setup
-    jobs = []
-    for r in s.refs:
-        srcs = s.sources[r][:n_src]
-        jobs.append(hp.make_job(ids[r], [ids[i] for i in srcs], hp.make_camera(*cam_of(s, r)),
-                                [hp.make_camera(*cam_of(s, i)) for i in srcs], *s.depth_range, seed=9 + r,
-                                view_id=r, iterations=4))
-    res = []
-    for er in (1, -1):
-        outs = [hp.host_maps(s.height, s.width) for _ in jobs]
-        ctx.solve(jobs, hp.default_params(precision=hp.PRECISION_F16ACC, radius=7, stride=2, top_k=top_k,
-                                          early_reject=er), [o[0] for o in outs])
-        res.append([o[1:] for o in outs])
-    for a, b in zip(*res):
-        for x, y in zip(a, b):
-            assert np.array_equal(x, y)
-
-
 @pytest.mark.parametrize("schedule", [1, 2])
 def test_tile4_plans_equal_solve(hp, setup, schedule):
     s, ctx, ids = setup
     jobs = [_job(hp, s, ids, r, iterations=it) for r, it in ((0, 3), (2, 2), (4, 1))]
     want = [hp.host_maps(s.height, s.width) for _ in jobs]
-    ctx.solve(jobs, _params(hp, 8, 4, radius=7, stride=2, filter_min_consistent=2, early_reject=-1),
-              [w[0] for w in want])
+    ctx.solve(jobs, _params(hp, 8, 4, radius=7, stride=2, filter_min_consistent=2), [w[0] for w in want])
     got = [hp.host_maps(s.height, s.width) for _ in jobs]
-    with hp.Plan(ctx, jobs, _params(hp, 4, 8, radius=7, stride=2, filter_min_consistent=2, early_reject=1),
-                 [g[0] for g in got],
+    with hp.Plan(ctx, jobs, _params(hp, 4, 8, radius=7, stride=2, filter_min_consistent=2), [g[0] for g in got],
                  hp.plan_options(schedule=schedule)) as plan:
         for _ in range(2):
             plan.run()
