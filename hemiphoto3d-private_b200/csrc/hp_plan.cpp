@@ -613,6 +613,18 @@ hp_status hp_plan_tune(hp_plan* p, int repeats, hp_plan_info* best) {
         return HP_OK;
     };
     hp_status st;
+    // A failure while the device side is rebuilt for another tile height
+    // (device memory, say) restores the plan's configuration before returning.
+    const int keep_th = p->tile_h, keep_depth = p->depth;
+    auto restore = [&](hp_status err) {
+        p->opt = keep;
+        p->depth = keep_depth;
+        if (p->tile_h != keep_th || !p->block) {
+            if (build_device(p, keep_th) != HP_OK) return err;  // the plan stays unusable: err says why
+        }
+        plan_occupancy(p);
+        return err;
+    };
     // Stage 1 (FP16-acc path, where the caller left them to the engine): tile
     // height x staging depth, each timed with the per-pass graph.
     const bool f16 = p->params.precision == HP_PRECISION_F16ACC;
@@ -623,15 +635,12 @@ hp_status hp_plan_tune(hp_plan* p, int repeats, hp_plan_info* best) {
         float best_ms = -1.f;
         int best_th = p->tile_h, best_d = p->depth;
         for (int th : th_opts) {
-            if (th != p->tile_h && (st = build_device(p, th)) != HP_OK) return st;
+            if (th != p->tile_h && (st = build_device(p, th)) != HP_OK) return restore(st);
             for (int d : d_opts) {
                 p->depth = d;
                 p->opt.schedule = HP_SCHEDULE_PER_PASS;
                 float ms = 0.f;
-                if ((st = timed(&ms)) != HP_OK) {
-                    p->opt = keep;
-                    return st;
-                }
+                if ((st = timed(&ms)) != HP_OK) return restore(st);
                 if (best_ms < 0.f || ms < best_ms) {
                     best_ms = ms;
                     best_th = th;
@@ -639,9 +648,9 @@ hp_status hp_plan_tune(hp_plan* p, int repeats, hp_plan_info* best) {
                 }
             }
         }
-        if (best_th != p->tile_h && (st = build_device(p, best_th)) != HP_OK) return st;
+        if (best_th != p->tile_h && (st = build_device(p, best_th)) != HP_OK) return restore(st);
         p->depth = best_d;
-        if ((st = plan_occupancy(p)) != HP_OK) return st;
+        if ((st = plan_occupancy(p)) != HP_OK) return restore(st);
     }
     // Stage 2: the schedule - the per-pass graph, or the persistent kernel at
     // each resident-CTA count up to its occupancy maximum.
