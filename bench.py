@@ -53,7 +53,7 @@ BATCHED = dict(name="batched_uneven_64", views=64, sizes=[[640, 480], [1280, 720
                sources=[2, 8], iterations=[6, 12], radius=7, stride=2, views_per_size=9, runs=2, tune_repeats=1)
 SERVING = dict(name="serving_poisson", sizes=[[640, 480], [1920, 1080], [4000, 3000]], sources=[2, 8],
                iterations=[4, 12], radius=7, stride=2, requests=480, rate_per_s=10.0, views_per_size=9,
-               mem_fraction=0.8, passes_per_step=8, policy=0, step_budget_mpix=1200.0)
+               mem_fraction=0.8, passes_per_step=32, policy=1, step_budget_mpix=1200.0)
 
 
 def parse():
@@ -658,20 +658,18 @@ def run_serving(args, hp, device: int):
     srv.drain(timeout_ms=120000)
     srv.poll(capacity=16)
     srv.reset_stats()
-    done, outs = [], {}
-    lock = threading.Lock()
+    done = []
+    first_failure = None
 
     def producer():
+        # The server keeps each request's maps alive until its completion is polled.
         t0 = time.perf_counter()
         for t_arr, job, w, h, _ in reqs:
             dt = t_arr - (time.perf_counter() - t0)
             if dt > 0:
                 time.sleep(dt)
-            m = hp.maps_of(torch.empty(h, w, device="cuda"), torch.empty(h, w, 3, device="cuda"),
-                           torch.empty(h, w, device="cuda"))
-            rid = srv.submit(job, m)
-            with lock:
-                outs[rid] = m
+            srv.submit(job, hp.maps_of(torch.empty(h, w, device="cuda"), torch.empty(h, w, 3, device="cuda"),
+                                       torch.empty(h, w, device="cuda")))
 
     t_start = time.perf_counter()
     th = threading.Thread(target=producer)
@@ -680,19 +678,25 @@ def run_serving(args, hp, device: int):
     while len(done) < len(reqs) and time.perf_counter() < deadline:
         for c in srv.poll(timeout_ms=100):
             done.append(c)
-            with lock:
-                outs.pop(c["request_id"], None)
+            if c["status"] != 0 and first_failure is None:
+                first_failure = {"at_s": round(time.perf_counter() - t_start, 1), "status": c["status"],
+                                 "server_error": srv.last_error()}
     wall = time.perf_counter() - t_start
     th.join()
     st = srv.stats()
     srv.close()
     ctx.close()
     ok = [c for c in done if c["status"] == 0]
+    statuses = {}
+    for c in done:
+        if c["status"] != 0:
+            statuses[str(c["status"])] = statuses.get(str(c["status"]), 0) + 1
     lat = np.array([c["latency_ms"] for c in ok]) if ok else np.zeros(1)
     pix_iter = sum(r[4] for r in reqs) / 1e6
     offered = pix_iter / reqs[-1][0]
     return {
         "workload": SERVING["name"], "requests": len(reqs), "completed": len(ok), "failed": len(done) - len(ok),
+        "failed_by_status": statuses, "failed_steps": st["failed_steps"], "first_failure": first_failure,
         "rate_per_s": args.serve_rate, "offered_mpix_iter_per_s": round(offered, 1),
         "p50_ms": round(float(np.percentile(lat, 50)), 1), "p90_ms": round(float(np.percentile(lat, 90)), 1),
         "p99_ms": round(float(np.percentile(lat, 99)), 1),

@@ -126,7 +126,8 @@ class ServerOptions(C.Structure):
     _fields_ = [("max_active", C.c_int), ("mem_fraction", C.c_float), ("mem_limit", C.c_uint64),
                 ("passes_per_step", C.c_int), ("split_launches", C.c_int), ("ctas_per_sm", C.c_int),
                 ("inflight_steps", C.c_int), ("wait_limit_ms", C.c_int), ("policy", C.c_int),
-                ("step_budget_mpix", C.c_double)]
+                ("step_budget_mpix", C.c_double), ("debug_stall_request", C.c_uint64),
+                ("debug_stall_tile", C.c_int)]
 
 
 class Completion(C.Structure):
@@ -140,7 +141,7 @@ class ServerStats(C.Structure):
                 ("active", C.c_int), ("peak_active", C.c_int), ("p50_ms", C.c_double), ("p99_ms", C.c_double),
                 ("mean_ms", C.c_double), ("max_ms", C.c_double), ("pixel_iterations", C.c_double),
                 ("device_ms", C.c_double), ("state_bytes", C.c_uint64), ("peak_state_bytes", C.c_uint64),
-                ("budget_bytes", C.c_uint64)]
+                ("budget_bytes", C.c_uint64), ("failed_steps", C.c_uint64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -605,11 +606,14 @@ class Server:
 
     def submit(self, job: Job, maps: Maps) -> int:
         rid = C.c_uint64()
-        st = lib.hp_submit(self._h, C.byref(job), C.byref(maps), C.byref(rid))
+        # The maps are registered under the lock that poll() takes to release them, so a request that
+        # completes before submit returns still finds its entry.
+        with self._lock:
+            st = lib.hp_submit(self._h, C.byref(job), C.byref(maps), C.byref(rid))
+            if st == OK:
+                self._maps[rid.value] = maps
         if st != OK:
             self._fail(st, "hp_submit")
-        with self._lock:
-            self._maps[rid.value] = maps
         return rid.value
 
     def poll(self, timeout_ms: int = 0, capacity: int = 256) -> List[dict]:
@@ -641,6 +645,10 @@ class Server:
 
     def reset_stats(self):
         lib.hp_server_stats_reset(self._h)
+
+    def last_error(self) -> str:
+        """The server's most recent error message (a failed step names the request, stage and tile)."""
+        return lib.hp_server_last_error(self._h).decode()
 
     def close(self):
         if getattr(self, "_h", None):

@@ -92,10 +92,15 @@ struct BatchList {
 // later plain loads (PTX memory model: release/acquire at gpu scope, then
 // bar.sync), so the stage bodies read state with ordinary loads.  Waits are
 // bounded by wait_limit_ns; a wait that
-// runs out records SCHED_TIMEOUT in status[0] and raises status[1], and every
-// CTA then stops taking tickets.
+// runs out records SCHED_TIMEOUT in status[0] and its ticket in status[2] and
+// raises the abort flag, and every CTA then stops taking tickets.  The abort
+// flag is status[1] unless the launcher gives another word: the server shares
+// one between its launches, so the launches queued behind one that gave up
+// stop at their first claim (SCHED_ABORTED) instead of each waiting out the
+// limit on the state the first left unfinished.
 constexpr int SCHED_OK = 0;
 constexpr int SCHED_TIMEOUT = 1;
+constexpr int SCHED_ABORTED = 2;
 struct Schedule {
     const ViewDesc* views;
     const int* entry_ticket;      // n_entries + 1 (the last is the ticket total)
@@ -103,7 +108,8 @@ struct Schedule {
     int n_entries;
     int total;
     unsigned* counter;            // next ticket
-    int* status;                  // [0] SCHED_* code, [1] abort flag
+    int* status;                  // [0] SCHED_* code, [1] abort flag, [2] ticket whose wait ran out
+    int* abort;                   // abort flag (null: status + 1; the launchers fill it in)
     unsigned long long wait_limit_ns;
     int stall_view, stall_tile;   // this tile never reports completion (bounded-wait test); -1 = none
     SolveConsts sc;

@@ -41,7 +41,9 @@ cudaError_t launch_propagate_f16(const BatchList& bl, const SolveConsts& sc, int
 
 cudaError_t launch_persistent_f16(const Schedule& s, int grid, cudaStream_t st) {
     if (s.total <= 0 || grid <= 0) return cudaSuccess;
-    return dispatch(2, s.sc.tile_h, s.sc, nullptr, 0, 0, &s, grid, st, nullptr);
+    Schedule k = s;
+    if (!k.abort) k.abort = k.status + 1;
+    return dispatch(2, k.sc.tile_h, k.sc, nullptr, 0, 0, &k, grid, st, nullptr);
 }
 
 cudaError_t persistent_occupancy_f16(const SolveConsts& sc, int* blocks_per_sm) {

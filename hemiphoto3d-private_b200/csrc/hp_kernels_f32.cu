@@ -533,7 +533,9 @@ cudaError_t persistent_dispatch(int radius, int stride, const Schedule* s, int g
 
 cudaError_t launch_persistent_f32(const Schedule& s, int grid, cudaStream_t st) {
     if (s.total <= 0 || grid <= 0) return cudaSuccess;
-    return persistent_dispatch(s.sc.radius, s.sc.stride, &s, grid, st, nullptr);
+    Schedule k = s;
+    if (!k.abort) k.abort = k.status + 1;
+    return persistent_dispatch(k.sc.radius, k.sc.stride, &k, grid, st, nullptr);
 }
 
 cudaError_t persistent_occupancy_f32(int radius, int stride, int* blocks_per_sm) {

@@ -66,7 +66,7 @@ struct hp_plan {
     int* d_entry_ticket = nullptr;
     int2* d_entry_info = nullptr;
     int n_entries = 0, total = 0;
-    unsigned* d_counter = nullptr;  // [0] counter, then status[2] at +4 bytes, main_done at +16
+    unsigned* d_counter = nullptr;  // [0] counter, then status[3] at +4 bytes, main_done at +16
     int* d_status = nullptr;
     // Geometric-consistency stages: the filtered views in the order they run,
     // their per-view finished-tile counts, and the tickets of the solve proper.
@@ -159,7 +159,7 @@ cudaError_t enqueue(hp_plan* p) {
         const int grid = persistent_grid(p);
         e = f16 ? hp::launch_persistent_f16(s, grid, st) : hp::launch_persistent_f32(s, grid, st);
         if (e != cudaSuccess) return e;
-        return cudaMemcpyAsync(p->h_status, p->d_status, 2 * sizeof(int), cudaMemcpyDeviceToHost, st);
+        return cudaMemcpyAsync(p->h_status, p->d_status, 3 * sizeof(int), cudaMemcpyDeviceToHost, st);
     }
     const hp::SolveConsts sc = plan_consts(p);
     const hp::BatchList all = list_of(p, 0);
@@ -263,8 +263,9 @@ hp_status finish_run(hp_plan* p, float* ms) {
         ctx->prof.timed[kind] += 1;
     }
     if (effective_schedule(p) == HP_SCHEDULE_PERSISTENT && p->h_status[0] != hp::SCHED_OK)
-        return fail(ctx, HP_ERR_TIMEOUT, "plan: a persistent dependency wait ran out (status %d); no result",
-                    p->h_status[0]);
+        return fail(ctx, HP_ERR_TIMEOUT,
+                    "plan: a persistent dependency wait ran out (status %d, ticket %d of %d); no result",
+                    p->h_status[0], p->h_status[2], p->total);
     for (size_t k = 0; k < p->host.size(); ++k) {
         if (!p->staging[k]) continue;
         const hp::ViewDesc& v = p->host[k];
@@ -459,8 +460,8 @@ hp_status build_device(hp_plan* p, int tile_h) {
     HP_CUDA(cudaMemcpy(p->d_lists, ints.data(), ints.size() * sizeof(int), cudaMemcpyHostToDevice));
     HP_CUDA(cudaMemcpy(p->d_entry_ticket, eticket.data(), eticket.size() * sizeof(int), cudaMemcpyHostToDevice));
     HP_CUDA(cudaMemcpy(p->d_entry_info, einfo.data(), einfo.size() * sizeof(int2), cudaMemcpyHostToDevice));
-    HP_CUDA(cudaMallocHost(&p->h_status, 2 * sizeof(int)));
-    p->h_status[0] = p->h_status[1] = 0;
+    HP_CUDA(cudaMallocHost(&p->h_status, 3 * sizeof(int)));
+    p->h_status[0] = p->h_status[1] = p->h_status[2] = 0;
     HP_CUDA(cudaEventCreate(&p->ev0));
     HP_CUDA(cudaEventCreate(&p->ev1));
     return plan_occupancy(p);

@@ -19,13 +19,25 @@
 // copies and stream-ordered frees of finishing requests; an event.  Up to
 // inflight_steps steps are enqueued ahead of the oldest unfinished one, and
 // a request is reported complete once the event of its last step has fired.
+//
+// Failure containment: a step whose launch fails, or whose persistent kernel
+// gives up on a dependency wait, leaves its members' state part-way through
+// a stage.  Every admitted request is a member of every step, so the steps
+// queued behind it would wait on that state in turn, and so would each
+// request admitted later.  The launches of a server therefore share one
+// abort flag: the launches behind a failed one stop at their first ticket
+// claim.  The worker then retires the steps in flight, completes every
+// admitted request with the failure, clears the flag and goes on with the
+// queue, which is untouched.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
+#include <cstdio>
 #include <cstring>
+#include <string>
 #include <deque>
 #include <memory>
 #include <mutex>
@@ -145,15 +157,21 @@ struct SrvReq {
 struct StepRec {
     int ring = 0;
     int launches = 0;
+    bool launch_failed = false;  // an upload or launch error: the members' state is part-way
     std::vector<SrvReq*> members;
     std::vector<SrvReq*> finishing;
+    // Per launch the schedule's entry tickets and (member, stage) infos, kept
+    // to name the tile of a wait that ran out.
+    std::vector<std::vector<int>> tickets;
+    std::vector<std::vector<int2>> infos;
+    uint64_t step_no = 0;
 };
 
 // A ring slot: pinned upload area + device copy, status words read back.
 struct RingSlot {
     char* host = nullptr;
     char* dev = nullptr;
-    int* host_status = nullptr;  // 2 ints per launch
+    int* host_status = nullptr;  // 4 ints per launch: code, unused, ticket whose wait ran out, pad
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 
@@ -171,6 +189,7 @@ struct hp_server {
     size_t ring_bytes = 0;
     int max_launches = 1;
     RingSlot ring[kRing];
+    int* d_abort = nullptr;  // abort flag shared by the server's launches
 
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
@@ -376,6 +395,7 @@ bool enqueue_step(hp_server* s) {
     auto fail_step = [&](const char* what, cudaError_t e) {
         cudaGetLastError();
         set_err(s, what, e);
+        rec.launch_failed = true;
         for (CoreReq* c : sp.reqs) static_cast<SrvReq*>(c->user)->failed = true;
     };
     if (bytes > s->ring_bytes || rec.launches > s->max_launches) {
@@ -409,14 +429,21 @@ bool enqueue_step(hp_server* s) {
         sch.total = totals[l];
         sch.counter = reinterpret_cast<unsigned*>(slot.dev + off_ctr + 16 * l);
         sch.status = reinterpret_cast<int*>(slot.dev + off_ctr + 16 * l + 4);
+        sch.abort = s->d_abort;
         sch.wait_limit_ns = static_cast<unsigned long long>(ms) * 1000000ull;
         sch.stall_view = -1;
         sch.stall_tile = -1;
+        if (s->opt.debug_stall_request)
+            for (int k = 0; k < n; ++k)
+                if (static_cast<SrvReq*>(sp.reqs[k]->user)->id == s->opt.debug_stall_request) {
+                    sch.stall_view = k;
+                    sch.stall_tile = s->opt.debug_stall_tile;
+                }
         sch.sc = s->sc;
         const int grid = std::max(1, std::min(totals[l], s->sms * s->cpsm));
         e = f16 ? hp::launch_persistent_f16(sch, grid, s->stream) : hp::launch_persistent_f32(sch, grid, s->stream);
         if (e == cudaSuccess)
-            e = cudaMemcpyAsync(slot.host_status + 2 * l, sch.status, 2 * sizeof(int), cudaMemcpyDeviceToHost,
+            e = cudaMemcpyAsync(slot.host_status + 4 * l, sch.status, 3 * sizeof(int), cudaMemcpyDeviceToHost,
                                 s->stream);
         if (e != cudaSuccess) {
             fail_step("server: persistent launch", e);
@@ -452,6 +479,9 @@ bool enqueue_step(hp_server* s) {
     cudaEventRecord(slot.ev1, s->stream);
     for (CoreReq* c : sp.reqs) rec.members.push_back(static_cast<SrvReq*>(c->user));
     for (CoreReq* c : sp.finishing) rec.finishing.push_back(static_cast<SrvReq*>(c->user));
+    rec.tickets = std::move(tickets);
+    rec.infos = std::move(infos);
+    rec.step_no = s->step_no;
     {
         std::lock_guard<std::mutex> lk(s->mu);
         s->st.steps++;
@@ -464,33 +494,88 @@ bool enqueue_step(hp_server* s) {
     return true;
 }
 
-// Wait for the oldest step and report its finishing requests.
-void retire_oldest(hp_server* s) {
+// The member, stage and tile of `ticket` in launch l of a step, as text.
+std::string describe_ticket(const StepRec& rec, int l, int ticket) {
+    if (l < 0 || l >= static_cast<int>(rec.tickets.size())) return "an unknown tile";
+    const std::vector<int>& t = rec.tickets[l];
+    const std::vector<int2>& info = rec.infos[l];
+    if (info.empty() || ticket < 0 || ticket >= t.back()) return "an unknown tile";
+    const size_t e = static_cast<size_t>(std::upper_bound(t.begin(), t.begin() + info.size(), ticket) - t.begin()) - 1;
+    const int m = info[e].x;
+    if (m < 0 || m >= static_cast<int>(rec.members.size())) return "an unknown tile";
+    const SrvReq* r = rec.members[m];
+    char buf[192];
+    std::snprintf(buf, sizeof(buf), "request %llu (%dx%d, %d sources), stage %d, tile %d of %dx%d",
+                  static_cast<unsigned long long>(r->id), r->desc.W, r->desc.H, r->desc.S, info[e].y,
+                  ticket - t[e], r->desc.tiles_x, r->desc.tiles_y);
+    return buf;
+}
+
+// Wait for the oldest step and report its finishing requests.  True when the
+// step failed: an upload or launch error, a device error, or a persistent
+// launch that gave up (its own wait ran out, or it stopped on the shared
+// abort flag raised by an earlier launch).
+bool retire_oldest(hp_server* s) {
     StepRec rec = std::move(s->inflight.front());
     s->inflight.pop_front();
     RingSlot& slot = s->ring[rec.ring];
     cudaError_t e = cudaEventSynchronize(slot.ev1);
     const auto now = Clock::now();
-    bool timed_out = false;
+    bool failed = rec.launch_failed;
     if (e != cudaSuccess) {
         set_err(s, "server: step", e);
-        timed_out = true;
+        failed = true;
     } else {
-        for (int l = 0; l < rec.launches; ++l)
-            if (slot.host_status[2 * l] != hp::SCHED_OK) timed_out = true;
+        for (int l = 0; l < rec.launches; ++l) {
+            const int code = slot.host_status[4 * l];
+            if (code == hp::SCHED_OK) continue;
+            failed = true;
+            if (code == hp::SCHED_TIMEOUT) {
+                const std::string where = describe_ticket(rec, l, slot.host_status[4 * l + 2]);
+                std::lock_guard<std::mutex> lk(s->mu);
+                s->err = "server: a persistent dependency wait ran out in step " + std::to_string(rec.step_no) +
+                         " at " + where;
+            }
+        }
         float t = 0.f;
         if (cudaEventElapsedTime(&t, slot.ev0, slot.ev1) == cudaSuccess) {
             std::lock_guard<std::mutex> lk(s->mu);
             s->st.device_ms += t;
         }
     }
-    if (timed_out) {
-        // The kernel stopped taking work: every request in the step is suspect.
+    if (failed) {
         for (SrvReq* r : rec.members) r->failed = true;
         std::lock_guard<std::mutex> lk(s->mu);
-        if (s->err.empty()) s->err = "server: a persistent dependency wait ran out";
+        s->st.failed_steps++;
+        if (s->err.empty()) s->err = "server: a step stopped";
     }
     for (SrvReq* r : rec.finishing) complete(s, r, r->failed ? (e != cudaSuccess ? HP_ERR_CUDA : HP_ERR_TIMEOUT) : HP_OK, now);
+    return failed;
+}
+
+// After a failed step: retire the steps still in flight (their launches stop
+// at their first claim on the raised flag), complete every admitted request
+// with the failure (each was a member of the failed step or of one queued
+// behind it), release their state, and clear the abort flag.  The queue is
+// kept; its requests are admitted into clean steps afterwards.
+void recover(hp_server* s) {
+    while (!s->inflight.empty()) retire_oldest(s);
+    cudaError_t e = cudaStreamSynchronize(s->stream);
+    const auto now = Clock::now();
+    std::vector<CoreReq*> lost;
+    lost.swap(s->core.active);
+    for (CoreReq* c : lost) {
+        SrvReq* r = static_cast<SrvReq*>(c->user);
+        s->core.held -= c->bytes;
+        if (r->mem) cudaFreeAsync(r->mem, s->stream);
+        r->mem = nullptr;
+        complete(s, r, e != cudaSuccess ? HP_ERR_CUDA : HP_ERR_TIMEOUT, now);
+    }
+    cudaMemsetAsync(s->d_abort, 0, sizeof(int), s->stream);
+    cudaStreamSynchronize(s->stream);
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->st.active = 0;
+    s->st.state_bytes = s->core.held;
 }
 
 void worker_main(hp_server* s) {
@@ -531,12 +616,15 @@ void worker_main(hp_server* s) {
                     continue;
                 }
             }
-            retire_oldest(s);
+            if (retire_oldest(s)) recover(s);
         }
     }
 }
 
 void free_server(hp_server* s) {
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    if (s->d_abort) cudaFree(s->d_abort);
+    s->d_abort = nullptr;
     for (RingSlot& r : s->ring) {
         if (r.host) cudaFreeHost(r.host);
         if (r.dev) cudaFree(r.dev);
@@ -603,6 +691,8 @@ hp_status hp_server_create(hp_ctx* ctx, const hp_params* params, const hp_server
     if (o.inflight_steps < 1 || o.inflight_steps > kRing)
         return fail(ctx, HP_ERR_INVALID_ARG, "server_create: inflight_steps %d outside 1..%d", o.inflight_steps,
                     kRing);
+    if (o.debug_stall_request && o.debug_stall_tile < 0)
+        return fail(ctx, HP_ERR_INVALID_ARG, "server_create: debug_stall_tile %d negative", o.debug_stall_tile);
     if (o.wait_limit_ms < 1 || o.ctas_per_sm < 0)
         return fail(ctx, HP_ERR_INVALID_ARG, "server_create: invalid wait limit or CTA count");
     std::unique_ptr<hp_server> s(new hp_server);
@@ -642,8 +732,10 @@ hp_status hp_server_create(hp_ctx* ctx, const hp_params* params, const hp_server
     const size_t entries = static_cast<size_t>(o.max_active) * o.passes_per_step;
     s->ring_bytes = align256(o.max_active * sizeof(hp::ViewDesc)) + align256(16 * s->max_launches) +
                     s->max_launches * (align256((entries + 1) * sizeof(int)) + align256(entries * sizeof(int2)));
+    HP_CUDA(cudaMalloc(&s->d_abort, sizeof(int)));
+    HP_CUDA(cudaMemset(s->d_abort, 0, sizeof(int)));
     for (RingSlot& r : s->ring) {
-        HP_CUDA(cudaMallocHost(&r.host, s->ring_bytes + 2 * sizeof(int) * s->max_launches));
+        HP_CUDA(cudaMallocHost(&r.host, s->ring_bytes + 4 * sizeof(int) * s->max_launches));
         r.host_status = reinterpret_cast<int*>(r.host + s->ring_bytes);
         HP_CUDA(cudaMalloc(&r.dev, s->ring_bytes));
         HP_CUDA(cudaEventCreate(&r.ev0));

@@ -126,30 +126,41 @@ __device__ __forceinline__ SchedTile decode_ticket(const Schedule& s, int t) {
     return r;
 }
 
-// Raise the abort flag with `code` (the first code recorded wins).
-__device__ __forceinline__ void sched_abort(const Schedule& s, int code) {
-    atomicCAS(s.status, SCHED_OK, code);
-    atomicExch(s.status + 1, 1);
+// A wait of `ticket` ran out: record SCHED_TIMEOUT and the ticket (the first
+// recorded wins) and raise the abort flag.
+__device__ __forceinline__ void sched_abort(const Schedule& s, int ticket) {
+    if (atomicCAS(s.status, SCHED_OK, SCHED_TIMEOUT) == SCHED_OK) atomicExch(s.status + 2, ticket);
+    atomicExch(s.abort, 1);
 }
 
-// Bounded poll of thread 0: spins while ready() is false.  Bounded by the
-// schedule's time limit and by a poll count (in case the global timer stands
-// still); false when this or another CTA gave up.
+// The abort flag is up.  When another launch raised it (a shared flag), this
+// launch records SCHED_ABORTED: it stops with work left undone.
+__device__ __forceinline__ bool sched_aborted(const Schedule& s) {
+    if (!ld_relaxed_gpu(s.abort)) return false;
+    atomicCAS(s.status, SCHED_OK, SCHED_ABORTED);
+    return true;
+}
+
+// Bounded poll of thread 0 for `ticket`: spins while ready() is false.
+// Bounded by the schedule's time limit and by a poll count (in case the
+// global timer stands still); false when this or another CTA gave up.  The
+// time limit counts only after kMinPolls sleeping polls, so a step of the
+// global timer during a short wait cannot end it.
 struct WaitBudget {
     unsigned long long start = 0;
     unsigned polls = 0;
 };
 
 template <class Ready>
-__device__ __forceinline__ bool sched_poll(const Schedule& s, WaitBudget& b, Ready ready) {
-    constexpr unsigned kMaxPolls = 1u << 26;
+__device__ __forceinline__ bool sched_poll(const Schedule& s, int ticket, WaitBudget& b, Ready ready) {
+    constexpr unsigned kMinPolls = 4096, kMaxPolls = 1u << 26;
     while (!ready()) {
-        if (ld_relaxed_gpu(s.status + 1)) return false;
+        if (sched_aborted(s)) return false;
         if (++b.polls > 16) {
             const unsigned long long now = global_ns();
             if (b.start == 0) b.start = now;
-            if (now - b.start > s.wait_limit_ns || b.polls > kMaxPolls) {
-                sched_abort(s, SCHED_TIMEOUT);
+            if ((now - b.start > s.wait_limit_ns && b.polls > kMinPolls) || b.polls > kMaxPolls) {
+                sched_abort(s, ticket);
                 return false;
             }
             __nanosleep(256);
@@ -178,17 +189,18 @@ __device__ __forceinline__ bool sched_wait(const Schedule& s, const SchedTile& t
     WaitBudget b;
     for (int i = 0; i < n; ++i) {
         const int* flag = done + deps[i];
-        if (!sched_poll(s, b, [&] { return ld_acquire_gpu(flag) >= need; })) return false;
+        if (!sched_poll(s, t.ticket, b, [&] { return ld_acquire_gpu(flag) >= need; })) return false;
     }
     if (s.main_done && is_filter_stage(t.v, t.stage)) {
         const unsigned main_total = static_cast<unsigned>(s.main_total);
-        if (!sched_poll(s, b, [&] { return ld_acquire_gpu_u32(s.main_done) >= main_total; })) return false;
+        if (!sched_poll(s, t.ticket, b, [&] { return ld_acquire_gpu_u32(s.main_done) >= main_total; }))
+            return false;
         const int prev = t.v->filter->prev;
         if (prev >= 0) {
             const ViewDesc* pv = &s.views[prev];
             const int* cnt = pv->filter->tiles_done;
             const int want = pv->tiles_x * pv->tiles_y;
-            if (!sched_poll(s, b, [&] { return ld_acquire_gpu(cnt) >= want; })) return false;
+            if (!sched_poll(s, t.ticket, b, [&] { return ld_acquire_gpu(cnt) >= want; })) return false;
         }
     }
     return true;
@@ -211,7 +223,7 @@ __device__ __forceinline__ void sched_publish(const Schedule& s, const SchedTile
 // the schedule is exhausted or aborted (including a dependency wait of this
 // ticket that ran out).
 __device__ __forceinline__ bool sched_claim(const Schedule& s, SchedTile* out) {
-    if (ld_relaxed_gpu(s.status + 1)) return false;
+    if (sched_aborted(s)) return false;
     const int t = static_cast<int>(atomicAdd(s.counter, 1u));
     if (t >= s.total) return false;
     const SchedTile d = decode_ticket(s, t);

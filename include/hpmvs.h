@@ -435,6 +435,9 @@ typedef struct hp_server_options {
     int policy;             /* hp_server_policy (0 = round robin) */
     double step_budget_mpix; /* HP_SERVER_POLICY_BUDGET: work per step, in 1e6 pixel x source stage
                               * units (0 = 1200, ~0.2 s of FP16-acc r 7 s 2 work on a B200) */
+    uint64_t debug_stall_request; /* tests only: in the request with this id (0 = off), tile */
+    int debug_stall_tile;         /*   debug_stall_tile never reports completion, so the step's
+                                   *   bounded waits run out and the failure is contained */
 } hp_server_options;
 
 /* One finished request. */
@@ -454,6 +457,8 @@ typedef struct hp_server_stats {
     double device_ms;                         /* device time of all finished steps */
     uint64_t state_bytes, peak_state_bytes;   /* request state held now / at most */
     uint64_t budget_bytes;                    /* admission budget at the last admission */
+    uint64_t failed_steps;                    /* steps that failed (each fails the requests admitted
+                                               * at the time; hp_server_last_error says where) */
 } hp_server_stats;
 
 void hp_server_options_default(hp_server_options* o);

@@ -213,6 +213,45 @@ def test_device_outputs_and_memory_budget(hp, gctx, scenes, ids):
         assert np.array_equal(d.cpu().numpy(), ed) and np.array_equal(c.cpu().numpy(), ec)
 
 
+HP_ERR_TIMEOUT = 5
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [0, 1])
+def test_a_failed_step_is_contained(hp, gctx, scenes, ids, precision):
+    """A request with a tile that never reports completion (a test hook): the step's bounded waits run out
+    after 100 ms, the requests admitted with it fail with HP_ERR_TIMEOUT, the server's error names the request,
+    and requests submitted afterwards complete, bit-identical to hp_solve alone.  Before the shared abort
+    flag and the recovery, every later step waited on the failed request's unfinished tiles and failed too."""
+    params = hp.default_params(radius=5, stride=2, precision=precision)
+    reqs = _requests(hp, scenes, ids, 6, seed=21 + precision)
+
+    def run(srv, batch):
+        got, rid = {}, {}
+        for k, (j, h, w) in batch:
+            m, d, n, c = hp.host_maps(h, w)
+            rid[srv.submit(j, m)] = k
+            got[k] = (d, n, c)
+        srv.drain(timeout_ms=60000)
+        return {rid[c["request_id"]]: c["status"] for c in srv.poll(capacity=64)}, got, rid
+
+    with hp.Server(gctx, params, passes_per_step=4, wait_limit_ms=100, debug_stall_request=2,
+                   debug_stall_tile=1) as srv:
+        first, _, _ = run(srv, [(0, reqs[0])])
+        assert first == {0: 0}
+        # Request id 2 stalls; request 3 may be admitted beside it (and then fails with it) or after.
+        mid, _, rid = run(srv, [(1, reqs[1]), (2, reqs[2])])
+        assert mid[1] == HP_ERR_TIMEOUT and mid[2] in (0, HP_ERR_TIMEOUT)
+        assert "request 2 " in srv.last_error() and "wait ran out" in srv.last_error()
+        later, got, _ = run(srv, list(enumerate(reqs))[3:])
+        st = srv.stats()
+    assert later == {3: 0, 4: 0, 5: 0}
+    assert st["failed_steps"] >= 1 and st["failed"] == sum(v != 0 for v in mid.values())
+    for k, (d, n, c) in got.items():
+        ed, en, ec = _alone(hp, gctx, *reqs[k][:1], params, *reqs[k][1:])
+        assert np.array_equal(d, ed) and np.array_equal(n, en) and np.array_equal(c, ec), f"request {k}"
+
+
 @pytest.mark.gpu
 def test_queued_requests_are_cancelled_on_shutdown(hp, gctx, scenes, ids):
     params = hp.default_params(radius=5, stride=2, precision=1)
