@@ -90,6 +90,10 @@ def parse():
     ap.add_argument("--serve-budget", type=float, default=SERVING["step_budget_mpix"],
                     help="budget policy: work per step, 1e6 pixel x source stage units")
     ap.add_argument("--serve-seed", type=int, default=2024, help="arrival and request draw seed")
+    ap.add_argument("--serve-range", type=int, nargs=2, default=None, metavar=("FIRST", "END"),
+                    help="replay only requests [FIRST, END) of the drawn stream, arrivals shifted to start at 0")
+    ap.add_argument("--serve-log", default=None,
+                    help="write a memory/progress timeline, the failed requests and the server's errors here (JSON)")
     return ap.parse_args()
 
 
@@ -645,6 +649,10 @@ def run_serving(args, hp, device: int):
         job = hp.make_job(ids[r], [ids[j] for j in srcs], cams[r], [cams[j] for j in srcs], *sc.depth_range,
                           seed=7 + i, view_id=r, iterations=it)
         reqs.append((t, job, w, h, w * h * it))
+    if args.serve_range:
+        first, end = args.serve_range
+        t0_arr = reqs[first][0] - (reqs[first][0] - reqs[first - 1][0] if first > 0 else 0.0)
+        reqs = [(t - t0_arr, job, w, h, pi) for t, job, w, h, pi in reqs[first:end]]
     params = hp.default_params(radius=SERVING["radius"], stride=SERVING["stride"], precision=hp.PRECISION_F16ACC)
     srv = hp.Server(ctx, params, mem_fraction=SERVING["mem_fraction"], passes_per_step=args.serve_passes,
                     split_launches=args.serve_split, policy=args.serve_policy,
@@ -675,13 +683,27 @@ def run_serving(args, hp, device: int):
     th = threading.Thread(target=producer)
     th.start()
     deadline = t_start + reqs[-1][0] + 600
+    timeline, failures, t_next = [], [], 0.0
     while len(done) < len(reqs) and time.perf_counter() < deadline:
         for c in srv.poll(timeout_ms=100):
+            c["done_s"] = round(time.perf_counter() - t_start, 3)
             done.append(c)
-            if c["status"] != 0 and first_failure is None:
-                first_failure = {"at_s": round(time.perf_counter() - t_start, 1), "status": c["status"],
-                                 "server_error": srv.last_error()}
+            c["index"] = c["request_id"] - (len(pools) + 1) + (args.serve_range[0] if args.serve_range else 0)
+            if c["status"] != 0:
+                if first_failure is None:
+                    first_failure = {"at_s": c["done_s"], "status": c["status"], "server_error": srv.first_error()}
+                if len(failures) < 64:
+                    failures.append(c)
+        if args.serve_log and time.perf_counter() - t_start >= t_next:
+            t_next += 2.0
+            st_now = srv.stats()
+            timeline.append({"t": round(time.perf_counter() - t_start, 1), "done": len(done),
+                             **{k: st_now[k] for k in ("completed", "failed", "active", "queued", "state_bytes",
+                                                       "pool_reserved_bytes", "device_free_bytes", "budget_bytes",
+                                                       "steps", "failed_steps")},
+                             "torch_reserved": torch.cuda.memory_reserved()})
     wall = time.perf_counter() - t_start
+    first_error, last_error = srv.first_error(), srv.last_error()
     th.join()
     st = srv.stats()
     srv.close()
@@ -691,12 +713,24 @@ def run_serving(args, hp, device: int):
     for c in done:
         if c["status"] != 0:
             statuses[str(c["status"])] = statuses.get(str(c["status"]), 0) + 1
+    check = None
+    if hasattr(hp.lib, "hp_debug_check"):  # self-checking engine: the first failed range check, if any
+        import ctypes as C
+        a8, a4 = (C.c_int * 12)(), (C.c_int * 12)()
+        rc = hp.lib.hp_debug_check(a8, a4)
+        check = {"rc": rc, "th8": list(a8), "th4": list(a4)}
+    if args.serve_log:
+        with open(args.serve_log, "w") as f:
+            json.dump({"first_error": first_error, "last_error": last_error, "first_failure": first_failure,
+                       "failures": failures, "self_check": check, "timeline": timeline,
+                       "first_request": args.serve_range[0] if args.serve_range else 0}, f)
     lat = np.array([c["latency_ms"] for c in ok]) if ok else np.zeros(1)
     pix_iter = sum(r[4] for r in reqs) / 1e6
     offered = pix_iter / reqs[-1][0]
     return {
         "workload": SERVING["name"], "requests": len(reqs), "completed": len(ok), "failed": len(done) - len(ok),
         "failed_by_status": statuses, "failed_steps": st["failed_steps"], "first_failure": first_failure,
+        **({"self_check": check} if check is not None else {}),
         "rate_per_s": args.serve_rate, "offered_mpix_iter_per_s": round(offered, 1),
         "p50_ms": round(float(np.percentile(lat, 50)), 1), "p90_ms": round(float(np.percentile(lat, 90)), 1),
         "p99_ms": round(float(np.percentile(lat, 99)), 1),

@@ -141,7 +141,8 @@ class ServerStats(C.Structure):
                 ("active", C.c_int), ("peak_active", C.c_int), ("p50_ms", C.c_double), ("p99_ms", C.c_double),
                 ("mean_ms", C.c_double), ("max_ms", C.c_double), ("pixel_iterations", C.c_double),
                 ("device_ms", C.c_double), ("state_bytes", C.c_uint64), ("peak_state_bytes", C.c_uint64),
-                ("budget_bytes", C.c_uint64), ("failed_steps", C.c_uint64)]
+                ("budget_bytes", C.c_uint64), ("failed_steps", C.c_uint64), ("pool_reserved_bytes", C.c_uint64),
+                ("device_free_bytes", C.c_uint64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -219,6 +220,7 @@ def _load() -> C.CDLL:
         "hp_server_stats_get": (C.c_int, [C.c_void_p, P(ServerStats)]),
         "hp_server_stats_reset": (C.c_int, [C.c_void_p]),
         "hp_server_last_error": (C.c_char_p, [C.c_void_p]),
+        "hp_server_first_error": (C.c_char_p, [C.c_void_p]),
         "hp_server_destroy": (C.c_int, [C.c_void_p]),
         "hp_server_simulate": (C.c_int, [C.c_int, P(C.c_int), P(C.c_uint64), P(C.c_int), C.c_int, C.c_uint64,
                                          C.c_int, P(C.c_int), P(C.c_int), P(C.c_int)]),
@@ -249,7 +251,7 @@ EXPORTS = (
     "hp_plan_options_default", "hp_plan_create", "hp_plan_run", "hp_plan_launch", "hp_plan_wait", "hp_plan_tune",
     "hp_plan_get_info", "hp_plan_destroy", "hp_schedule_build", "hp_server_options_default", "hp_server_create",
     "hp_submit", "hp_poll", "hp_server_drain", "hp_server_stats_get", "hp_server_stats_reset",
-    "hp_server_last_error", "hp_server_destroy", "hp_server_simulate", "hp_server_simulate_policy",
+    "hp_server_last_error", "hp_server_first_error", "hp_server_destroy", "hp_server_simulate", "hp_server_simulate_policy",
     "hp_select_sources", "hp_project_seeds",
     "hp_ctx_set_image_cache", "hp_fuse_params_default", "hp_fuse_depth_maps",
 )
@@ -649,6 +651,10 @@ class Server:
     def last_error(self) -> str:
         """The server's most recent error message (a failed step names the request, stage and tile)."""
         return lib.hp_server_last_error(self._h).decode()
+
+    def first_error(self) -> str:
+        """The server's first error since creation ("" if none)."""
+        return lib.hp_server_first_error(self._h).decode()
 
     def close(self):
         if getattr(self, "_h", None):

@@ -30,6 +30,7 @@
 
 #include <cuda_fp16.h>
 
+#include "hp_check.cuh"
 #include "hp_internal.h"
 #include "hp_rng.cuh"
 #include "hp_filter.cuh"
@@ -318,6 +319,17 @@ __device__ __forceinline__ float source_cost(const Plane& P, cudaTextureObject_t
                         bu = skip ? SOFT_ORIGIN : bu;  // an in-bounds quad; the tap is masked
                         bv = skip ? SOFT_ORIGIN : bv;
                     }
+#ifdef HP_SELF_CHECK
+                    {
+                        const int xi = static_cast<int>(bu - SOFT_ORIGIN) >> 8;
+                        const int yi = static_cast<int>(bv - SOFT_ORIGIN) >> 8;
+                        if (!HP_CHECK(xi >= 0 && xi < static_cast<int>(fW) && yi >= 0 && yi < static_cast<int>(fH),
+                                      HP_CHECK_QUAD, x, y, xi, yi, CHECK ? 1 : 0, i * SIDE + j, wx, wy, wz, 0.f)) {
+                            bu = SOFT_ORIGIN;
+                            bv = SOFT_ORIGIN;
+                        }
+                    }
+#endif
                     wb[jj] = __byte_perm(bu, bv, 0x7430);
                     q[jj] = __ldg(qbase + soft_offset(bu, bv));
                     const float2 next = __fadd2_rn(wxy, make_float2(hx0, hx1));
@@ -655,6 +667,9 @@ __device__ __forceinline__ void tile_propagate16(const ViewDesc* v, int tile_x, 
             const float2 os = sm.stat[oly * 32 + owner];
             const int nxp = ox + (cand == 0 ? -1 : (cand == 1 ? 1 : 0));
             const int nyp = oy + (cand == 2 ? -1 : (cand == 3 ? 1 : 0));
+            if (!HP_CHECK(nxp >= 0 && nxp < W && nyp >= 0 && nyp < H, HP_CHECK_NEIGHBOUR, ox, oy, nxp, nyp, W, H,
+                          0.f, 0.f, 0.f, 0.f))
+                continue;
             const float4 h = v->hyp[static_cast<size_t>(nyp) * W + nxp];
             sm.cost[oly][item & 127] = cost_f16<R, ST, NT, D>(RefStats{os.x, os.y}, s_win + (oly * 32 + owner) * Win<R, ST>::VEC, s_ref, tw,
                                                        olx, oly, ox, oy, h.x, h.y, h.z, h.w, v, sc.top_k,
@@ -737,6 +752,20 @@ __global__ void __launch_bounds__(Tile<TH>::NT, Tile<TH>::MIN_BLOCKS) persistent
         // loaded from shared memory is generic: the FP32 kernel ran 22% slower).
         const ViewDesc* v = &s.views[s_tile.view];
         const int stage = s_tile.stage, tx = s_tile.tx, ty = s_tile.ty;
+#ifdef HP_SELF_CHECK
+        const bool state_ok = HP_CHECK(v->hyp && v->cost && v->done && v->W > 0 && v->H > 0, HP_CHECK_STATE, v->W,
+                                       v->H, stage, s_tile.tile, s_tile.view, 0, 0.f, 0.f, 0.f, 0.f);
+        const bool ticket_ok =
+            HP_CHECK(s_tile.tile >= 0 && s_tile.tile < v->tiles_x * v->tiles_y && stage >= 0 &&
+                         stage <= 2 * v->iterations + 1 + (v->filter ? 1 : 0),
+                     HP_CHECK_TICKET, s_tile.view, stage, s_tile.tile, v->tiles_x * v->tiles_y, v->iterations, 0, 0.f,
+                     0.f, 0.f, 0.f);
+        if (!state_ok || !ticket_ok) {
+            __syncthreads();
+            if (threadIdx.x == 0) sched_publish(s, s_tile);
+            continue;
+        }
+#endif
         if (stage == 0) {
             tile_init(v, tx, ty);
             __syncthreads();

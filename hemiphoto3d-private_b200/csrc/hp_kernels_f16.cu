@@ -8,6 +8,9 @@ namespace hp {
 #ifdef HP_COUNT_TAPS
 unsigned long long f16_taps_th8() { return f16::taps_read_reset(); }
 #endif
+#ifdef HP_SELF_CHECK
+cudaError_t f16_check_th8(int* out) { return check_read_reset(out); }
+#endif
 
 cudaError_t f16_dispatch_th8(int mode, int radius, int stride, int staging, const BatchList* bl,
                              const SolveConsts& sc, int iteration, int color, const Schedule* s, int grid,
@@ -51,6 +54,19 @@ cudaError_t persistent_occupancy_f16(const SolveConsts& sc, int* blocks_per_sm) 
 }
 
 }  // namespace hp
+
+#ifdef HP_SELF_CHECK
+namespace hp {
+cudaError_t f16_check_th4(int* out);
+}
+// Self-checking builds only: the first failed range check of the FP16 kernels
+// of each tile height since the last call (12 ints each: hits, kind, six
+// integers, four floats as bits; hits 0 = none), then cleared.
+extern "C" int hp_debug_check(int* th8, int* th4) {
+    if (hp::f16_check_th8(th8) != cudaSuccess) return 1;
+    return hp::f16_check_th4(th4) != cudaSuccess ? 1 : 0;
+}
+#endif
 
 #ifdef HP_COUNT_TAPS
 // Instrumented builds only: taps sampled by the FP32 and FP16 kernels since

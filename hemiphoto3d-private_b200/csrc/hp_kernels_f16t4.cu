@@ -8,6 +8,9 @@ namespace hp {
 #ifdef HP_COUNT_TAPS
 unsigned long long f16_taps_th4() { return f16::taps_read_reset(); }
 #endif
+#ifdef HP_SELF_CHECK
+cudaError_t f16_check_th4(int* out) { return check_read_reset(out); }
+#endif
 
 cudaError_t f16_dispatch_th4(int mode, int radius, int stride, int staging, const BatchList* bl,
                              const SolveConsts& sc, int iteration, int color, const Schedule* s, int grid,

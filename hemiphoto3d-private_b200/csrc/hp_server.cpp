@@ -200,6 +200,7 @@ struct hp_server {
     uint64_t next_id = 1;
     uint64_t outstanding = 0;           // submitted and not yet completed
     std::string err;
+    std::string first_err;              // the worker's first error since creation
     hp_server_stats st{};
     std::vector<double> latencies;
 
@@ -211,9 +212,16 @@ struct hp_server {
 
 namespace {
 
+// Worker-side error message (the caller-side ones of hp_submit do not count
+// as the server's first error).  Call with s->mu held.
+void note_err_locked(hp_server* s, std::string msg) {
+    if (s->first_err.empty()) s->first_err = msg;
+    s->err = std::move(msg);
+}
+
 void set_err(hp_server* s, const char* what, cudaError_t e) {
     std::lock_guard<std::mutex> lk(s->mu);
-    s->err = std::string(what) + ": " + cudaGetErrorString(e);
+    note_err_locked(s, std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
 }
 
 // Bytes of request state the server may hold: the byte limit, or the part of
@@ -224,6 +232,11 @@ uint64_t admission_budget(hp_server* s) {
     if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return 0;
     uint64_t pool_reserved = 0;
     cudaMemPoolGetAttribute(s->pool, cudaMemPoolAttrReservedMemCurrent, &pool_reserved);
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->st.device_free_bytes = fr;
+        s->st.pool_reserved_bytes = pool_reserved;
+    }
     const double used = static_cast<double>(tot - fr);
     const double other = std::max(0.0, used - static_cast<double>(pool_reserved));
     const double b = static_cast<double>(s->opt.mem_fraction) * static_cast<double>(tot) - other;
@@ -328,7 +341,7 @@ bool enqueue_step(hp_server* s) {
         s->core.queue.pop_front();
         {
             std::lock_guard<std::mutex> lk(s->mu);
-            s->err = "server: request state exceeds the admission budget";
+            note_err_locked(s, "server: request state exceeds the admission budget");
         }
         complete(s, r, HP_ERR_OUT_OF_MEMORY, Clock::now());
         return false;
@@ -511,6 +524,27 @@ std::string describe_ticket(const StepRec& rec, int l, int ticket) {
     return buf;
 }
 
+// The members of a step with their stage ranges, as text.
+std::string describe_members(const StepRec& rec) {
+    std::vector<int> lo(rec.members.size(), 1 << 30), hi(rec.members.size(), -1);
+    for (const std::vector<int2>& info : rec.infos)
+        for (const int2& e : info)
+            if (e.x >= 0 && e.x < static_cast<int>(rec.members.size())) {
+                lo[e.x] = std::min(lo[e.x], e.y);
+                hi[e.x] = std::max(hi[e.x], e.y);
+            }
+    std::string out;
+    for (size_t k = 0; k < rec.members.size(); ++k) {
+        const SrvReq* r = rec.members[k];
+        char buf[128];
+        std::snprintf(buf, sizeof(buf), "%s%llu (%dx%d, %d sources, stages %d-%d of %d)", k ? ", " : "",
+                      static_cast<unsigned long long>(r->id), r->desc.W, r->desc.H, r->desc.S, lo[k], hi[k],
+                      r->core.stages);
+        out += buf;
+    }
+    return out;
+}
+
 // Wait for the oldest step and report its finishing requests.  True when the
 // step failed: an upload or launch error, a device error, or a persistent
 // launch that gave up (its own wait ran out, or it stopped on the shared
@@ -523,7 +557,10 @@ bool retire_oldest(hp_server* s) {
     const auto now = Clock::now();
     bool failed = rec.launch_failed;
     if (e != cudaSuccess) {
-        set_err(s, "server: step", e);
+        const std::string msg = "server: step " + std::to_string(rec.step_no) + ": " + cudaGetErrorName(e) + " (" +
+                                cudaGetErrorString(e) + "); members: " + describe_members(rec);
+        std::lock_guard<std::mutex> lk(s->mu);
+        note_err_locked(s, msg);
         failed = true;
     } else {
         for (int l = 0; l < rec.launches; ++l) {
@@ -533,8 +570,8 @@ bool retire_oldest(hp_server* s) {
             if (code == hp::SCHED_TIMEOUT) {
                 const std::string where = describe_ticket(rec, l, slot.host_status[4 * l + 2]);
                 std::lock_guard<std::mutex> lk(s->mu);
-                s->err = "server: a persistent dependency wait ran out in step " + std::to_string(rec.step_no) +
-                         " at " + where;
+                note_err_locked(s, "server: a persistent dependency wait ran out in step " +
+                                       std::to_string(rec.step_no) + " at " + where);
             }
         }
         float t = 0.f;
@@ -547,7 +584,7 @@ bool retire_oldest(hp_server* s) {
         for (SrvReq* r : rec.members) r->failed = true;
         std::lock_guard<std::mutex> lk(s->mu);
         s->st.failed_steps++;
-        if (s->err.empty()) s->err = "server: a step stopped";
+        if (s->err.empty()) note_err_locked(s, "server: a step stopped");
     }
     for (SrvReq* r : rec.finishing) complete(s, r, r->failed ? (e != cudaSuccess ? HP_ERR_CUDA : HP_ERR_TIMEOUT) : HP_OK, now);
     return failed;
@@ -873,6 +910,14 @@ const char* hp_server_last_error(hp_server* s) {
     std::lock_guard<std::mutex> lk(s->mu);
     thread_local std::string copy;
     copy = s->err;
+    return copy.c_str();
+}
+
+const char* hp_server_first_error(hp_server* s) {
+    if (!s) return "null server";
+    std::lock_guard<std::mutex> lk(s->mu);
+    thread_local std::string copy;
+    copy = s->first_err;
     return copy.c_str();
 }
 

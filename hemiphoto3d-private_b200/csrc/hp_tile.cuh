@@ -3,6 +3,7 @@
 // schedule (ticket decoding, bounded dependency waits, completion flags).
 #pragma once
 
+#include "hp_check.cuh"
 #include "hp_internal.h"
 #include "hp_rng.cuh"
 
@@ -52,6 +53,9 @@ __device__ __forceinline__ void tile_unpack(const ViewDesc* v, int tile_x, int t
     const int ly = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int y = tile_y * v->tile_h + ly;
     if (y >= v->H) return;
+    if (!HP_CHECK(v->out_depth && v->out_normal && v->out_cost, HP_CHECK_OUTPUT, v->W, v->H, tile_x, tile_y, 0, 0,
+                  0.f, 0.f, 0.f, 0.f))
+        return;
     for (int j = 0; j < 2; ++j) {
         const int x = tile_x * TILE_W + j * 32 + lane;
         if (x >= v->W) continue;

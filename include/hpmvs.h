@@ -459,6 +459,8 @@ typedef struct hp_server_stats {
     uint64_t budget_bytes;                    /* admission budget at the last admission */
     uint64_t failed_steps;                    /* steps that failed (each fails the requests admitted
                                                * at the time; hp_server_last_error says where) */
+    uint64_t pool_reserved_bytes;             /* the server's memory pool at the last admission check */
+    uint64_t device_free_bytes;               /* free device memory at the last admission check */
 } hp_server_stats;
 
 void hp_server_options_default(hp_server_options* o);
@@ -477,6 +479,9 @@ hp_status hp_server_drain(hp_server* s, int timeout_ms);
 hp_status hp_server_stats_get(hp_server* s, hp_server_stats* stats);
 hp_status hp_server_stats_reset(hp_server* s);
 const char* hp_server_last_error(hp_server* s);
+/* The worker's first error since the server was created ("" if none): a later
+ * error (say, admissions refused after a device fault) does not replace it. */
+const char* hp_server_first_error(hp_server* s);
 /* Stops the worker after the requests already admitted finish; queued
  * requests complete with HP_ERR_CANCELLED (their completions are dropped). */
 hp_status hp_server_destroy(hp_server* s);
