@@ -639,7 +639,8 @@ def run_serving(args, hp, device: int):
         pools.append((sc, ids, cams, w, h))
     reqs = []
     t = 0.0
-    for i in range(args.serve_requests):
+    n_draw = max(args.serve_requests, args.serve_range[1]) if args.serve_range else args.serve_requests
+    for i in range(n_draw):
         t += rng.exponential(1.0 / args.serve_rate)
         sc, ids, cams, w, h = pools[int(rng.integers(0, len(pools)))]
         r = int(rng.integers(0, len(sc.views)))
