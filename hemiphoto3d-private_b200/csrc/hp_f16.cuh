@@ -444,10 +444,11 @@ __device__ __forceinline__ float cost_f16(RefStats st, const __half2* s_win, con
         }
         // Corner test: in front of the source (w_z > 1e-6) with all four
         // corners inside [lo, W - 1 + lo) x [lo, H - 1 + lo) by a 0.05 px
-        // margin (which covers the rounding of the row-stepped taps and of the
-        // corners themselves, stepped here from the first along the window's
-        // edges).  The warp of the window rectangle is then the convex quad of
-        // its corners, so every tap is valid by the per-tap rules too.
+        // margin, which covers the rounding of the row-stepped taps and of the
+        // corners themselves (stepped here from the first along the window's
+        // edges) where the homography is well conditioned (below).  The warp
+        // of the window rectangle is then the convex quad of its corners, so
+        // every tap is valid by the per-tap rules too.
         const float ulo = __fadd_rn(lo, 0.05f), uhi = __fsub_rn(__fadd_rn(fW, lo), 1.05f);
         const float vhi = __fsub_rn(__fadd_rn(fH, lo), 1.05f);
         constexpr float SPAN = static_cast<float>((Win<R, ST>::SIDE - 1) * ST);
@@ -493,7 +494,28 @@ __device__ __forceinline__ float cost_f16(RefStats st, const __half2* s_win, con
                 zmin = fminf(zmin, cz[c]);
             }
         }
-        const bool front = zmin > 1e-6f;
+        // Conditioning.  The corners above and the row-stepped taps of
+        // source_cost evaluate the homography in different orders, so their
+        // rounding differs: by at most (SIDE + 5) roundings of the largest
+        // partial sum, Mx = |h0| X1 + |h1| Y1 + |h2| for w_x (X1, Y1 bound the
+        // window's absolute pixel coordinates), likewise My and Mz.  In the
+        // projected coordinate that is (Mx + |u| Mz) (SIDE + 5) 2^-24 / z_min.
+        // A plane seen nearly edge-on makes the terms large and cancelling,
+        // and the corners can then pass the test while a tap falls outside
+        // the source.  The decision stands only while the bound (with |u|
+        // taken as at least 1, which also bounds the error of z) stays within
+        // 0.04 px of the 0.05 px margin; other windows take the per-tap
+        // checked form, which gives the same bits whenever every tap is valid.
+        // NaN or infinite corners fail the comparison too.
+        constexpr float COND = 0.04f / ((Win<R, ST>::SIDE + 6) * 5.9604645e-8f);
+        const float X1 = fabsf(xa) + SPAN, Y1 = fabsf(ya) + SPAN;
+        const float Mx = __fmaf_rn(fabsf(P.h[0]), X1, __fmaf_rn(fabsf(P.h[1]), Y1, fabsf(P.h[2])));
+        const float My = __fmaf_rn(fabsf(P.h[3]), X1, __fmaf_rn(fabsf(P.h[4]), Y1, fabsf(P.h[5])));
+        const float Mz = __fmaf_rn(fabsf(P.h[6]), X1, __fmaf_rn(fabsf(P.h[7]), Y1, fabsf(P.h[8])));
+        const float Ua = fmaxf(1.0f, fmaxf(fabsf(umin), fabsf(umax)));
+        const float Va = fmaxf(1.0f, fmaxf(fabsf(vmin), fabsf(vmax)));
+        const float zc = __fmul_rn(zmin, COND);
+        const bool front = zmin > 1e-6f && __fmaf_rn(Ua, Mz, Mx) <= zc && __fmaf_rn(Va, Mz, My) <= zc;
         const bool inside = front && umin >= ulo && umax < uhi && vmin >= ulo && vmax < vhi;
         const bool left = umax < olo, right = umin >= ohi, top = vmax < olo, bottom = vmin >= ovhi;
         const bool outside = front && (left || right || top || bottom);
