@@ -226,10 +226,12 @@ void set_err(hp_server* s, const char* what, cudaError_t e) {
 
 // Bytes of request state the server may hold: the byte limit, or the part of
 // mem_fraction * total that memory outside the server's pool leaves free.
-uint64_t admission_budget(hp_server* s) {
+// 0 with *err set when the device cannot be queried (a faulted context).
+uint64_t admission_budget(hp_server* s, cudaError_t* err) {
+    *err = cudaSuccess;
     if (s->opt.mem_limit) return s->opt.mem_limit;
     size_t fr = 0, tot = 0;
-    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return 0;
+    if ((*err = cudaMemGetInfo(&fr, &tot)) != cudaSuccess) return 0;
     uint64_t pool_reserved = 0;
     cudaMemPoolGetAttribute(s->pool, cudaMemPoolAttrReservedMemCurrent, &pool_reserved);
     {
@@ -316,9 +318,10 @@ cudaError_t materialise(hp_server* s, SrvReq* r) {
 // Compose and enqueue one step.  Returns false when nothing was enqueued.
 bool enqueue_step(hp_server* s) {
     uint64_t budget = 0;
+    cudaError_t budget_err = cudaSuccess;
     std::vector<CoreReq*> admitted;
     if (!s->core.queue.empty()) {
-        budget = admission_budget(s);
+        budget = admission_budget(s, &budget_err);
         s->core.admit(budget, &admitted);
     }
     const auto now = Clock::now();
@@ -341,9 +344,13 @@ bool enqueue_step(hp_server* s) {
         s->core.queue.pop_front();
         {
             std::lock_guard<std::mutex> lk(s->mu);
-            note_err_locked(s, "server: request state exceeds the admission budget");
+            if (budget_err != cudaSuccess)
+                note_err_locked(s, std::string("server: device memory query: ") + cudaGetErrorName(budget_err) +
+                                       " (" + cudaGetErrorString(budget_err) + ")");
+            else
+                note_err_locked(s, "server: request state exceeds the admission budget");
         }
-        complete(s, r, HP_ERR_OUT_OF_MEMORY, Clock::now());
+        complete(s, r, budget_err != cudaSuccess ? HP_ERR_CUDA : HP_ERR_OUT_OF_MEMORY, Clock::now());
         return false;
     }
     {
