@@ -501,6 +501,11 @@ def run_engine(args, rank, world, local_rank):
             line["batched"] = run_batched(args, hp, bctx)
         finally:
             bctx.close()
+    if hasattr(hp.lib, "hp_debug_check"):  # self-checking engine: failed range checks of every leg since serving's
+        import ctypes as C
+        a8, a4 = (C.c_int * 12)(), (C.c_int * 12)()
+        rc = hp.lib.hp_debug_check(a8, a4)
+        line["self_check"] = {"rc": rc, "th8": list(a8), "th4": list(a4)}
     # CPU baseline (rank 0, N = 1)
     if world == 1 and not args.no_cpu_baseline:
         rate, secs, thr, desc = cpu_sample(s, args.cpu_rows)
