@@ -61,6 +61,39 @@ int main(void) {
     assert [int(v) for v in out] == want
 
 
+# Every struct of the ABI and its ctypes mirror (field names are the header's).
+MIRRORS = [("hp_camera", "Camera"), ("hp_params", "Params"), ("hp_seed", "Seed"), ("hp_job", "Job"),
+           ("hp_maps", "Maps"), ("hp_profile", "Profile"), ("hp_plan_options", "PlanOptions"),
+           ("hp_plan_info", "PlanInfo"), ("hp_server_options", "ServerOptions"), ("hp_completion", "Completion"),
+           ("hp_server_stats", "ServerStats"), ("hp_sparse_points", "SparsePoints"),
+           ("hp_view_selection", "ViewSelection"), ("hp_fuse_view", "FuseView"), ("hp_fuse_params", "FuseParams"),
+           ("hp_point_cloud", "PointCloudC")]
+
+
+def test_every_mirror_matches_the_header_field_by_field(hp):
+    """sizeof and every field's offset of each ABI struct, from the C compiler, against the ctypes mirror."""
+    lines = []
+    for cname, pyname in MIRRORS:
+        fields = [f[0] for f in getattr(hp, pyname)._fields_]
+        lines.append(f'  printf("{cname} %zu", sizeof({cname}));')
+        for f in fields:
+            lines.append(f'  printf(" %zu", offsetof({cname}, {f}));')
+        lines.append('  printf("\\n");')
+    src = "#include <stdio.h>\n#include <stddef.h>\n#include \"hpmvs.h\"\nint main(void) {\n" + "\n".join(lines) + \
+        "\n  return 0; }\n"
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "t.c")
+        open(c, "w").write(src)
+        exe = os.path.join(d, "t")
+        subprocess.run(["gcc", "-std=c11", "-I", os.path.dirname(HEADER), "-o", exe, c], check=True)
+        out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout.splitlines()
+    got = {ln.split()[0]: [int(v) for v in ln.split()[1:]] for ln in out}
+    for cname, pyname in MIRRORS:
+        cls = getattr(hp, pyname)
+        want = [C.sizeof(cls)] + [getattr(cls, f[0]).offset for f in cls._fields_]
+        assert got[cname] == want, f"{cname} vs {pyname}: C {got[cname]}, ctypes {want}"
+
+
 def test_default_params_are_the_reference_constants(hp):
     p = hp.default_params()
     assert (p.radius, p.stride, p.top_k, p.refine_steps, p.precision) == (5, 1, 3, 2, 0)
