@@ -695,9 +695,9 @@ void hp_server_options_default(hp_server_options* o) {
     o->max_active = 64;
     o->mem_fraction = 0.8f;
     o->mem_limit = 0;
-    o->passes_per_step = 8;
-    o->policy = HP_SERVER_POLICY_ROUND_ROBIN;
-    o->step_budget_mpix = 0.0;
+    o->passes_per_step = 32;
+    o->policy = HP_SERVER_POLICY_BUDGET;
+    o->step_budget_mpix = 1200.0;
     o->split_launches = 0;
     o->ctas_per_sm = 0;
     o->inflight_steps = 2;

@@ -425,14 +425,18 @@ typedef struct hp_server_options {
     float mem_fraction;     /* admit while device memory in use stays <= this fraction
                              * of the device total (0 = 0.8) */
     uint64_t mem_limit;     /* if nonzero: byte budget for request state instead */
-    int passes_per_step;    /* stages per request per step, 1..64 (0 = 8; on B200 with mixed
-                             * 0.3-12 Mpix requests 8-12 gave the lowest p99 latency) */
+    int passes_per_step;    /* stages per request per step, 1..64 (0 = 8); with the budget
+                             * policy the most a request takes in one step */
     int split_launches;     /* 1: one launch per stage offset of a step (no waits between
                              * tiles); 0: one persistent launch per step */
     int ctas_per_sm;        /* resident CTAs per SM (0 = the occupancy maximum) */
     int inflight_steps;     /* steps enqueued ahead of the oldest unfinished one, 1..4 (0 = 2) */
     int wait_limit_ms;      /* bound on one inter-tile dependency wait (0 = 2000) */
-    int policy;             /* hp_server_policy (0 = round robin) */
+    int policy;             /* hp_server_policy (0 = round robin).  hp_server_options_default
+                             * sets the budget policy with 32 stages and 1200 M units a step:
+                             * on B200 with mixed 0.3-12 Mpix requests at 10/s it cut the
+                             * median p90 / p99 latency by about 20% against round robin
+                             * with 8 stages a step */
     double step_budget_mpix; /* HP_SERVER_POLICY_BUDGET: work per step, in 1e6 pixel x source stage
                               * units (0 = 1200, ~0.2 s of FP16-acc r 7 s 2 work on a B200) */
     uint64_t debug_stall_request; /* tests only: in the request with this id (0 = off), tile */

@@ -147,13 +147,16 @@ def _request_bytes(h, w):
 @pytest.mark.gpu
 @pytest.mark.parametrize("precision", [0, 1])
 @pytest.mark.parametrize("split", [0, 1])
-def test_results_same_alone_and_in_the_mix(hp, gctx, scenes, ids, precision, split):
-    """Requests submitted in waves while earlier ones run; each result equals hp_solve alone, bit for bit."""
+@pytest.mark.parametrize("policy", [0, 1])
+def test_results_same_alone_and_in_the_mix(hp, gctx, scenes, ids, precision, split, policy):
+    """Requests submitted in waves while earlier ones run; each result equals hp_solve alone, bit for bit,
+    under either step policy (the budget here is small enough that requests take different stage counts)."""
     params = hp.default_params(radius=5, stride=2, precision=precision)
     reqs = _requests(hp, scenes, ids, 12, seed=precision * 10 + split)
     expect = [_alone(hp, gctx, j, params, h, w) for j, h, w in reqs]
     got = {}
-    with hp.Server(gctx, params, max_active=6, passes_per_step=3, split_launches=split) as srv:
+    with hp.Server(gctx, params, max_active=6, passes_per_step=3, split_launches=split, policy=policy,
+                   step_budget_mpix=0.5) as srv:
         rid = {}
         pending = list(enumerate(reqs))
         done = []
