@@ -58,7 +58,7 @@ class Params(C.Structure):
         ("refine_steps", C.c_int), ("iter_decay", C.c_float), ("step_decay", C.c_float),
         ("tile_w", C.c_int), ("tile_h", C.c_int), ("soft_sources", C.c_int),
         ("filter_min_consistent", C.c_int), ("filter_depth_tol", C.c_float), ("filter_normal_cos", C.c_float),
-        ("staging", C.c_int),
+        ("staging", C.c_int), ("debug_checked_taps", C.c_int),
     ]
 
 

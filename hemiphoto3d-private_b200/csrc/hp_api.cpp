@@ -79,6 +79,12 @@ hp_status check_params(hp_ctx* ctx, const hp_params* p) {
         return fail(ctx, HP_ERR_UNSUPPORTED, "tile height %d: 8, or 4 on the FP16-acc path", p->tile_h);
     if (p->staging != 0 && p->staging != 4 && p->staging != 8)
         return fail(ctx, HP_ERR_INVALID_ARG, "staging %d not 0, 4 or 8", p->staging);
+    if (p->debug_checked_taps != 0 && p->debug_checked_taps != 1)
+        return fail(ctx, HP_ERR_INVALID_ARG, "debug_checked_taps %d not 0 or 1", p->debug_checked_taps);
+#ifndef HP_SELF_CHECK
+    if (p->debug_checked_taps)
+        return fail(ctx, HP_ERR_UNSUPPORTED, "debug_checked_taps needs the self-checking build (make check)");
+#endif
     return HP_OK;
 }
 
@@ -94,6 +100,7 @@ hp::SolveConsts consts_of(const hp_params* p) {
     sc.soft_mask = p->precision == HP_PRECISION_F16ACC
                        ? (p->soft_sources < 0 ? 0xFFu : static_cast<unsigned>(p->soft_sources) & 0xFFu)
                        : 0u;
+    if (p->precision == HP_PRECISION_F16ACC && p->debug_checked_taps) sc.soft_mask |= hp::SOFT_MASK_CHECKED;
     sc.tile_h = p->tile_h > 0 ? p->tile_h : hp::TILE_H;
     sc.staging = p->staging > 0 ? p->staging : 4;
     return sc;
@@ -500,6 +507,7 @@ void hp_params_default(hp_params* p) {
     p->filter_depth_tol = 0.12f;
     p->filter_normal_cos = -1.0f;
     p->staging = 0;
+    p->debug_checked_taps = 0;
 }
 
 hp_status hp_ctx_create(int device, hp_ctx** out) {

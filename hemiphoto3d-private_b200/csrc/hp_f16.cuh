@@ -516,13 +516,20 @@ __device__ __forceinline__ float cost_f16(RefStats st, const __half2* s_win, con
         const float Va = fmaxf(1.0f, fmaxf(fabsf(vmin), fabsf(vmax)));
         const float zc = __fmul_rn(zmin, COND);
         const bool front = zmin > 1e-6f && __fmaf_rn(Ua, Mz, Mx) <= zc && __fmaf_rn(Va, Mz, My) <= zc;
+        // SOFT_MASK_CHECKED (self-checking builds only, uniform over the
+        // launch) turns both shortcuts off, to test that they change no result.
+#ifdef HP_SELF_CHECK
+        const bool shortcuts = (soft_mask & SOFT_MASK_CHECKED) == 0u;
+#else
+        constexpr bool shortcuts = true;
+#endif
         const bool inside = front && umin >= ulo && umax < uhi && vmin >= ulo && vmax < vhi;
         const bool left = umax < olo, right = umin >= ohi, top = vmax < olo, bottom = vmin >= ovhi;
-        const bool outside = front && (left || right || top || bottom);
+        const bool outside = shortcuts && front && (left || right || top || bottom);
         // One form per warp for the lanes that sample: the checked form gives
         // the unchecked form's bits whenever every tap is valid, so lanes that
         // are inside lose nothing.
-        const bool all_inside = __all_sync(__activemask(), inside || outside);
+        const bool all_inside = shortcuts && __all_sync(__activemask(), inside || outside);
         float c = 2.0f;
         if (outside) {
         } else if (soft) {

@@ -57,10 +57,14 @@ struct ViewDesc {
 };
 
 // Solver constants for one launch.
+// SolveConsts::soft_mask bit 31 (tests only): no corner-test shortcuts in the
+// FP16 cost, every window through the per-tap checked form.
+constexpr unsigned SOFT_MASK_CHECKED = 1u << 31;
+
 struct SolveConsts {
     int radius, stride, top_k, refine_steps;
     float iter_decay, step_decay;
-    unsigned soft_mask;  // FP16 path: sources sampled in software (bit per source)
+    unsigned soft_mask;  // FP16 path: sources sampled in software (bit per source); SOFT_MASK_CHECKED
     int tile_h;          // rows of a CTA's tile (TILE_W x tile_h pixels, tile_h warps): 8, or 4 (FP16 path)
     int staging;         // FP16 path: quad loads in flight per window row, 4 or 8
 };

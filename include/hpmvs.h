@@ -118,6 +118,12 @@ typedef struct hp_params {
     /* FP16-acc path: quad loads in flight per window row (the staging depth):
      * 4 or 8; 0 = 4, or for plans the autotuner's pick.  Same bits either way. */
     int staging;
+    /* Tests only (0 = off; the self-checking build alone accepts 1, others
+     * return HP_ERR_UNSUPPORTED): 1 turns the FP16-acc path's corner-test
+     * shortcuts off, so every window takes the per-tap checked form and
+     * wholly-outside sources are sampled too.  The results are the same bits;
+     * the switch exists to test that. */
+    int debug_checked_taps;
 } hp_params;
 
 /* One SfM seed in a reference view: pixel, depth and camera-frame normal. */

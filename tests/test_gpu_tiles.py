@@ -102,3 +102,4 @@ def test_tuner_chooses_tile_and_staging(hp, setup):
         for g, w in zip(got, want):
             for x, y in zip(g[1:], w[1:]):
                 assert np.array_equal(x, y)
+
