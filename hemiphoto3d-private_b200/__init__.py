@@ -127,7 +127,7 @@ class ServerOptions(C.Structure):
                 ("passes_per_step", C.c_int), ("split_launches", C.c_int), ("ctas_per_sm", C.c_int),
                 ("inflight_steps", C.c_int), ("wait_limit_ms", C.c_int), ("policy", C.c_int),
                 ("step_budget_mpix", C.c_double), ("debug_stall_request", C.c_uint64),
-                ("debug_stall_tile", C.c_int)]
+                ("debug_stall_tile", C.c_int), ("debug_fail_step", C.c_int)]
 
 
 class Completion(C.Structure):

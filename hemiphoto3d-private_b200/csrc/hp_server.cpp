@@ -412,11 +412,16 @@ bool enqueue_step(hp_server* s) {
         off = align256(off + infos[l].size() * sizeof(int2));
     }
     const size_t bytes = off;
+    // A step that cannot run leaves its members part-way: raise the shared
+    // abort flag in stream order, so the launches queued behind it stop at
+    // their first claim instead of waiting out the limit on that state.
     auto fail_step = [&](const char* what, cudaError_t e) {
         cudaGetLastError();
         set_err(s, what, e);
         rec.launch_failed = true;
         for (CoreReq* c : sp.reqs) static_cast<SrvReq*>(c->user)->failed = true;
+        cudaMemsetAsync(s->d_abort, 0xff, sizeof(int), s->stream);
+        cudaGetLastError();
     };
     if (bytes > s->ring_bytes || rec.launches > s->max_launches) {
         // Cannot happen with the sizes fixed at creation (max_active views, passes_per_step offsets).
@@ -440,6 +445,11 @@ bool enqueue_step(hp_server* s) {
     }
     const bool f16 = s->params.precision == HP_PRECISION_F16ACC;
     const int ms = s->opt.wait_limit_ms > 0 ? s->opt.wait_limit_ms : 2000;
+    if (s->opt.debug_fail_step > 0 && s->step_no + 1 == static_cast<uint64_t>(s->opt.debug_fail_step) &&
+        rec.launches > 0) {  // tests: this step's launch fails on the host, nothing runs
+        fail_step("server: persistent launch (injected failure)", cudaErrorLaunchOutOfResources);
+        rec.launches = 0;
+    }
     for (int l = 0; l < rec.launches; ++l) {
         hp::Schedule sch{};
         sch.views = reinterpret_cast<const hp::ViewDesc*>(slot.dev);
@@ -552,11 +562,11 @@ std::string describe_members(const StepRec& rec) {
     return out;
 }
 
-// Wait for the oldest step and report its finishing requests.  True when the
-// step failed: an upload or launch error, a device error, or a persistent
-// launch that gave up (its own wait ran out, or it stopped on the shared
-// abort flag raised by an earlier launch).
-bool retire_oldest(hp_server* s) {
+// Wait for the oldest step and report its finishing requests.  HP_OK, or the
+// status its members fail with: HP_ERR_CUDA for an upload, launch or device
+// error, HP_ERR_TIMEOUT for a persistent launch that gave up (its own wait
+// ran out, or it stopped on the shared abort flag raised before it).
+hp_status retire_oldest(hp_server* s) {
     StepRec rec = std::move(s->inflight.front());
     s->inflight.pop_front();
     RingSlot& slot = s->ring[rec.ring];
@@ -587,14 +597,16 @@ bool retire_oldest(hp_server* s) {
             s->st.device_ms += t;
         }
     }
+    const hp_status code = !failed ? HP_OK : (e != cudaSuccess || rec.launch_failed ? HP_ERR_CUDA : HP_ERR_TIMEOUT);
     if (failed) {
         for (SrvReq* r : rec.members) r->failed = true;
         std::lock_guard<std::mutex> lk(s->mu);
         s->st.failed_steps++;
         if (s->err.empty()) note_err_locked(s, "server: a step stopped");
     }
-    for (SrvReq* r : rec.finishing) complete(s, r, r->failed ? (e != cudaSuccess ? HP_ERR_CUDA : HP_ERR_TIMEOUT) : HP_OK, now);
-    return failed;
+    // In a step that ran, a finishing request fails alone only when its result copy failed.
+    for (SrvReq* r : rec.finishing) complete(s, r, r->failed ? (failed ? code : HP_ERR_CUDA) : HP_OK, now);
+    return code;
 }
 
 // After a failed step: retire the steps still in flight (their launches stop
@@ -602,7 +614,7 @@ bool retire_oldest(hp_server* s) {
 // with the failure (each was a member of the failed step or of one queued
 // behind it), release their state, and clear the abort flag.  The queue is
 // kept; its requests are admitted into clean steps afterwards.
-void recover(hp_server* s) {
+void recover(hp_server* s, hp_status code) {
     while (!s->inflight.empty()) retire_oldest(s);
     cudaError_t e = cudaStreamSynchronize(s->stream);
     const auto now = Clock::now();
@@ -613,7 +625,7 @@ void recover(hp_server* s) {
         s->core.held -= c->bytes;
         if (r->mem) cudaFreeAsync(r->mem, s->stream);
         r->mem = nullptr;
-        complete(s, r, e != cudaSuccess ? HP_ERR_CUDA : HP_ERR_TIMEOUT, now);
+        complete(s, r, e != cudaSuccess ? HP_ERR_CUDA : code, now);
     }
     cudaMemsetAsync(s->d_abort, 0, sizeof(int), s->stream);
     cudaStreamSynchronize(s->stream);
@@ -660,7 +672,8 @@ void worker_main(hp_server* s) {
                     continue;
                 }
             }
-            if (retire_oldest(s)) recover(s);
+            const hp_status st = retire_oldest(s);
+            if (st != HP_OK) recover(s, st);
         }
     }
 }
@@ -737,6 +750,8 @@ hp_status hp_server_create(hp_ctx* ctx, const hp_params* params, const hp_server
                     kRing);
     if (o.debug_stall_request && o.debug_stall_tile < 0)
         return fail(ctx, HP_ERR_INVALID_ARG, "server_create: debug_stall_tile %d negative", o.debug_stall_tile);
+    if (o.debug_fail_step < 0)
+        return fail(ctx, HP_ERR_INVALID_ARG, "server_create: debug_fail_step %d negative", o.debug_fail_step);
     if (o.wait_limit_ms < 1 || o.ctas_per_sm < 0)
         return fail(ctx, HP_ERR_INVALID_ARG, "server_create: invalid wait limit or CTA count");
     std::unique_ptr<hp_server> s(new hp_server);

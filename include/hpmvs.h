@@ -448,6 +448,8 @@ typedef struct hp_server_options {
     uint64_t debug_stall_request; /* tests only: in the request with this id (0 = off), tile */
     int debug_stall_tile;         /*   debug_stall_tile never reports completion, so the step's
                                    *   bounded waits run out and the failure is contained */
+    int debug_fail_step;          /* tests only: step n (1-based; 0 = off) fails to launch on the
+                                   *   host, as a launch error would (its requests: HP_ERR_CUDA) */
 } hp_server_options;
 
 /* One finished request. */

@@ -265,3 +265,37 @@ def test_queued_requests_are_cancelled_on_shutdown(hp, gctx, scenes, ids):
         srv.submit(j, m)
     time.sleep(0.01)
     srv.close()  # returns once the admitted request has finished; the rest are cancelled
+
+
+HP_ERR_CUDA = 2
+
+
+@pytest.mark.gpu
+def test_a_failed_launch_is_contained_without_waiting_out_the_limit(hp, gctx, scenes, ids):
+    """A step whose launch fails on the host (a test hook injects it; nothing runs on the device): its
+    requests fail with HP_ERR_CUDA, the launches queued behind it stop at once on the raised abort flag
+    instead of waiting out the 30 s dependency limit, and later requests complete bit-identical to hp_solve."""
+    params = hp.default_params(radius=5, stride=2, precision=1)
+    reqs = _requests(hp, scenes, ids, 6, seed=31)
+    t0 = time.time()
+    with hp.Server(gctx, params, passes_per_step=2, wait_limit_ms=30000, debug_fail_step=2) as srv:
+        got, rid = {}, {}
+        for k, (j, h, w) in enumerate(reqs[:3]):
+            m, d, n, c = hp.host_maps(h, w)
+            rid[srv.submit(j, m)] = k
+        srv.drain(timeout_ms=60000)
+        first = {rid[c["request_id"]]: c["status"] for c in srv.poll(capacity=64)}
+        assert "injected" in srv.first_error()
+        for k, (j, h, w) in list(enumerate(reqs))[3:]:
+            m, d, n, c = hp.host_maps(h, w)
+            rid[srv.submit(j, m)] = k
+            got[k] = (d, n, c)
+        srv.drain(timeout_ms=60000)
+        later = {rid[c["request_id"]]: c["status"] for c in srv.poll(capacity=64)}
+        st = srv.stats()
+    assert time.time() - t0 < 20, "a queued launch waited out the dependency limit"
+    assert set(first.values()) <= {0, HP_ERR_CUDA} and HP_ERR_CUDA in first.values()
+    assert later == {3: 0, 4: 0, 5: 0} and st["failed_steps"] >= 1
+    for k, (d, n, c) in got.items():
+        ed, en, ec = _alone(hp, gctx, *reqs[k][:1], params, *reqs[k][1:])
+        assert np.array_equal(d, ed) and np.array_equal(n, en) and np.array_equal(c, ec), f"request {k}"
