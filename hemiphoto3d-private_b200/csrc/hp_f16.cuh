@@ -506,7 +506,8 @@ __device__ __forceinline__ float cost_f16(RefStats st, const __half2* s_win, con
         // taken as at least 1, which also bounds the error of z) stays within
         // 0.04 px of the 0.05 px margin; other windows take the per-tap
         // checked form, which gives the same bits whenever every tap is valid.
-        // NaN or infinite corners fail the comparison too.
+        // NaN or infinite corners fail the comparison too.  COND counts one
+        // rounding more than the bound above, for slack.
         constexpr float COND = 0.04f / ((Win<R, ST>::SIDE + 6) * 5.9604645e-8f);
         const float X1 = fabsf(xa) + SPAN, Y1 = fabsf(ya) + SPAN;
         const float Mx = __fmaf_rn(fabsf(P.h[0]), X1, __fmaf_rn(fabsf(P.h[1]), Y1, fabsf(P.h[2])));
