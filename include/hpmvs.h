@@ -440,9 +440,9 @@ typedef struct hp_server_options {
     int wait_limit_ms;      /* bound on one inter-tile dependency wait (0 = 2000) */
     int policy;             /* hp_server_policy (0 = round robin).  hp_server_options_default
                              * sets the budget policy with 32 stages and 1200 M units a step:
-                             * on B200 with mixed 0.3-12 Mpix requests at 10/s it cut the
-                             * median p90 / p99 latency by about 20% against round robin
-                             * with 8 stages a step */
+                             * on B200 with mixed 0.3-12 Mpix requests at 10/s it lowered p50
+                             * and p90 latency by 15-20% against round robin with 8 stages
+                             * a step; p99 moved by -20% to +5% over the runs measured */
     double step_budget_mpix; /* HP_SERVER_POLICY_BUDGET: work per step, in 1e6 pixel x source stage
                               * units (0 = 1200, ~0.2 s of FP16-acc r 7 s 2 work on a B200) */
     uint64_t debug_stall_request; /* tests only: in the request with this id (0 = off), tile */
