@@ -299,3 +299,14 @@ def test_a_failed_launch_is_contained_without_waiting_out_the_limit(hp, gctx, sc
     for k, (d, n, c) in got.items():
         ed, en, ec = _alone(hp, gctx, *reqs[k][:1], params, *reqs[k][1:])
         assert np.array_equal(d, ed) and np.array_equal(n, en) and np.array_equal(c, ec), f"request {k}"
+
+
+def test_server_option_defaults(hp):
+    """hp_server_options_default: the budget policy (oldest first, at most 32 stages a request, 1200 M
+    W*H*S units a step), 64 slots, 80% of device memory, 2 steps in flight, 2 s dependency limit, no
+    test hooks."""
+    o = hp.server_options()
+    assert (o.policy, o.passes_per_step, o.step_budget_mpix) == (hp.SERVER_POLICY_BUDGET, 32, 1200.0)
+    assert (o.max_active, o.inflight_steps, o.wait_limit_ms, o.split_launches) == (64, 2, 2000, 0)
+    assert abs(o.mem_fraction - 0.8) < 1e-7 and o.mem_limit == 0
+    assert (o.debug_stall_request, o.debug_stall_tile, o.debug_fail_step) == (0, 0, 0)
