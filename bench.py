@@ -80,6 +80,8 @@ def parse():
     ap.add_argument("--views", type=int, default=WORKLOAD["views"], help="reduce for profiling captures only")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving leg (N = 1 only)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-plan leg (N = 1 only)")
+    ap.add_argument("--precision-form", action="store_true",
+                    help="print only the config-3 throughput (32 x 3000x2000, S 8, r 7, 12 it., FP32 and FP16-acc)")
     ap.add_argument("--serve-requests", type=int, default=SERVING["requests"])
     ap.add_argument("--serve-rate", type=float, default=SERVING["rate_per_s"], help="Poisson arrivals per second")
     ap.add_argument("--serve-passes", type=int, default=SERVING["passes_per_step"], help="server stages per step")
@@ -838,6 +840,58 @@ def run_reference_params(hp, ctx, stream):
     return out
 
 
+def run_precision_form(hp, device: int):
+    """Config 3 throughput (the precision form's workload): 32 views at 3000x2000 stored FP16 in [0, 1] with
+    N(0, 0.01) noise, fx 2400, the 8 nearest sources each, r 7, 12 iterations, every view a reference - 2304
+    Mpix*iter per solve.  One hp_solve over all 32 views with device-resident maps, FP32 and FP16-acc, at
+    stride 2 (warm-up, then the best of 2) and stride 1 (one timed solve after the stride-2 runs), CUDA events on
+    the engine's stream."""
+    import torch
+    scene = importlib.import_module(PKG + ".scene")
+    s = scene.precision(n_refs=0)
+    n = len(s.views)
+    srcs = [scene.nearest_sources([v.cam for v in s.views], r, 8) for r in range(n)]
+    ctx = hp.Context(device)
+    try:
+        stream = torch.cuda.ExternalStream(ctx.stream_handle)
+        ids = [ctx.upload(v.image) for v in s.views]
+        cam = lambda i: hp.make_camera(s.views[i].cam.K, s.views[i].cam.R, s.views[i].cam.t)
+        jobs = [hp.make_job(ids[r], [ids[i] for i in srcs[r]], cam(r), [cam(i) for i in srcs[r]], *s.depth_range,
+                            seed=42 + r, view_id=r, iterations=12) for r in range(n)]
+        H, W = s.height, s.width
+        maps = [hp.maps_of(torch.empty(H, W, device="cuda"), torch.empty(H, W, 3, device="cuda"),
+                           torch.empty(H, W, device="cuda")) for _ in range(n)]
+        units = n * H * W * 12 / 1e6
+        out = {"workload": f"precision_form_{n}x{W}x{H}", "views": n, "sources": 8, "radius": 7, "iterations": 12,
+               "images": "f16 + N(0, 0.01)", "mpix_iter_per_solve": round(units, 1)}
+
+        def timed(params, reps):
+            best = None
+            for _ in range(reps):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                ctx.solve(jobs, params, maps)
+                e1.record(stream)
+                e1.synchronize()
+                t = e0.elapsed_time(e1)
+                best = t if best is None else min(best, t)
+            return best
+
+        for stride in (2, 1):
+            rates = {}
+            for prec, pk in (("f32", hp.PRECISION_F32), ("f16acc", hp.PRECISION_F16ACC)):
+                params = hp.default_params(radius=7, stride=stride, precision=pk)
+                if stride == 2:
+                    ctx.solve(jobs, params, maps)  # warm-up
+                ms = timed(params, 2 if stride == 2 else 1)
+                rates[prec] = {"ms": round(ms, 1), "mpix_iter_per_s": round(units / (ms / 1e3), 1)}
+            rates["f16acc_over_f32"] = round(rates["f16acc"]["mpix_iter_per_s"] / rates["f32"]["mpix_iter_per_s"], 3)
+            out[f"stride{stride}"] = rates
+        return out
+    finally:
+        ctx.close()
+
+
 def run_reference_gpu(scene_mod):
     """The reference's own kernels (oracle/_ref/libpmref.so: patchmatch_mvs.cu compiled unmodified) on
     REF_PARAM_WORKLOADS, on this box's GPU: pmref.solve_view = init, initial cost and the red-black passes
@@ -912,6 +966,10 @@ def main():
         print(f"warning: --gpus {args.gpus} but WORLD_SIZE {world}", file=sys.stderr)
     if args.count_taps:
         print(json.dumps({"executed_taps": run_count_taps(args)}))
+        return
+    if args.precision_form:
+        hp = importlib.import_module(PKG)
+        print(json.dumps({"precision_form": run_precision_form(hp, local_rank)}))
         return
     if args.serve_only:
         hp = importlib.import_module(PKG)
