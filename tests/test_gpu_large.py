@@ -149,3 +149,32 @@ def test_filter_matches_reference_kernel_at_4000x3000(hp, ctx, scene, pmref):
                                [maps[i][0] for i in srcs], [maps[i][1] for i in srcs], 0.12, cos_tol, 2)
         assert (de == dr).mean() >= 0.9999 and (ce == cr).mean() >= 0.9999, ((de == dr).mean(), (ce == cr).mean())
         assert 0.05 < (de == 0).mean() < 0.95, "the test maps exercise both outcomes"
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_persistent_plan_and_server_equal_solve_at_4000x3000(hp, ctx, ids, scene, precision):
+    """Two 4000x3000 views (23 625 tiles each at 64x8) through one persistent plan and through the server
+    give hp_solve's maps bit for bit: the ticket schedule at the largest view size of the mixes."""
+    s = scene
+    jobs = [hp.make_job(ids[r], [ids[i] for i in s.sources[r][:4]], hp.make_camera(*cam_of(s, r)),
+                        [hp.make_camera(*cam_of(s, i)) for i in s.sources[r][:4]], *s.depth_range, seed=90 + r,
+                        view_id=r, iterations=2) for r in (0, 8)]
+    params = hp.default_params(radius=7, stride=2, precision=precision)
+    want = [hp.host_maps(s.height, s.width) for _ in jobs]
+    ctx.solve(jobs, params, [w[0] for w in want])
+    got = [hp.host_maps(s.height, s.width) for _ in jobs]
+    with hp.Plan(ctx, jobs, params, [g[0] for g in got], hp.plan_options(schedule=hp.SCHEDULE_PERSISTENT)) as plan:
+        plan.run()
+    for g, w in zip(got, want):
+        for a, b in zip(g[1:], w[1:]):
+            assert np.array_equal(a, b)
+    srv_out = [hp.host_maps(s.height, s.width) for _ in jobs]
+    with hp.Server(ctx, params, passes_per_step=3) as srv:
+        for j, o in zip(jobs, srv_out):
+            srv.submit(j, o[0])
+        srv.drain(timeout_ms=120000)
+        done = srv.poll(capacity=8)
+    assert len(done) == 2 and all(c["status"] == 0 for c in done)
+    for g, w in zip(srv_out, want):
+        for a, b in zip(g[1:], w[1:]):
+            assert np.array_equal(a, b)
