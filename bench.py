@@ -82,6 +82,7 @@ def parse():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-plan leg (N = 1 only)")
     ap.add_argument("--precision-form", action="store_true",
                     help="print only the config-3 throughput (32 x 3000x2000, S 8, r 7, 12 it., FP32 and FP16-acc)")
+    ap.add_argument("--no-precision-form", action="store_true", help="skip the config-3 throughput leg (N = 1 only)")
     ap.add_argument("--serve-requests", type=int, default=SERVING["requests"])
     ap.add_argument("--serve-rate", type=float, default=SERVING["rate_per_s"], help="Poisson arrivals per second")
     ap.add_argument("--serve-passes", type=int, default=SERVING["passes_per_step"], help="server stages per step")
@@ -503,6 +504,8 @@ def run_engine(args, rank, world, local_rank):
             line["batched"] = run_batched(args, hp, bctx)
         finally:
             bctx.close()
+    if world == 1 and not args.no_precision_form:
+        line["precision_form"] = run_precision_form(hp, local_rank)
     if hasattr(hp.lib, "hp_debug_check"):  # self-checking engine: failed range checks of every leg since serving's
         import ctypes as C
         a8, a4 = (C.c_int * 12)(), (C.c_int * 12)()
