@@ -565,8 +565,10 @@ std::string describe_members(const StepRec& rec) {
 // Wait for the oldest step and report its finishing requests.  HP_OK, or the
 // status its members fail with: HP_ERR_CUDA for an upload, launch or device
 // error, HP_ERR_TIMEOUT for a persistent launch that gave up (its own wait
-// ran out, or it stopped on the shared abort flag raised before it).
-hp_status retire_oldest(hp_server* s) {
+// ran out, or it stopped on the shared abort flag raised before it).  `cause`
+// (during a recovery): the failed step's status, which the requests of the
+// steps retired behind it take.
+hp_status retire_oldest(hp_server* s, hp_status cause = HP_OK) {
     StepRec rec = std::move(s->inflight.front());
     s->inflight.pop_front();
     RingSlot& slot = s->ring[rec.ring];
@@ -604,8 +606,10 @@ hp_status retire_oldest(hp_server* s) {
         s->st.failed_steps++;
         if (s->err.empty()) note_err_locked(s, "server: a step stopped");
     }
-    // In a step that ran, a finishing request fails alone only when its result copy failed.
-    for (SrvReq* r : rec.finishing) complete(s, r, r->failed ? (failed ? code : HP_ERR_CUDA) : HP_OK, now);
+    // In a step that ran, a finishing request fails alone only when its result copy failed.  During a
+    // recovery (cause set) the requests of the steps behind the failed one fail with its status.
+    const hp_status fail_as = cause != HP_OK ? cause : code;
+    for (SrvReq* r : rec.finishing) complete(s, r, r->failed ? (failed ? fail_as : HP_ERR_CUDA) : HP_OK, now);
     return code;
 }
 
@@ -615,7 +619,7 @@ hp_status retire_oldest(hp_server* s) {
 // behind it), release their state, and clear the abort flag.  The queue is
 // kept; its requests are admitted into clean steps afterwards.
 void recover(hp_server* s, hp_status code) {
-    while (!s->inflight.empty()) retire_oldest(s);
+    while (!s->inflight.empty()) retire_oldest(s, code);
     cudaError_t e = cudaStreamSynchronize(s->stream);
     const auto now = Clock::now();
     std::vector<CoreReq*> lost;

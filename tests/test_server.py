@@ -294,7 +294,7 @@ def test_a_failed_launch_is_contained_without_waiting_out_the_limit(hp, gctx, sc
         later = {rid[c["request_id"]]: c["status"] for c in srv.poll(capacity=64)}
         st = srv.stats()
     assert time.time() - t0 < 20, "a queued launch waited out the dependency limit"
-    assert set(first.values()) <= {0, HP_ERR_CUDA} and HP_ERR_CUDA in first.values()
+    assert set(first.values()) <= {0, HP_ERR_CUDA} and HP_ERR_CUDA in first.values(), first
     assert later == {3: 0, 4: 0, 5: 0} and st["failed_steps"] >= 1
     for k, (d, n, c) in got.items():
         ed, en, ec = _alone(hp, gctx, *reqs[k][:1], params, *reqs[k][1:])
